@@ -1,0 +1,133 @@
+/*
+ * wellbalanced_b200 — C ABI of the B200 ideal-MHD step (libwb200.so).
+ *
+ * Every pointer argument is a DEVICE pointer unless its name ends in `_host`; arrays are
+ * C-contiguous (row-major, the last index fastest). `stream` is a cudaStream_t (NULL:
+ * the legacy default stream). Functions return 0 on success or a negative status
+ * (WB_BAD_ARGUMENT, WB_CUDA_ERROR, WB_UNSUPPORTED, WB_TOO_LARGE); wb_last_error() then
+ * describes the failure (thread-local). Nothing here allocates device memory except
+ * where a function says so.
+ *
+ * Two groups of entry points:
+ *
+ *  1. The reference's six block kernels, same arguments and out-parameter convention
+ *     as `carafe.kernels.<name>.kernel` (float64, one haloed block of X x Y cells):
+ *     the drop-in for the cunumpy kernel slot of carafe/kernels/<name>/__init__.py:9-10.
+ *
+ *  2. The fused engine used by the whole-step path (MHD2D / MHD3D): stage kernels over
+ *     a device work list of patch tiles, the per-step rate / dt reduction, and the
+ *     halo / restriction / flux-register op lists. Structs are laid out as in
+ *     wellbalanced_b200/csrc/layout.cuh and halo.cuh (mirrored by the Python host).
+ */
+#ifndef WELLBALANCED_B200_H
+#define WELLBALANCED_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WB_OK 0
+#define WB_BAD_ARGUMENT (-1)
+#define WB_CUDA_ERROR (-2)
+#define WB_UNSUPPORTED (-3)
+#define WB_TOO_LARGE (-4)
+
+/* Version string of the library. */
+const char* wb_version(void);
+/* Text of the last failure on the calling thread ("" if none). */
+const char* wb_last_error(void);
+
+/* ---- 1. the reference's block kernels (float64) ------------------------------------ */
+
+/* carafe/kernels/mhd_primitive/mhd_primitive_pyccel.py:23-87 — mhd_primitive(rho, mx, my,
+ * mz, energy, bz, az, dx, dy, b0x, b0y, gamma, prim, bxf, byf, ecc) -> int.
+ * Cells (X, Y); az (X+1, Y+1); prim (8, X, Y); bxf (X+1, Y); byf (X, Y+1); ecc (X, Y).
+ * The bad-cell count is ADDED to *bad (a device counter the caller zeroes); the
+ * reference returns it. */
+int wb_mhd_primitive(const double* rho, const double* mx, const double* my, const double* mz,
+                     const double* energy, const double* bz, const double* az, int64_t X, int64_t Y,
+                     double dx, double dy, double b0x, double b0y, double gamma, double* prim,
+                     double* bxf, double* byf, double* ecc, unsigned long long* bad, void* stream);
+
+/* carafe/kernels/mhd_sweep/mhd_sweep_pyccel.py:254-319 — mhd_sweep(prim, bn, axis, limiter,
+ * gamma, flux). prim (8, X, Y); bn (X+1, Y) for axis 0, (X, Y+1) for axis 1; flux
+ * (7, X-3, Y) or (7, X, Y-3). limiter: 0 minmod, 1 vanleer, 2 mc, 3 none. */
+int wb_mhd_sweep(const double* prim, const double* bn, int axis, int limiter, double gamma, int64_t X,
+                 int64_t Y, double* flux, void* stream);
+
+/* carafe/kernels/ct_contact/ct_contact_pyccel.py:26-61 — ct_contact(fx_by, gy_bx, fx_rho,
+ * gy_rho, ecc, ez). fx_* (X-3, Y); gy_* (X, Y-3); ecc (X, Y); ez (na, nb). */
+int wb_ct_contact(const double* fx_by, const double* gy_bx, const double* fx_rho, const double* gy_rho,
+                  const double* ecc, int64_t X, int64_t Y, int64_t na, int64_t nb, double* ez, void* stream);
+
+/* carafe/kernels/mhd_rate/mhd_rate_pyccel.py:30-83 — mhd_rate(rho, mx, my, mz, energy, bz, az,
+ * halo, dx, dy, b0x, b0y, gamma, out). out: device double[2] = (largest rate, smallest rho). */
+int wb_mhd_rate(const double* rho, const double* mx, const double* my, const double* mz,
+                const double* energy, const double* bz, const double* az, int64_t X, int64_t Y, int halo,
+                double dx, double dy, double b0x, double b0y, double gamma, double* out, void* stream);
+
+/* carafe/kernels/mhd_resistive/mhd_resistive_pyccel.py:21-67 — mhd_resistive(prim, bxf, byf,
+ * dx, dy, eta, fx, fy, ez): adds the resistive terms in place. */
+int wb_mhd_resistive(const double* prim, const double* bxf, const double* byf, int64_t X, int64_t Y,
+                     double dx, double dy, double eta, double* fx, double* fy, double* ez, void* stream);
+
+/* carafe/kernels/mhd_conductive/mhd_conductive_pyccel.py:38-100 — mhd_conductive(prim, bxf,
+ * byf, dx, dy, parallel, perpendicular, fx, fy): subtracts the heat flux in place. */
+int wb_mhd_conductive(const double* prim, const double* bxf, const double* byf, int64_t X, int64_t Y,
+                      double dx, double dy, double parallel, double perpendicular, double* fx, double* fy,
+                      void* stream);
+
+/* ---- 2. the fused engine -------------------------------------------------------------- */
+
+/* One RK stage of every tile in `tiles` (struct Tile[ntiles]) of the patches in `patches`
+ * (struct PatchDesc[]), replacing carafe/mhd.py:889-927 (_advance) for MHD2D and
+ * carafe/mhd3d.py:635-671 for MHD3D, with the Heun combine of mhd.py:983-988:
+ *   base == NULL: dst = src - dt L(src);   else dst = (src - dt L(src) + base) / 2.
+ * `precision`: 32 (float state) or 64 (double state); src/base/dst are pools of that type.
+ * dt: device double per instance. bad: device counter of bad cells (added to).
+ * bflux: device double array of boundary-face fluxes (NULL to skip).
+ * lx (3D only): cell planes per tile along x. */
+int wb_stage2d(int precision, const void* src, const void* base, void* dst, const void* patches,
+               const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+               int limiter, unsigned long long* bad, double* bflux, void* stream);
+int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches,
+               const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+               double b0z, int limiter, int lx, unsigned long long* bad, double* bflux, void* stream);
+
+/* Tile shape of the stage kernels: 2D (TX, TY); 3D (TY, TZ). */
+int wb_tile_shape(int ndim, int precision, int* a, int* b);
+
+/* Per-instance max fast-wave rate and min density (carafe/mhd.py:930-963,
+ * carafe/mhd3d.py:674-724) as order-preserving keys: keys[2i], keys[2i+1]. Work list:
+ * chunk_patch[c], chunk_start[c] (up to 2048 cells per chunk). */
+int wb_rate(int precision, int ndim, const void* state, const void* patches, int npatches,
+            const int* chunk_patch, const int* chunk_start, int nchunks, double b0x, double b0y, double b0z,
+            double gamma, unsigned long long* keys, int ninstances, void* stream);
+
+/* dt[i] = cfl * min(1 / rate_i, 0.5 / (D_i * inv_dx2_sum[i])), D_i = max(eta, (gamma - 1)
+ * kappa / min rho_i); with end != NULL clipped to end[i] - time[i] (0 once reached);
+ * advance != 0 adds dt[i] to time[i]. */
+int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, double eta, double kappa,
+                   double gamma, const double* inv_dx2_sum, double* time, const double* end, double* dt,
+                   int advance, void* stream);
+
+/* Halo / restriction / refluxing op lists (struct CopyOp / InterpOp / RestrictOp /
+ * RegisterOp / RefluxOp), replacing patchwork's exchange_halos, restrict and
+ * FluxRegister (carafe/mhd.py:744-777, 906-919, 981, 989-991). */
+int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
+int wb_interp_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
+int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
+int wb_register_ops(const double* bflux, const void* ops, int nops, double* reg, double scale, void* stream);
+int wb_reflux_ops(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
+                  void* stream);
+
+/* Sizes of the engine structs, for callers that mirror them. */
+int wb_struct_sizes(int64_t* sizes_host, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WELLBALANCED_B200_H */

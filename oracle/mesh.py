@@ -161,6 +161,15 @@ class Hierarchy:
             if not self.periodic[a]:
                 continue
             n, e = shape[a], extra[a]
+            if e and len(arrays) == 2:
+                # node n and node 0 are one node: take it from whichever patch covers it
+                values = np.moveaxis(arrays[0], a, 0)
+                mask = np.moveaxis(arrays[1], a, 0)
+                first, last = mask[h].copy(), mask[h + n].copy()
+                values[h + n] = np.where(~last & first, values[h], values[h + n])
+                values[h] = np.where(~first & last, values[h + n], values[h])
+                mask[h] = first | last
+                mask[h + n] = first | last
             for array in arrays:
                 moved = np.moveaxis(array, a, 0)
                 for k in range(1, h + 1):

@@ -1,0 +1,251 @@
+"""The fused device step (MHD2D / MHD3D) against the reference's own runs (GPU).
+
+float64 state: the reference's step to 1e-12 (the golden runs of the reference's
+``MHD2D``/``MHD3D`` — Orszag–Tang, all limiters, outflow rotor, uniform state, multi-patch
+level, Alfvén wave, z-uniform 3D, 3D blast, 3D turbulence). float32 state: the stated
+L1 error against the float64 reference, div B at round-off from the stored potential.
+"""
+
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).with_name("golden")
+
+
+@pytest.fixture(scope="module")
+def runs2d():
+    return np.load(GOLDEN / "runs2d.npz")
+
+
+@pytest.fixture(scope="module")
+def runs3d():
+    return np.load(GOLDEN / "runs3d.npz")
+
+
+def close(state, runs, prefix, tol):
+    for key, value in state.items():
+        np.testing.assert_allclose(value, runs[f"{prefix}_{key}"], rtol=tol, atol=tol, err_msg=f"{prefix}: {key}")
+
+
+def rel_l1(a, b):
+    return float(np.sum(np.abs(a - b)) / np.sum(np.abs(b)))
+
+
+# --- 2D ---------------------------------------------------------------------------------------
+def test_orszag_tang_steps_match_the_reference(runs2d):
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D.orszag_tang(32, precision=64)
+    dts = [model.step() for _ in range(5)]
+    np.testing.assert_allclose(dts, runs2d["ot32_5_dts"], rtol=1e-13)
+    close(model.state(), runs2d, "ot32_5", 1e-12)
+
+
+def test_orszag_tang_run_keeps_div_b_zero_and_conserves(runs2d):
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D.orszag_tang(32, precision=64)
+    before = model.totals()
+    model.run(0.1)
+    after = model.totals()
+    assert model.steps == int(runs2d["ot32_run_steps"])
+    assert model.divergence() < 1e-14
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-13
+    close(model.state(), runs2d, "ot32_run", 1e-11)
+    assert float(model.dataset().pressure.min()) > 0.0
+
+
+@pytest.mark.parametrize("limiter", ["minmod", "vanleer", "mc", "none"])
+def test_every_limiter_matches_the_reference(runs2d, limiter):
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D.orszag_tang(24, limiter=limiter, precision=64)
+    for _ in range(8):
+        model.step()
+    close(model.state(), runs2d, f"ot24_{limiter}", 1e-12)
+
+
+def test_outflow_rotor_uniform_and_alfven_match_the_reference(runs2d):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D.rotor(32, precision=64)
+    model.run(0.02)
+    close(model.state(), runs2d, "rotor32", 1e-11)
+    model = MHD2D(AMRHierarchy((8, 6), ((0.0, 1.0), (0.0, 1.0))), mean_field=(0.3, -0.2), limiter="mc", precision=64)
+    model.set_state(1.0, (0.2, -0.1, 0.05), 0.5, bz=0.4)
+    model.run(0.2)
+    close(model.state(), runs2d, "uniform8x6", 1e-12)
+    model, _ = MHD2D.alfven_wave(16, limiter="none", precision=64)
+    model.run(model.period)
+    close(model.state(), runs2d, "alfven16", 1e-11)
+
+
+def test_brio_wu_along_both_axes_matches_the_reference(runs2d):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    for axis in (0, 1):
+        cells = 64
+        if axis == 0:
+            mesh = AMRHierarchy((cells, 2), ((0.0, 1.0), (0.0, 2.0 / cells)), periodic=(False, True))
+        else:
+            mesh = AMRHierarchy((2, cells), ((0.0, 2.0 / cells), (0.0, 1.0)), periodic=(True, False))
+        model = MHD2D(mesh, gamma=2.0, mean_field=(0.75, 0.0) if axis == 0 else (0.0, 0.75), precision=64)
+        sign = 1.0 if axis == 0 else -1.0
+
+        def s(x, y, axis=axis):
+            return x if axis == 0 else y
+
+        model.set_state(
+            lambda x, y: np.where(s(x, y) < 0.5, 1.0, 0.125),
+            (0.0, 0.0, 0.0),
+            lambda x, y: np.where(s(x, y) < 0.5, 1.0, 0.1),
+            vector_potential=lambda x, y: sign * np.abs(s(x, y) - 0.5),
+        )
+        model.run(0.1)
+        close(model.state(), runs2d, f"briowu{axis}", 1e-11)
+
+
+def test_a_multi_patch_level_matches_the_reference():
+    from wellbalanced_b200.mhd import MHD2D
+
+    golden = np.load(GOLDEN / "multipatch.npz")
+    model = MHD2D.orszag_tang(32, split=(2, 3), precision=64)
+    for _ in range(5):
+        model.step()
+    np.testing.assert_allclose(model.state()["density"], golden["split_density"], rtol=1e-12, atol=1e-12)
+
+
+def test_float32_orszag_tang_error_against_the_float64_reference(runs2d):
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D.orszag_tang(64, limiter="mc", cfl=0.4, precision=32)
+    model.run(0.5)
+    state = model.state()
+    err_rho = rel_l1(state["density"], runs2d["ot64_mc_density"])
+    err_e = rel_l1(state["energy"], runs2d["ot64_mc_energy"])
+    print(f"float32 OT 64^2 to t=0.5: rel L1 rho {err_rho:.3e}, E {err_e:.3e}, steps {model.steps}")
+    assert err_rho < 1e-4 and err_e < 1e-4
+    assert model.divergence() < 1e-12
+
+
+def test_negative_pressure_is_reported():
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    model = MHD2D(AMRHierarchy((8, 8), periodic=(True, True)), precision=64)
+    model.set_state(1.0, (0.0, 0.0, 0.0), 1e-3)
+    (patch,) = model.hierarchy.patches
+    view = model.engine.view(model.engine.state, patch, 4)
+    view[5, 5] = -1.0
+    with pytest.raises(FloatingPointError, match="pressure"):
+        model.step(1e-3)
+
+
+# --- 3D ---------------------------------------------------------------------------------------
+def test_z_uniform_3d_matches_the_reference(runs3d):
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    flat = MHD3D.orszag_tang(16, layers=2, precision=64)
+    for dt in runs3d["ot3d16_dts"]:
+        flat.step(float(dt))
+    close(flat.state(), runs3d, "ot3d16", 1e-12)
+
+
+def test_3d_alfven_blast_and_outflow_match_the_reference(runs3d):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    model, _ = MHD3D.alfven_wave(8, limiter="none", precision=64)
+    model.run(0.1)
+    close(model.state(), runs3d, "alfven3d8", 1e-12)
+    # The blast's quiescent exterior has exactly zero mass flux, where CT-contact's upwind
+    # pick (ct_contact_pyccel.py:17-24) is discontinuous: the reference algorithm itself
+    # moves by 4e-5 after these 6 steps when its energy is perturbed by 1e-15 (oracle
+    # experiment), so this case is compared within that envelope, conservation exactly.
+    model = MHD3D.blast_wave(12, precision=64)
+    before = model.totals()
+    model.run(0.01)
+    close(model.state(), runs3d, "blast3d12", 1e-4)
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-12 * max(1.0, abs(before[name]))
+    assert model.divergence() < 1e-14
+    mesh = AMRHierarchy((6, 4, 5), ((0.0, 1.0),) * 3, periodic=(False, True, False))
+    model = MHD3D(mesh, mean_field=(0.3, -0.2, 0.5), precision=64)
+    model.set_state(1.2, (0.1, -0.2, 0.3), 0.7)
+    for _ in range(4):
+        model.step()
+    close(model.state(), runs3d, "uniform3d", 1e-12)
+    mesh = AMRHierarchy((8, 6, 7), ((0.0, 1.0),) * 3, periodic=(False, True, False))
+    model = MHD3D(mesh, mean_field=(0.3, -0.2, 0.5), limiter="mc", precision=64)
+    model.set_state(
+        lambda x, y, z: 1.0 + 0.3 * np.exp(-((x - 0.4) ** 2 + (y - 0.5) ** 2 + (z - 0.6) ** 2) / 0.05),
+        (0.1, -0.2, 0.3),
+        lambda x, y, z: 0.7 + 0.2 * np.cos(2 * np.pi * y),
+        vector_potential=(
+            lambda x, y, z: 0.05 * np.sin(2 * np.pi * y) * z,
+            lambda x, y, z: 0.05 * x * z,
+            lambda x, y, z: 0.05 * np.cos(2 * np.pi * y) * x,
+        ),
+    )
+    for _ in range(4):
+        model.step()
+    close(model.state(), runs3d, "outflow3d", 1e-12)
+
+
+def _turbulence(precision):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+    from wellbalanced_b200.problems import turbulence_3d
+
+    rho, velocity, p, potential = turbulence_3d(16, seed=7)
+    model = MHD3D(AMRHierarchy((16,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3,
+                  precision=precision)
+    model.set_state(rho, velocity, p, vector_potential=potential)
+    return model
+
+
+def test_3d_turbulence_float64_matches_the_reference(runs3d):
+    model = _turbulence(64)
+    close(model.state(), runs3d, "turb16_init", 1e-14)
+    dts = [model.step() for _ in range(4)]
+    np.testing.assert_allclose(dts, runs3d["turb16_dts"], rtol=1e-13)
+    close(model.state(), runs3d, "turb16", 1e-12)
+
+
+def test_3d_turbulence_float32_error_and_div_b(runs3d):
+    model = _turbulence(32)
+    before = model.totals()
+    for dt in runs3d["turb16_dts"]:
+        model.step(float(dt))
+    state = model.state()
+    err_rho = rel_l1(state["density"], runs3d["turb16_density"])
+    err_e = rel_l1(state["energy"], runs3d["turb16_energy"])
+    print(f"float32 turbulence 16^3, 4 steps: rel L1 rho {err_rho:.3e}, E {err_e:.3e}")
+    assert err_rho < 1e-5 and err_e < 1e-5
+    assert model.divergence() < 1e-12
+    after = model.totals()
+    assert abs(after["density"] - before["density"]) < 1e-5
+
+
+def test_3d_negative_pressure_is_reported():
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    model = MHD3D(AMRHierarchy((4, 4, 4), ((0.0, 1.0),) * 3, periodic=(True,) * 3), precision=64)
+    model.set_state(1.0, (0.0, 0.0, 0.0), 1.0)
+    (patch,) = model.hierarchy.patches
+    model.engine.view(model.engine.state, patch, 4)[3, 3, 3] = -1.0
+    with pytest.raises(FloatingPointError, match="pressure"):
+        model.step(1e-3)

@@ -1,0 +1,147 @@
+"""ctypes binding of libwb200.so (the C ABI of include/wellbalanced_b200.h).
+
+The library is built in-tree (``python -m wellbalanced_b200.build``). Loading fails
+loudly when it is missing: there is no CPU fallback for any product path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "libwb200.so"
+
+_lib = None
+
+c_dp = ctypes.c_void_p
+c_i64 = ctypes.c_int64
+c_int = ctypes.c_int
+c_double = ctypes.c_double
+
+# C signatures: name -> argument types (all return int status)
+SIGNATURES = {
+    "wb_mhd_primitive": [c_dp] * 7 + [c_i64, c_i64] + [c_double] * 5 + [c_dp] * 5 + [c_dp],
+    "wb_mhd_sweep": [c_dp, c_dp, c_int, c_int, c_double, c_i64, c_i64, c_dp, c_dp],
+    "wb_ct_contact": [c_dp] * 5 + [c_i64] * 4 + [c_dp, c_dp],
+    "wb_mhd_rate": [c_dp] * 7 + [c_i64, c_i64, c_int] + [c_double] * 5 + [c_dp, c_dp],
+    "wb_mhd_resistive": [c_dp] * 3 + [c_i64, c_i64] + [c_double] * 3 + [c_dp] * 3 + [c_dp],
+    "wb_mhd_conductive": [c_dp] * 3 + [c_i64, c_i64] + [c_double] * 4 + [c_dp] * 2 + [c_dp],
+    "wb_stage2d": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_int, c_dp,
+                   c_dp, c_dp],
+    "wb_stage3d": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_double,
+                   c_int, c_int, c_dp, c_dp, c_dp],
+    "wb_tile_shape": [c_int, c_int, c_dp, c_dp],
+    "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
+                c_int, c_dp],
+    "wb_finalize_dt": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_copy_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_interp_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_register_ops": [c_dp, c_dp, c_int, c_dp, c_double, c_dp],
+    "wb_reflux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp],
+    "wb_struct_sizes": [c_dp, c_int],
+}
+
+#: Every symbol include/wellbalanced_b200.h declares.
+EXPORTS = ("wb_version", "wb_last_error", *SIGNATURES)
+
+
+class WBError(RuntimeError):
+    """A failure reported by the C ABI (status and wb_last_error text)."""
+
+
+def load():
+    """The loaded library; raises if it is missing (build it first)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBRARY.exists():
+        raise RuntimeError(
+            f"{LIBRARY.name} is not built: run `python -m wellbalanced_b200.build` "
+            "(the CUDA path has no CPU fallback)"
+        )
+    lib = ctypes.CDLL(str(LIBRARY))
+    lib.wb_version.restype = ctypes.c_char_p
+    lib.wb_last_error.restype = ctypes.c_char_p
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    sizes = np.zeros(7, dtype=np.int64)
+    status = lib.wb_struct_sizes(sizes.ctypes.data, 7)
+    if status != 0:
+        raise WBError(lib.wb_last_error().decode())
+    expected = [d.itemsize for d in (PATCH, TILE, COPY_OP, INTERP_OP, RESTRICT_OP, REGISTER_OP, REFLUX_OP)]
+    if list(sizes) != expected:
+        raise RuntimeError(f"struct layout mismatch between host and library: {list(sizes)} != {expected}")
+    _lib = lib
+    return lib
+
+
+def call(name, *args):
+    """Call a C-ABI function; raise WBError on a negative status."""
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != 0:
+        raise WBError(f"{name}: status {status}: {lib.wb_last_error().decode()}")
+    return status
+
+
+def version() -> str:
+    return load().wb_version().decode()
+
+
+# ---- struct mirrors (layout.cuh, halo.cuh) ------------------------------------------------
+PATCH = np.dtype(
+    {
+        "names": ["off", "fstride", "pitch0", "pitch1", "n", "instance", "flags", "level", "dx", "bflux"],
+        "formats": ["<i8", "<i8", "<i8", "<i8", ("<i4", 3), "<i4", "<i4", "<i4", ("<f8", 3), "<i8"],
+        "offsets": [0, 8, 16, 24, 32, 44, 48, 52, 56, 80],
+        "itemsize": 88,
+    }
+)
+TILE = np.dtype({"names": ["patch", "x0", "y0", "z0"], "formats": ["<i4"] * 4, "itemsize": 16})
+COPY_OP = np.dtype(
+    {
+        "names": ["dst", "src1", "src2", "field_lo", "field_hi", "negate", "n", "d", "s1", "m1", "s2", "m2", "w1", "w2"],
+        "formats": ["<i4"] * 6 + [("<i4", 3)] * 6 + ["<f8", "<f8"],
+        "offsets": [0, 4, 8, 12, 16, 20, 24, 36, 48, 60, 72, 84, 96, 104],
+        "itemsize": 112,
+    }
+)
+INTERP_OP = np.dtype(
+    {
+        "names": ["fine", "coarse", "field_lo", "field_hi", "node_mask", "ndim", "n", "d", "fine_lo", "coarse_lo"],
+        "formats": ["<i4"] * 6 + [("<i4", 3)] * 4,
+        "offsets": [0, 4, 8, 12, 16, 20, 24, 36, 48, 60],
+        "itemsize": 72,
+    }
+)
+RESTRICT_OP = np.dtype(
+    {
+        "names": ["fine", "coarse", "field_lo", "field_hi", "node_mask", "ndim", "n", "c", "f"],
+        "formats": ["<i4"] * 6 + [("<i4", 3)] * 3,
+        "offsets": [0, 4, 8, 12, 16, 20, 24, 36, 48],
+        "itemsize": 60,
+    }
+)
+REGISTER_OP = np.dtype(
+    {
+        "names": ["coarse_off", "fine_off", "coarse_stride", "fine_stride", "coarse_start", "fine_start",
+                  "coarse_row", "fine_row", "reg_off", "len", "width", "ncomp", "fine_a", "fine_b"],
+        "formats": ["<i8"] * 9 + ["<i4"] * 5,
+        "offsets": [0, 8, 16, 24, 32, 40, 48, 56, 64, 72, 76, 80, 84, 88],
+        "itemsize": 96,
+    }
+)
+REFLUX_OP = np.dtype(
+    {
+        "names": ["coarse", "len", "width", "ncomp", "c", "t1", "t2", "field", "sign", "dx", "reg_off"],
+        "formats": ["<i4", "<i4", "<i4", "<i4", ("<i4", 3), "<i4", "<i4", ("<i4", 8), "<f8", "<f8", "<i8"],
+        "offsets": [0, 4, 8, 12, 16, 28, 32, 36, 72, 80, 88],
+        "itemsize": 96,
+    }
+)

@@ -1,0 +1,81 @@
+// Op lists of the halo, restriction and reflux kernels (built by the host per layout).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "layout.cuh"
+
+namespace wb {
+
+// dst[d + p] = w1 * src1[s1 + m1 * p] + w2 * src2[s2 + m2 * p], p over the box n,
+// fields [field_lo, field_hi), field `negate` negated. Indices are haloed patch indices.
+struct CopyOp {
+  int32_t dst, src1, src2;
+  int32_t field_lo, field_hi, negate;
+  int32_t n[3];
+  int32_t d[3];
+  int32_t s1[3], m1[3];
+  int32_t s2[3], m2[3];
+  double w1, w2;
+};
+
+// Fine halo box d .. d + n (haloed fine indices) interpolated from the coarse patch.
+struct InterpOp {
+  int32_t fine, coarse;
+  int32_t field_lo, field_hi;
+  int32_t node_mask;  // bit a: axis a is node-centred for these fields
+  int32_t ndim;
+  int32_t n[3];
+  int32_t d[3];
+  int32_t fine_lo[3];    // level index of the fine patch's first interior cell
+  int32_t coarse_lo[3];  // level index of the coarse patch's first interior cell
+};
+
+// Coarse box c .. c + n (haloed coarse indices) from the fine values starting at f.
+struct RestrictOp {
+  int32_t fine, coarse;
+  int32_t field_lo, field_hi;
+  int32_t node_mask;
+  int32_t ndim;
+  int32_t n[3];
+  int32_t c[3];
+  int32_t f[3];
+};
+
+// One coarse-fine interface side: faces of a coarse patch's boundary-flux record and
+// the fine faces over them, accumulated into the register.
+struct RegisterOp {
+  int64_t coarse_off, fine_off;  // offsets of the two patches' boundary-flux blocks
+  int64_t coarse_stride, fine_stride;  // elements between components
+  int64_t coarse_start, fine_start;    // first face of the interface within the side
+  int64_t coarse_row, fine_row;        // elements between rows of the second transverse axis
+  int64_t reg_off;
+  int32_t len, width, ncomp;           // faces (len = rows * width), components
+  int32_t fine_a, fine_b;              // fine faces per coarse face along each transverse axis
+};
+
+// Apply the register of one interface to the coarse cells beside it.
+struct RefluxOp {
+  int32_t coarse;
+  int32_t len, width, ncomp;
+  int32_t c[3];   // haloed index of the first coarse cell
+  int32_t t1, t2; // transverse axes (t2 = -1 in 2D)
+  int32_t field[8];
+  double sign, dx;
+  int64_t reg_off;
+};
+
+template <typename S>
+int launch_copy_ops(S* pool, const PatchDesc* patches, const CopyOp* ops, int nops, cudaStream_t stream);
+template <typename S>
+int launch_interp_ops(S* pool, const PatchDesc* patches, const InterpOp* ops, int nops, cudaStream_t stream);
+template <typename S>
+int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream);
+int launch_register_ops(const double* bflux, const RegisterOp* ops, int nops, double* reg, double scale,
+                        cudaStream_t stream);
+template <typename S>
+int launch_reflux_ops(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
+                      cudaStream_t stream);
+
+}  // namespace wb

@@ -1,0 +1,155 @@
+// Stable time step on device: the fast-wave rate of every cell reduced per instance
+// (carafe/kernels/mhd_rate/mhd_rate_pyccel.py:30-83 in 2D, carafe/mhd3d.py:674-724 in
+// 3D), then dt = cfl / max rate with the diffusion limit (carafe/mhd.py:930-963).
+// Works on the patch pool; no host synchronisation, so a step can be captured in a graph.
+#include "layout.cuh"
+#include "numerics.cuh"
+#include "stage.cuh"
+#include "wb_internal.cuh"
+
+namespace wb {
+
+__global__ void init_keys_kernel(unsigned long long* keys) {
+  keys[0] = double_to_key(0.0);
+  keys[1] = double_to_key(__longlong_as_double(0x7ff0000000000000ll));
+}
+
+__global__ void init_keys_n_kernel(unsigned long long* keys, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    keys[2 * i] = double_to_key(0.0);
+    keys[2 * i + 1] = double_to_key(__longlong_as_double(0x7ff0000000000000ll));
+  }
+}
+
+// 2D: one block per (patch, chunk of cells); grid.y unused.
+template <typename S>
+__global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
+                                                    int npatches, const int* chunk_patch,
+                                                    const int* chunk_start, double b0x, double b0y,
+                                                    double gamma, unsigned long long* keys) {
+  const int pi = chunk_patch[blockIdx.x];
+  const PatchDesc P = patches[pi];
+  const int nx = P.n[0], ny = P.n[1];
+  const S* src = pool + P.off;
+  const int64_t pitch = P.pitch0, fs = P.fstride;
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+  const S g = S(gamma), bx0 = S(b0x), by0 = S(b0y);
+  double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+  const int64_t total = int64_t(nx) * ny;
+  const int64_t start = chunk_start[blockIdx.x];
+  for (int s = 0; s < 8; ++s) {
+    const int64_t t = start + int64_t(s) * blockDim.x + threadIdx.x;
+    if (t >= total) break;
+    const int i = int(t / ny) + kHalo, j = int(t % ny) + kHalo;
+    const int64_t c = int64_t(i) * pitch + j;
+    const S* A = src + 6 * fs;
+    const S r = src[c];
+    const S u = src[fs + c] / r, v = src[2 * fs + c] / r, w = src[3 * fs + c] / r;
+    const S bx = S(0.5) * ((A[c + 1] - A[c]) / dy + bx0 + ((A[c + pitch + 1] - A[c + pitch]) / dy + bx0));
+    const S by = S(0.5) * (-(A[c + pitch] - A[c]) / dx + by0 + (-(A[c + pitch + 1] - A[c + 1]) / dx + by0));
+    const S bz = src[5 * fs + c];
+    const S p = (g - S(1)) * (src[4 * fs + c] - S(0.5) * r * (u * u + v * v + w * w) - S(0.5) * (bx * bx + by * by + bz * bz));
+    const S rate = (rabs(u) + fast_speed(r, p, bx, by, bz, g)) / dx + (rabs(v) + fast_speed(r, p, by, bx, bz, g)) / dy;
+    largest = fmax(largest, double(rate));
+    smallest = fmin(smallest, double(r));
+  }
+  block_reduce_keys(largest, smallest, keys + 2 * P.instance);
+}
+
+template <typename S>
+__global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
+                                                    int npatches, const int* chunk_patch,
+                                                    const int* chunk_start, double b0x, double b0y,
+                                                    double b0z, double gamma, unsigned long long* keys) {
+  const int pi = chunk_patch[blockIdx.x];
+  const PatchDesc P = patches[pi];
+  const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+  const S* src = pool + P.off;
+  const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+  const S g = S(gamma);
+  double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+  const int64_t total = int64_t(nx) * ny * nz;
+  const int64_t start = chunk_start[blockIdx.x];
+  for (int s = 0; s < 8; ++s) {
+    const int64_t t = start + int64_t(s) * blockDim.x + threadIdx.x;
+    if (t >= total) break;
+    const int i = int(t / (int64_t(ny) * nz)) + kHalo;
+    const int j = int((t / nz) % ny) + kHalo;
+    const int k = int(t % nz) + kHalo;
+    const int64_t o = int64_t(i) * p0 + int64_t(j) * p1 + k;
+    const S* Ax = src + 5 * fs;
+    const S* Ay = src + 6 * fs;
+    const S* Az = src + 7 * fs;
+    const S bxl = (Az[o + p1] - Az[o]) / dy - (Ay[o + 1] - Ay[o]) / dz + S(b0x);
+    const S bxh = (Az[o + p0 + p1] - Az[o + p0]) / dy - (Ay[o + p0 + 1] - Ay[o + p0]) / dz + S(b0x);
+    const S byl = (Ax[o + 1] - Ax[o]) / dz - (Az[o + p0] - Az[o]) / dx + S(b0y);
+    const S byh = (Ax[o + p1 + 1] - Ax[o + p1]) / dz - (Az[o + p1 + p0] - Az[o + p1]) / dx + S(b0y);
+    const S bzl = (Ay[o + p0] - Ay[o]) / dx - (Ax[o + p1] - Ax[o]) / dy + S(b0z);
+    const S bzh = (Ay[o + p0 + 1] - Ay[o + 1]) / dx - (Ax[o + p1 + 1] - Ax[o + 1]) / dy + S(b0z);
+    const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
+    const S r = src[o];
+    const S u = src[fs + o] / r, v = src[2 * fs + o] / r, w = src[3 * fs + o] / r;
+    const S p = (g - S(1)) * (src[4 * fs + o] - S(0.5) * r * (u * u + v * v + w * w) - S(0.5) * (bx * bx + by * by + bz * bz));
+    const S rate = (rabs(u) + fast_speed(r, p, bx, by, bz, g)) / dx + (rabs(v) + fast_speed(r, p, by, bz, bx, g)) / dy +
+                   (rabs(w) + fast_speed(r, p, bz, bx, by, g)) / dz;
+    largest = fmax(largest, double(rate));
+    smallest = fmin(smallest, double(r));
+  }
+  block_reduce_keys(largest, smallest, keys + 2 * P.instance);
+}
+
+// The work list of the rate kernels is derived from the patch table on the host and
+// kept by the caller (chunks of 2048 cells).
+template <typename S>
+int launch_rate_chunks(const S* state, const PatchDesc* patches, int npatches, int ndim, const int* chunk_patch,
+                       const int* chunk_start, int nchunks, const double* b0, double gamma,
+                       unsigned long long* keys, int ninstances, cudaStream_t stream) {
+  init_keys_n_kernel<<<(ninstances + 255) / 256, 256, 0, stream>>>(keys, ninstances);
+  if (nchunks > 0) {
+    if (ndim == 2)
+      rate2d_kernel<S><<<nchunks, 256, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
+                                                    gamma, keys);
+    else
+      rate3d_kernel<S><<<nchunks, 256, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
+                                                    b0[2], gamma, keys);
+  }
+  return check_launch("rate");
+}
+
+template int launch_rate_chunks<float>(const float*, const PatchDesc*, int, int, const int*, const int*, int,
+                                       const double*, double, unsigned long long*, int, cudaStream_t);
+template int launch_rate_chunks<double>(const double*, const PatchDesc*, int, int, const int*, const int*, int,
+                                        const double*, double, unsigned long long*, int, cudaStream_t);
+
+__global__ void finalize_dt_kernel(const unsigned long long* keys, int n, double cfl, double eta, double kappa,
+                                   double gamma, const double* inv_dx2_sum, double* time, const double* end,
+                                   double* dt, int advance) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double rate = key_to_double(keys[2 * i]);
+  const double rho_min = key_to_double(keys[2 * i + 1]);
+  double smallest = 1.0 / rate;
+  const double diffusivity = fmax(eta, (gamma - 1.0) * kappa / rho_min);
+  if (diffusivity > 0.0) smallest = fmin(smallest, 0.5 / (diffusivity * inv_dx2_sum[i]));
+  double step = cfl * smallest;
+  if (end) {
+    const double remaining = end[i] - time[i];
+    if (!(time[i] < end[i] * (1.0 - 1e-14))) step = 0.0;
+    step = fmin(step, fmax(remaining, 0.0));
+  }
+  dt[i] = step;
+  if (advance && time) time[i] += step;
+}
+
+int launch_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, double eta, double kappa,
+                       double gamma, const double* inv_dx2_sum, double* time, const double* end, double* dt,
+                       int advance_time, cudaStream_t stream) {
+  if (ninstances > 0)
+    finalize_dt_kernel<<<(ninstances + 255) / 256, 256, 0, stream>>>(keys, ninstances, cfl, eta, kappa, gamma,
+                                                                     inv_dx2_sum, time, end, dt, advance_time);
+  return check_launch("finalize_dt");
+}
+
+}  // namespace wb

@@ -1,0 +1,51 @@
+// Arguments and launchers of the fused stage kernels and the per-step rate kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.cuh"
+
+namespace wb {
+
+// One RK stage over a work list of tiles:
+//   stage 1 (base == nullptr): dst = src - dt L(src)
+//   stage 2 (base != nullptr): dst = (src - dt L(src) + base) / 2   (Heun combine)
+// src is read with its halos; base and dst only at the tile's own cells / nodes, so
+// dst may alias base (stage 2 writes the new state over the start state in place).
+template <typename S>
+struct StageArgs {
+  const S* src;
+  const S* base;
+  S* dst;
+  const PatchDesc* patches;
+  const Tile* tiles;
+  const double* dt;             // per instance
+  double gamma, inv_gm1;
+  double b0[3];
+  unsigned long long* bad;      // count of non-positive / non-finite cells
+  double* bflux;                // boundary-face fluxes of each patch (nullable)
+  int lx;                       // 3D: cell planes per tile along x
+};
+
+template <typename S>
+int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream);
+template <typename S>
+int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream);
+
+void tile_shape_2d(int fp64, int* tx, int* ty);
+void tile_shape_3d(int fp64, int* ty, int* tz);
+
+// Fast-wave rate max and density min of every patch's cells, per instance, as
+// order-preserving keys: keys[2 * instance] (max rate), keys[2 * instance + 1] (min rho).
+// Work list: chunks of up to 2048 cells (chunk_patch[c], chunk_start[c]).
+template <typename S>
+int launch_rate_chunks(const S* state, const PatchDesc* patches, int npatches, int ndim, const int* chunk_patch,
+                       const int* chunk_start, int nchunks, const double* b0, double gamma,
+                       unsigned long long* keys, int ninstances, cudaStream_t stream);
+
+// dt[i] = min(cfl / rate_i, diffusion limit_i, remaining_i); advances time[i] by it.
+int launch_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, double diffusivity,
+                       double conduction, double gamma, const double* inv_dx2_sum, double* time,
+                       const double* end, double* dt, int advance_time, cudaStream_t stream);
+
+}  // namespace wb

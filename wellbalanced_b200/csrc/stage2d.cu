@@ -1,0 +1,275 @@
+// Fused 2D stage kernel: one RK stage of every tile of every patch in one launch.
+//
+// Per tile (TX x TY cells of a patch, a halo of two), all in shared memory:
+//   1. load the conserved cells and A_z nodes, form the face fields (curl of A_z), the
+//      cell field, the primitive variables (pressure recovery in float64), the cell E_z
+//      and count bad cells (mhd_primitive_pyccel.py:23-87);
+//   2. MUSCL + HLLD on every x- and y-face the tile needs (mhd_sweep_pyccel.py:254-319);
+//   3. CT-contact E_z at the tile's nodes (ct_contact_pyccel.py:26-61), walls, and the
+//      stage update of the cells (U -= dt div F, FluxRegister.update) and of A_z
+//      (A -= dt E_z), with the Heun combine in stage 2 (carafe/mhd.py:889-927, 965-994).
+// The primitive variables and fluxes never reach HBM; each stage reads its input state
+// (and, in stage 2, the start state at the cell itself) and writes the new state once.
+#include "layout.cuh"
+#include "numerics.cuh"
+#include "stage.cuh"
+#include "wb_internal.cuh"
+
+namespace wb {
+
+template <typename S>
+struct Tile2D;
+
+template <>
+struct Tile2D<float> {
+  static constexpr int TX = 16, TY = 32;
+};
+template <>
+struct Tile2D<double> {
+  static constexpr int TX = 8, TY = 32;
+};
+
+template <typename S>
+__device__ __forceinline__ S recover_pressure(S r, S m0, S m1, S m2, S e, S bx, S by, S bz, S u, S v,
+                                              S w, double gamma);
+
+// float64: the reference's expression (mhd_primitive_pyccel.py:60-64)
+template <>
+__device__ __forceinline__ double recover_pressure<double>(double r, double, double, double, double e,
+                                                           double bx, double by, double bz, double u,
+                                                           double v, double w, double gamma) {
+  return (gamma - 1.0) * (e - 0.5 * r * (u * u + v * v + w * w) - 0.5 * (bx * bx + by * by + bz * bz));
+}
+
+// float32 state: the same difference evaluated in float64 from the stored values, so
+// the cancellation of low-beta cells costs no extra rounding.
+template <>
+__device__ __forceinline__ float recover_pressure<float>(float r, float m0, float m1, float m2, float e,
+                                                         float bx, float by, float bz, float, float,
+                                                         float, double gamma) {
+  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) / double(r);
+  const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
+  return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
+}
+
+template <typename S>
+__device__ __forceinline__ bool bad_cell(S r, S u, S v, S w, S p, S bx, S by, S bz) {
+  if (!(r > S(0) && p > S(0))) return true;
+  return !(isfinite(r) && isfinite(u) && isfinite(v) && isfinite(w) && isfinite(p) && isfinite(bx) &&
+           isfinite(by) && isfinite(bz));
+}
+
+template <typename S, int LIM>
+__global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
+  constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
+  constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
+  constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sP = reinterpret_cast<S*>(smem_raw);  // [8][NC] primitive variables
+  S* sBx = sP + 8 * NC;                     // [NC] x-face field at each cell's lower x-face
+  S* sBy = sBx + NC;                        // [NC] y-face field at each cell's lower y-face
+  S* sE = sBy + NC;                         // [NC] cell E_z
+  S* sFx = sE + NC;                         // [7][NF] x-face fluxes, face (fi, fj) at fi*FY + fj+1
+  S* sFy = sFx + 7 * NF;                    // [7][NF] y-face fluxes, face (fi, fj) at (fi+1)*FY + fj
+
+  const Tile tile = a.tiles[blockIdx.x];
+  const PatchDesc P = a.patches[tile.patch];
+  const int nx = P.n[0], ny = P.n[1];
+  const int64_t pitch = P.pitch0, fs = P.fstride;
+  const S* __restrict__ src = a.src + P.off;
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+  const S b0x = S(a.b0[0]), b0y = S(a.b0[1]);
+  const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
+  const int x0 = tile.x0, y0 = tile.y0;
+  const int own_nx = nx + ((P.flags & kOwnLast0) ? 1 : 0);
+  const int own_ny = ny + ((P.flags & kOwnLast1) ? 1 : 0);
+
+  // 1. cells and nodes -> primitive variables -------------------------------------
+  unsigned bad = 0;
+  for (int t = threadIdx.x; t < NC; t += blockDim.x) {
+    const int li = t / CY, lj = t - (t / CY) * CY;
+    const int gi = x0 + li, gj = y0 + lj;  // haloed indices
+    S r = S(1), m0 = S(0), m1 = S(0), m2 = S(0), e = S(1), bz = S(0);
+    S bxl = S(0), bxh = S(0), byl = S(0), byh = S(0);
+    const bool valid = gi < nx + 4 && gj < ny + 4;
+    if (valid) {
+      const int64_t c = int64_t(gi) * pitch + gj;
+      r = src[c];
+      m0 = src[fs + c];
+      m1 = src[2 * fs + c];
+      m2 = src[3 * fs + c];
+      e = src[4 * fs + c];
+      bz = src[5 * fs + c];
+      const S* A = src + 6 * fs;
+      const S a00 = A[c], a01 = A[c + 1], a10 = A[c + pitch], a11 = A[c + pitch + 1];
+      bxl = (a01 - a00) / dy + b0x;
+      bxh = (a11 - a10) / dy + b0x;
+      byl = -(a10 - a00) / dx + b0y;
+      byh = -(a11 - a01) / dx + b0y;
+    }
+    const S u = m0 / r, v = m1 / r, w = m2 / r;
+    const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh);
+    S p = recover_pressure<S>(r, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
+    if (!valid) p = S(1);
+    sP[t] = r;
+    sP[NC + t] = u;
+    sP[2 * NC + t] = v;
+    sP[3 * NC + t] = w;
+    sP[4 * NC + t] = p;
+    sP[5 * NC + t] = bx;
+    sP[6 * NC + t] = by;
+    sP[7 * NC + t] = bz;
+    sBx[t] = bxl;
+    sBy[t] = byl;
+    sE[t] = bx * v - by * u;
+    // the tile's own cells
+    const int ci = li - 2, cj = lj - 2;
+    if (valid && ci >= 0 && ci < TX && cj >= 0 && cj < TY && x0 + ci < nx && y0 + cj < ny &&
+        bad_cell(r, u, v, w, p, bx, by, bz))
+      ++bad;
+  }
+  if (bad) atomicAdd(a.bad, (unsigned long long)bad);
+  __syncthreads();
+
+  // 2. x- and y-faces: MUSCL + HLLD -------------------------------------------------
+  for (int t = threadIdx.x; t < 2 * NF; t += blockDim.x) {
+    const bool xface = t < NF;
+    const int u = xface ? t : t - NF;
+    int fi, fj, base, step;
+    S bn;
+    int comp[7];
+    if (xface) {
+      fi = u / FY;           // face fi: between cells fi-1 and fi (tile-relative)
+      fj = u % FY - 1;       // row fj in [-1, TY)
+      base = fi * CY + (fj + 2);  // local cell fi-2 -> li = fi
+      step = CY;
+      bn = sBx[(fi + 2) * CY + fj + 2];
+      comp[0] = 0; comp[1] = 1; comp[2] = 2; comp[3] = 3; comp[4] = 4; comp[5] = 6; comp[6] = 7;
+    } else {
+      fi = u / FY - 1;       // column fi in [-1, TX)
+      fj = u % FY;           // face fj: between cells fj-1 and fj
+      base = (fi + 2) * CY + fj;
+      step = 1;
+      bn = sBy[(fi + 2) * CY + fj + 2];
+      comp[0] = 0; comp[1] = 2; comp[2] = 1; comp[3] = 3; comp[4] = 4; comp[5] = 5; comp[6] = 7;
+    }
+    S q0[7], q1[7], q2[7], q3[7];
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+      const S* row = sP + comp[c] * NC + base;
+      q0[c] = row[0];
+      q1[c] = row[step];
+      q2[c] = row[2 * step];
+      q3[c] = row[3 * step];
+    }
+    S L[7], Rt[7], F[7];
+    reconstruct<LIM>(q0, q1, q2, q3, L, Rt);
+    hlld_flux(L, Rt, bn, gamma, inv_gm1, F);
+    // walls: nothing but the pressure crosses (carafe/mhd.py:874-886)
+    bool wall;
+    if (xface) {
+      const int g = x0 + fi;
+      wall = ((P.flags & kWallLo0) && g == 0) || ((P.flags & kWallHi0) && g == nx);
+    } else {
+      const int g = y0 + fj;
+      wall = ((P.flags & kWallLo1) && g == 0) || ((P.flags & kWallHi1) && g == ny);
+    }
+    if (wall) {
+      F[0] = S(0);
+      F[2] = S(0);
+      F[3] = S(0);
+      F[4] = S(0);
+      F[6] = S(0);
+    }
+    S* out = xface ? sFx + fi * FY + (fj + 1) : sFy + (fi + 1) * FY + fj;
+#pragma unroll
+    for (int c = 0; c < 7; ++c) out[c * NF] = F[c];
+  }
+  __syncthreads();
+
+  // 3. CT-contact E_z at the nodes, A_z and the cells ---------------------------------
+  const S dt = S(a.dt[P.instance]);
+  const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
+  S* __restrict__ dst = a.dst + P.off;
+  for (int t = threadIdx.x; t < TX * TY; t += blockDim.x) {
+    const int ni = t / TY, nj = t % TY;
+    const int gx = x0 + ni, gy = y0 + nj;  // interior node / cell indices
+    if (gx < own_nx && gy < own_ny) {
+      S ez = ct_node(sFx[5 * NF + ni * FY + nj], sFx[5 * NF + ni * FY + nj + 1], sFx[ni * FY + nj],
+                     sFx[ni * FY + nj + 1], sFy[5 * NF + ni * FY + nj], sFy[5 * NF + (ni + 1) * FY + nj],
+                     sFy[ni * FY + nj], sFy[(ni + 1) * FY + nj], sE[(ni + 1) * CY + nj + 1],
+                     sE[(ni + 2) * CY + nj + 1], sE[(ni + 1) * CY + nj + 2], sE[(ni + 2) * CY + nj + 2]);
+      const bool wall = ((P.flags & kWallLo0) && gx == 0) || ((P.flags & kWallHi0) && gx == nx) ||
+                        ((P.flags & kWallLo1) && gy == 0) || ((P.flags & kWallHi1) && gy == ny);
+      if (wall) ez = S(0);
+      const int64_t node = 6 * fs + int64_t(gx + 2) * pitch + (gy + 2);
+      S value = src[node] - dt * ez;
+      if (base_state) value = (value + base_state[node]) * S(0.5);
+      dst[node] = value;
+    }
+    if (gx < nx && gy < ny && ni < TX && nj < TY) {
+      const int64_t cell = int64_t(gx + 2) * pitch + (gy + 2);
+      const int xrow[6] = {0, 1, 2, 3, 4, 6};
+      const int yrow[6] = {0, 2, 1, 3, 4, 6};
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const S div = (sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1]) / dx +
+                      (sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj]) / dy;
+        S value = src[q * fs + cell] - dt * div;
+        if (base_state) value = (value + base_state[q * fs + cell]) * S(0.5);
+        dst[q * fs + cell] = value;
+      }
+      if (a.bflux && P.bflux >= 0) {
+        // boundary-face fluxes of the patch for the flux register, float64
+        double* bf = a.bflux + P.bflux;
+        if (gx == 0 || gx == nx - 1) {
+          const int side = gx == 0 ? 0 : 1;
+          const int fi = gx == 0 ? ni : ni + 1;
+          for (int q = 0; q < 6; ++q)
+            bf[(side * 6 + q) * ny + gy] = double(sFx[xrow[q] * NF + fi * FY + nj + 1]);
+        }
+        if (gy == 0 || gy == ny - 1) {
+          const int side = gy == 0 ? 0 : 1;
+          const int fj = gy == 0 ? nj : nj + 1;
+          double* by = bf + 2 * 6 * ny;
+          for (int q = 0; q < 6; ++q)
+            by[(side * 6 + q) * nx + gx] = double(sFy[yrow[q] * NF + (ni + 1) * FY + fj]);
+        }
+      }
+    }
+  }
+}
+
+template <typename S>
+int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
+  constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
+  constexpr int NC = (TX + 4) * (TY + 4), NF = (TX + 1) * (TY + 1);
+  const size_t smem = sizeof(S) * (11 * NC + 14 * NF);
+  if (ntiles <= 0) return kOk;
+  switch (limiter) {
+#define WB_CASE(L)                                                                                   \
+  case L:                                                                                            \
+    cudaFuncSetAttribute(stage2d_kernel<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+    stage2d_kernel<S, L><<<ntiles, 256, smem, stream>>>(args);                                       \
+    break;
+    WB_CASE(0)
+    WB_CASE(1)
+    WB_CASE(2)
+    WB_CASE(3)
+#undef WB_CASE
+    default:
+      set_error("limiter code %d is not one of 0..3", limiter);
+      return kBadArgument;
+  }
+  return check_launch("stage2d");
+}
+
+template int launch_stage2d<float>(const StageArgs<float>&, int, int, cudaStream_t);
+template int launch_stage2d<double>(const StageArgs<double>&, int, int, cudaStream_t);
+
+void tile_shape_2d(int fp64, int* tx, int* ty) {
+  *tx = fp64 ? Tile2D<double>::TX : Tile2D<float>::TX;
+  *ty = fp64 ? Tile2D<double>::TY : Tile2D<float>::TY;
+}
+
+}  // namespace wb

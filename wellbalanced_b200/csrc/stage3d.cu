@@ -1,0 +1,365 @@
+// Fused 3D stage kernel: one RK stage of the 3D step over a work list of tiles.
+//
+// A tile is TY x TZ columns (y, z) of a patch, marched along x over `lx` cell planes.
+// 288 threads, each with fixed roles per plane:
+//   * one x-face column (j, k) of the L-shaped set the tile needs — its thread keeps
+//     the four cell planes of the x-stencil of that column in registers;
+//   * one y-face and one z-face of the current plane;
+//   * (the first 256) one cell column and the three edges at its lower corner.
+// Per plane p the kernel
+//   A: loads cell plane p+1 (conserved cells; face fields as the curl of the edge
+//      potential, carafe/mhd3d.py:361-386), forms the primitive variables (pressure in
+//      float64 for a float32 state) and the cell electric fields, counts bad cells
+//      (carafe/mhd3d.py:475-509);
+//   B: MUSCL + HLLD on x-face p and on the y- and z-faces of plane p, each in the cyclic
+//      frame of its axis (carafe/mhd3d.py:511-528, mhd_sweep_pyccel.py:254-319);
+//   C: CT-contact edge fields (carafe/mhd3d.py:530-559; ct_contact_pyccel.py:36-61):
+//      E_x on the x-edges of cell plane p, E_y and E_z on node plane p; updates A there
+//      (A -= dt E) and the cells of plane p-1 (U -= dt div F), with the Heun combine in
+//      stage 2 (carafe/mhd3d.py:635-671, 726-754).
+// Primitive variables, fluxes and edge fields stay on chip; each stage reads the state
+// once (plus halo overlap between tiles) and writes it once.
+#include "layout.cuh"
+#include "numerics.cuh"
+#include "stage.cuh"
+#include "wb_internal.cuh"
+
+namespace wb {
+
+template <typename S>
+struct Tile3D {
+  static constexpr int TY = 16, TZ = 16;
+};
+
+template <typename S>
+__device__ __forceinline__ S pressure3(S r, S m0, S m1, S m2, S e, S bx, S by, S bz, S u, S v, S w,
+                                       double gamma);
+
+template <>
+__device__ __forceinline__ double pressure3<double>(double r, double, double, double, double e, double bx,
+                                                    double by, double bz, double u, double v, double w,
+                                                    double gamma) {
+  return (gamma - 1.0) * (e - 0.5 * r * (u * u + v * v + w * w) - 0.5 * (bx * bx + by * by + bz * bz));
+}
+
+template <>
+__device__ __forceinline__ float pressure3<float>(float r, float m0, float m1, float m2, float e, float bx,
+                                                  float by, float bz, float, float, float, double gamma) {
+  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) / double(r);
+  const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
+  return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
+}
+
+template <typename S>
+__device__ __forceinline__ bool bad3(S r, S u, S v, S w, S p, S bx, S by, S bz) {
+  if (!(r > S(0) && p > S(0))) return true;
+  return !(isfinite(r) && isfinite(u) && isfinite(v) && isfinite(w) && isfinite(p) && isfinite(bx) &&
+           isfinite(by) && isfinite(bz));
+}
+
+template <typename S, int LIM>
+__global__ void __launch_bounds__(288) stage3d_kernel(const StageArgs<S> a) {
+  constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
+  constexpr int RZ = TZ + 4, NR = (TY + 4) * (TZ + 4);  // plane region j, k in [-2, T+2)
+  constexpr int GZ = TZ + 1, G = (TY + 1) * (TZ + 1);    // face / column grids
+  constexpr int NCORE = TY * TZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S* sP = reinterpret_cast<S*>(smem_raw);  // [2 slots][8][NR] primitive variables
+  S* sBn = sP + 2 * 8 * NR;                 // [2 slots][3][NR] field at each cell's lower faces
+  S* sEc = sBn + 2 * 3 * NR;                // [3 slots][3][G] cell E_x, E_y, E_z
+  S* sYZ = sEc + 3 * 3 * G;                 // [2 slots][2 dirs][7][G] y- and z-face fluxes
+  S* sX = sYZ + 2 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
+
+  const Tile tile = a.tiles[blockIdx.x];
+  const PatchDesc P = a.patches[tile.patch];
+  const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
+  const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
+  const S* __restrict__ src = a.src + P.off;
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+  const S b0x = S(a.b0[0]), b0y = S(a.b0[1]), b0z = S(a.b0[2]);
+  const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
+  const int x0 = tile.x0, y0 = tile.y0, z0 = tile.z0;
+  const int own_nx = nx + ((P.flags & kOwnLast0) ? 1 : 0);
+  const int own_ny = ny + ((P.flags & kOwnLast1) ? 1 : 0);
+  const int own_nz = nz + ((P.flags & kOwnLast2) ? 1 : 0);
+  const int xe = min(x0 + a.lx, nx);      // cell planes [x0, xe)
+  const int xn = min(x0 + a.lx, own_nx);  // node planes [x0, xn)
+  const int tid = threadIdx.x;
+
+  // roles ------------------------------------------------------------------------------
+  int cj, ck;  // x-face column
+  int yj, yk;  // y-face (face index yj, cell yk)
+  int zj, zk;  // z-face (cell zj, face index zk)
+  if (tid < NCORE) {
+    cj = yj = zj = tid / TZ;
+    ck = yk = zk = tid % TZ;
+  } else if (tid < NCORE + TZ) {
+    cj = -1, ck = tid - NCORE;
+    yj = TY, yk = tid - NCORE;
+    zj = tid - NCORE, zk = TZ;  // TY == TZ
+  } else {
+    cj = tid - NCORE - TZ, ck = -1;
+    yj = tid - NCORE - TZ, yk = -1;
+    zj = -1, zk = tid - NCORE - TZ;
+  }
+  const int col_r = (cj + 2) * RZ + (ck + 2);  // column's position in the plane region
+  const int col_g = (cj + 1) * GZ + (ck + 1);  // column's index in the face grid
+  const int y_g = yj * GZ + (yk + 1);
+  const int z_g = (zj + 1) * GZ + zk;
+
+  S q[4][7];  // x-stencil of the column: planes p-2 .. p+1 (x-frame rows)
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int c = 0; c < 7; ++c) q[s][c] = S(1);
+  S fprev[5] = {S(0), S(0), S(0), S(0), S(0)};
+  S fnow[5] = {S(0), S(0), S(0), S(0), S(0)};
+  const S dt = S(a.dt[P.instance]);
+  const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
+  S* __restrict__ dst = a.dst + P.off;
+  unsigned bad = 0;
+
+  for (int p = x0 - 3; p <= xe; ++p) {
+    // A: load cell plane c = p + 1 ------------------------------------------------------
+    {
+      const int c = p + 1;
+      const int slot = (c + 4) & 1;
+      const int slot3 = (c + 6) % 3;
+      S* P8 = sP + slot * 8 * NR;
+      S* B3 = sBn + slot * 3 * NR;
+      S* E3 = sEc + slot3 * 3 * G;
+      const int I = c + kHalo;
+      for (int r = tid; r < NR; r += blockDim.x) {
+        const int j = r / RZ - 2, k = r % RZ - 2;
+        const int J = y0 + j + kHalo, K = z0 + k + kHalo;
+        S rho = S(1), m0 = S(0), m1 = S(0), m2 = S(0), e = S(1);
+        S bxl = S(0), bxh = S(0), byl = S(0), byh = S(0), bzl = S(0), bzh = S(0);
+        const bool valid = J < ny + 4 && K < nz + 4 && I < nx + 4;
+        if (valid) {
+          const int64_t o = int64_t(I) * p0 + int64_t(J) * p1 + K;
+          rho = src[o];
+          m0 = src[fs + o];
+          m1 = src[2 * fs + o];
+          m2 = src[3 * fs + o];
+          e = src[4 * fs + o];
+          const S* Ax = src + 5 * fs;
+          const S* Ay = src + 6 * fs;
+          const S* Az = src + 7 * fs;
+          // x-faces at nodes I and I+1: dA_z/dy - dA_y/dz + B0x
+          bxl = (Az[o + p1] - Az[o]) / dy - (Ay[o + 1] - Ay[o]) / dz + b0x;
+          bxh = (Az[o + p0 + p1] - Az[o + p0]) / dy - (Ay[o + p0 + 1] - Ay[o + p0]) / dz + b0x;
+          // y-faces at nodes J and J+1: dA_x/dz - dA_z/dx + B0y
+          byl = (Ax[o + 1] - Ax[o]) / dz - (Az[o + p0] - Az[o]) / dx + b0y;
+          byh = (Ax[o + p1 + 1] - Ax[o + p1]) / dz - (Az[o + p1 + p0] - Az[o + p1]) / dx + b0y;
+          // z-faces at nodes K and K+1: dA_y/dx - dA_x/dy + B0z
+          bzl = (Ay[o + p0] - Ay[o]) / dx - (Ax[o + p1] - Ax[o]) / dy + b0z;
+          bzh = (Ay[o + p0 + 1] - Ay[o + 1]) / dx - (Ax[o + p1 + 1] - Ax[o + 1]) / dy + b0z;
+        }
+        const S u = m0 / rho, v = m1 / rho, w = m2 / rho;
+        const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
+        S pr = pressure3<S>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
+        if (!valid) pr = S(1);
+        P8[r] = rho;
+        P8[NR + r] = u;
+        P8[2 * NR + r] = v;
+        P8[3 * NR + r] = w;
+        P8[4 * NR + r] = pr;
+        P8[5 * NR + r] = bx;
+        P8[6 * NR + r] = by;
+        P8[7 * NR + r] = bz;
+        B3[r] = bxl;
+        B3[NR + r] = byl;
+        B3[2 * NR + r] = bzl;
+        if (j >= -1 && j < TY && k >= -1 && k < TZ) {
+          const int g = (j + 1) * GZ + (k + 1);
+          E3[g] = by * w - bz * v;          // E_x
+          E3[G + g] = bz * u - bx * w;      // E_y
+          E3[2 * G + g] = bx * v - by * u;  // E_z
+        }
+        if (valid && c >= x0 && c < xe && j >= 0 && j < TY && k >= 0 && k < TZ && y0 + j < ny &&
+            z0 + k < nz && bad3(rho, u, v, w, pr, bx, by, bz))
+          ++bad;
+      }
+    }
+    __syncthreads();
+
+    // B: faces -----------------------------------------------------------------------------
+    {
+      const int c = p + 1;
+      const S* Pn = sP + ((c + 4) & 1) * 8 * NR;
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) q[s][cc] = q[s + 1][cc];
+      {
+        const int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) q[3][cc] = Pn[xrow[cc] * NR + col_r];
+      }
+      const int slot = (p + 4) & 1;
+      const S* Pp = sP + slot * 8 * NR;
+      const S* Bp = sBn + slot * 3 * NR;
+      if (p >= x0) {
+        S L[7], Rt[7], F[7];
+        reconstruct<LIM>(q[0], q[1], q[2], q[3], L, Rt);
+        hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
+        // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
+        sX[col_g] = F[0];
+        sX[G + col_g] = F[5];
+        sX[2 * G + col_g] = F[6];
+#pragma unroll
+        for (int cc = 0; cc < 5; ++cc) fnow[cc] = F[cc];
+      }
+      const bool need_yz = p >= x0 - 1 && (p < xe || xn > xe);
+      if (need_yz) {
+        S* Y7 = sYZ + (slot * 2 + 0) * 7 * G;
+        S* Z7 = sYZ + (slot * 2 + 1) * 7 * G;
+        {
+          // y-face between cells (yj-1, yk) and (yj, yk): frame (y, z, x)
+          const int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
+          const int r0 = (yj - 2 + 2) * RZ + (yk + 2);
+          S a0[7], a1[7], a2[7], a3[7];
+#pragma unroll
+          for (int cc = 0; cc < 7; ++cc) {
+            const S* row = Pp + yrow[cc] * NR + r0;
+            a0[cc] = row[0];
+            a1[cc] = row[RZ];
+            a2[cc] = row[2 * RZ];
+            a3[cc] = row[3 * RZ];
+          }
+          S L[7], Rt[7], F[7];
+          reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
+          hlld_flux(L, Rt, Bp[NR + (yj + 2) * RZ + (yk + 2)], gamma, inv_gm1, F);
+#pragma unroll
+          for (int cc = 0; cc < 7; ++cc) Y7[cc * G + y_g] = F[cc];
+        }
+        {
+          // z-face between cells (zj, zk-1) and (zj, zk): frame (z, x, y)
+          const int zrow[7] = {0, 3, 1, 2, 4, 5, 6};
+          const int r0 = (zj + 2) * RZ + (zk - 2 + 2);
+          S a0[7], a1[7], a2[7], a3[7];
+#pragma unroll
+          for (int cc = 0; cc < 7; ++cc) {
+            const S* row = Pp + zrow[cc] * NR + r0;
+            a0[cc] = row[0];
+            a1[cc] = row[1];
+            a2[cc] = row[2];
+            a3[cc] = row[3];
+          }
+          S L[7], Rt[7], F[7];
+          reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
+          hlld_flux(L, Rt, Bp[2 * NR + (zj + 2) * RZ + (zk + 2)], gamma, inv_gm1, F);
+#pragma unroll
+          for (int cc = 0; cc < 7; ++cc) Z7[cc * G + z_g] = F[cc];
+        }
+      }
+    }
+    __syncthreads();
+
+    // C: edges and cells ----------------------------------------------------------------
+    if (p >= x0 && tid < NCORE) {
+      const int j = cj, k = ck;
+      const int gj = y0 + j, gk = z0 + k;
+      const int sc = (p + 4) & 1, sp = (p + 3) & 1;  // slots of planes p and p-1
+      const S* Yc = sYZ + (sc * 2 + 0) * 7 * G;
+      const S* Zc = sYZ + (sc * 2 + 1) * 7 * G;
+      const S* Yp = sYZ + (sp * 2 + 0) * 7 * G;
+      const S* Zp = sYZ + (sp * 2 + 1) * 7 * G;
+      const S* Ec = sEc + ((p + 6) % 3) * 3 * G;
+      const S* Ep = sEc + ((p + 5) % 3) * 3 * G;
+      auto yi = [&](int fj, int kk) { return fj * GZ + (kk + 1); };
+      auto zi = [&](int jj, int fk) { return (jj + 1) * GZ + fk; };
+      auto gi = [&](int jj, int kk) { return (jj + 1) * GZ + (kk + 1); };
+      const int I = p + kHalo, J = gj + kHalo, K = gk + kHalo;
+      // cells of plane p-1
+      if (p - 1 >= x0 && p - 1 < xe && gj < ny && gk < nz) {
+        const int64_t o = int64_t(I - 1) * p0 + int64_t(J) * p1 + K;
+        const int yrow[5] = {0, 3, 1, 2, 4};  // y-sweep rows of (rho, m_x, m_y, m_z, E)
+        const int zrow[5] = {0, 2, 3, 1, 4};  // z-sweep rows
+#pragma unroll
+        for (int qf = 0; qf < 5; ++qf) {
+          const S div = (fnow[qf] - fprev[qf]) / dx + (Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)]) / dy +
+                        (Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)]) / dz;
+          S value = src[qf * fs + o] - dt * div;
+          if (base_state) value = (value + base_state[qf * fs + o]) * S(0.5);
+          dst[qf * fs + o] = value;
+        }
+      }
+      // E_x on the x-edges of cell plane p: (a, b) = (y, z)
+      if (p < xe && gj < own_ny && gk < own_nz) {
+        const S ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
+                             Zc[6 * G + zi(j - 1, k)], Zc[6 * G + zi(j, k)], Zc[zi(j - 1, k)], Zc[zi(j, k)],
+                             Ec[gi(j - 1, k - 1)], Ec[gi(j, k - 1)], Ec[gi(j - 1, k)], Ec[gi(j, k)]);
+        const int64_t o = 5 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
+        S value = src[o] - dt * ex;
+        if (base_state) value = (value + base_state[o]) * S(0.5);
+        dst[o] = value;
+      }
+      if (p < xn) {
+        // E_y on the y-edges of node plane p: (a, b) = (z, x)
+        if (gj < ny && gk < own_nz) {
+          const S ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
+                               sX[2 * G + gi(j, k - 1)], sX[2 * G + gi(j, k)], sX[gi(j, k - 1)], sX[gi(j, k)],
+                               Ep[G + gi(j, k - 1)], Ep[G + gi(j, k)], Ec[G + gi(j, k - 1)], Ec[G + gi(j, k)]);
+          const int64_t o = 6 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
+          S value = src[o] - dt * ey;
+          if (base_state) value = (value + base_state[o]) * S(0.5);
+          dst[o] = value;
+        }
+        // E_z on the z-edges of node plane p: (a, b) = (x, y)
+        if (gj < own_ny && gk < nz) {
+          const S ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
+                               Yp[6 * G + yi(j, k)], Yc[6 * G + yi(j, k)], Yp[yi(j, k)], Yc[yi(j, k)],
+                               Ep[2 * G + gi(j - 1, k)], Ec[2 * G + gi(j - 1, k)], Ep[2 * G + gi(j, k)],
+                               Ec[2 * G + gi(j, k)]);
+          const int64_t o = 7 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
+          S value = src[o] - dt * ez;
+          if (base_state) value = (value + base_state[o]) * S(0.5);
+          dst[o] = value;
+        }
+      }
+#pragma unroll
+      for (int cc = 0; cc < 5; ++cc) fprev[cc] = fnow[cc];
+    }
+    __syncthreads();
+  }
+  if (bad) atomicAdd(a.bad, (unsigned long long)bad);
+}
+
+template <typename S>
+int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
+  constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
+  constexpr int NR = (TY + 4) * (TZ + 4), G = (TY + 1) * (TZ + 1);
+  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 3 * 3 * G + 2 * 2 * 7 * G + 3 * G);
+  if (ntiles <= 0) return kOk;
+  if (args.lx <= 0) {
+    set_error("stage3d: lx must be positive");
+    return kBadArgument;
+  }
+  switch (limiter) {
+#define WB_CASE(L)                                                                                   \
+  case L:                                                                                            \
+    cudaFuncSetAttribute(stage3d_kernel<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+    stage3d_kernel<S, L><<<ntiles, 288, smem, stream>>>(args);                                       \
+    break;
+    WB_CASE(0)
+    WB_CASE(1)
+    WB_CASE(2)
+    WB_CASE(3)
+#undef WB_CASE
+    default:
+      set_error("limiter code %d is not one of 0..3", limiter);
+      return kBadArgument;
+  }
+  return check_launch("stage3d");
+}
+
+template int launch_stage3d<float>(const StageArgs<float>&, int, int, cudaStream_t);
+template int launch_stage3d<double>(const StageArgs<double>&, int, int, cudaStream_t);
+
+void tile_shape_3d(int fp64, int* ty, int* tz) {
+  *ty = fp64 ? Tile3D<double>::TY : Tile3D<float>::TY;
+  *tz = fp64 ? Tile3D<double>::TZ : Tile3D<float>::TZ;
+}
+
+}  // namespace wb

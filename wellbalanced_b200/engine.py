@@ -1,0 +1,199 @@
+"""Device state and step driver shared by `MHD2D` and `MHD3D`.
+
+Holds the two state pools of the Heun step (the state U and the stage U1), the layout
+of a hierarchy (`wellbalanced_b200.mesh.Layout`) uploaded to the device, and launches
+through the C ABI:
+
+* ``fill(pool)`` — patchwork's ``exchange_halos`` plus the boundary faces, level by
+  level: interpolation from the level below, same-level copies, outflow / wall faces;
+* ``restrict(pool, groups)`` — patchwork's ``restrict``;
+* ``stage(...)`` — one fused RK stage over every tile;
+* ``rate()`` / ``finalize_dt()`` — the stable step on the device.
+
+One step is the reference's ``step`` (``carafe/mhd.py:965-994``,
+``carafe/mhd3d.py:726-754``): stage 1 into U1, restrict the potential, fill U1, stage 2
+back into U with the Heun combine, reflux, restrict, fill. torch is used for device
+memory and streams only; every numerical kernel is in ``libwb200.so``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from wellbalanced_b200 import _lib
+from wellbalanced_b200.mesh import Layout
+
+_DTYPES = {32: torch.float32, 64: torch.float64}
+
+
+def _ptr(t):
+    return ctypes_ptr(t)
+
+
+def ctypes_ptr(t):
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def _device_bytes(array, device):
+    """A uint8 device tensor holding a numpy structured array (None if empty)."""
+    if array is None or array.size == 0:
+        return None
+    raw = np.ascontiguousarray(array).view(np.uint8).reshape(-1)
+    return torch.from_numpy(raw.copy()).to(device)
+
+
+class Engine:
+    """Device pools + op lists of one hierarchy; the kernels' launch sequence."""
+
+    def __init__(self, hierarchy, *, precision=32, walls=None, limiter=1, gamma=5.0 / 3.0, mean_field=(0.0, 0.0, 0.0),
+                 instances=None, device="cuda", lx=32, stream=None):
+        if precision not in (32, 64):
+            raise ValueError("precision is 32 or 64")
+        if not torch.cuda.is_available():
+            raise RuntimeError("wellbalanced_b200 needs a CUDA device (there is no CPU path)")
+        _lib.load()
+        self.device = torch.device(device)
+        self.precision = precision
+        self.dtype = _DTYPES[precision]
+        self.limiter = int(limiter)
+        self.gamma = float(gamma)
+        self.mean_field = tuple(float(b) for b in mean_field) + (0.0,) * (3 - len(mean_field))
+        self.layout = Layout(hierarchy, walls=walls, precision=precision, lx=lx, instances=instances)
+        L = self.layout
+        self.ndim = L.ndim
+        self.state = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
+        self.stage_pool = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
+        self.patches = _device_bytes(L.rows, self.device)
+        self.tiles = _device_bytes(L.tiles, self.device)
+        self.ntiles = int(L.tiles.size)
+        self.chunk_patch = torch.from_numpy(L.chunk_patch).to(self.device)
+        self.chunk_start = torch.from_numpy(L.chunk_start).to(self.device)
+        self.nchunks = int(L.chunk_patch.size)
+        self.inv_dx2_sum = torch.from_numpy(L.inv_dx2_sum).to(self.device)
+        self.copy_phases = [
+            (_device_bytes(same, self.device), same.size, [(_device_bytes(b, self.device), b.size) for b in bnd])
+            for same, bnd in L.copy_phases
+        ]
+        self.interp_levels = [(_device_bytes(ops, self.device), ops.size) for ops in L.interp_levels]
+        self.restrict_levels = {
+            level: {g: (_device_bytes(ops, self.device), ops.size) for g, ops in groups.items()}
+            for level, groups in L.restrict_levels.items()
+        }
+        n = L.ninstances
+        self.ninstances = n
+        self.dt = torch.zeros(n, dtype=torch.float64, device=self.device)
+        self.keys = torch.zeros(2 * n, dtype=torch.int64, device=self.device)
+        self.time = torch.zeros(n, dtype=torch.float64, device=self.device)
+        self.end = torch.zeros(n, dtype=torch.float64, device=self.device)
+        self.bad = torch.zeros(1, dtype=torch.int64, device=self.device)
+        self.bflux = torch.zeros(max(L.bflux_size, 1), dtype=torch.float64, device=self.device)
+        self.stream = stream
+        #: kernels launched by this engine (counted per C-ABI call)
+        self.launches = 0
+        #: optional list collecting (start, end) CUDA events around each stage kernel
+        self.stage_events = None
+
+    # low-level launches ----------------------------------------------------------------------
+    def _s(self):
+        if self.stream is not None:
+            return self.stream.cuda_stream
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def fill(self, pool, levels=None):
+        """Halos of every patch of `pool`, level by level (coarse first)."""
+        L = self.layout
+        prec = self.precision
+        s = self._s()
+        for level, (same, nsame, boundary) in enumerate(self.copy_phases):
+            if levels is not None and level not in levels:
+                continue
+            interp, ninterp = self.interp_levels[level]
+            if ninterp:
+                _lib.call("wb_interp_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp, s)
+                self.launches += 1
+            if nsame:
+                _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), same.data_ptr(), nsame, s)
+                self.launches += 1
+            for ops, nops in boundary:
+                if nops:
+                    _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), ops.data_ptr(), nops, s)
+                    self.launches += 1
+        del L
+
+    def restrict(self, pool, groups):
+        """Coarse values under finer patches from the fine ones (finest level first)."""
+        s = self._s()
+        for level in range(self.layout.h.max_level, 0, -1):
+            for g in groups:
+                ops, nops = self.restrict_levels[level][g]
+                if nops:
+                    _lib.call("wb_restrict_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                              ops.data_ptr(), nops, s)
+                    self.launches += 1
+
+    def stage(self, src, base, dst, bflux=None):
+        b = self.mean_field
+        s = self._s()
+        if self.ntiles == 0:
+            return
+        timing = self.stage_events is not None
+        if timing:
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(torch.cuda.current_stream(self.device) if self.stream is None else self.stream)
+        self.launches += 1
+        if self.ndim == 2:
+            _lib.call("wb_stage2d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
+                      dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
+                      self.gamma, b[0], b[1], self.limiter, self.bad.data_ptr(),
+                      None if bflux is None else bflux.data_ptr(), s)
+        else:
+            _lib.call("wb_stage3d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
+                      dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
+                      self.gamma, b[0], b[1], b[2], self.limiter, self.layout.lx, self.bad.data_ptr(),
+                      None if bflux is None else bflux.data_ptr(), s)
+        if timing:
+            end.record(torch.cuda.current_stream(self.device) if self.stream is None else self.stream)
+            self.stage_events.append((start, end))
+
+    def rate(self, pool=None):
+        pool = self.state if pool is None else pool
+        b = self.mean_field
+        _lib.call("wb_rate", self.precision, self.ndim, pool.data_ptr(), self.patches.data_ptr(),
+                  self.layout.npatches, self.chunk_patch.data_ptr(), self.chunk_start.data_ptr(), self.nchunks,
+                  b[0], b[1], b[2], self.gamma, self.keys.data_ptr(), self.ninstances, self._s())
+        self.launches += 2 if self.nchunks else 1
+
+    def finalize_dt(self, cfl, eta=0.0, kappa=0.0, *, clip_to_end=False, advance=False):
+        _lib.call("wb_finalize_dt", self.keys.data_ptr(), self.ninstances, float(cfl), float(eta), float(kappa),
+                  self.gamma, self.inv_dx2_sum.data_ptr(), self.time.data_ptr(),
+                  self.end.data_ptr() if clip_to_end else None, self.dt.data_ptr(), int(advance), self._s())
+        self.launches += 1
+
+    def rate_values(self):
+        """(max rate, min density) per instance, on the host."""
+        keys = self.keys.view(torch.int64).cpu().numpy().view(np.uint64).reshape(-1, 2)
+        out = np.empty(keys.shape)
+        for index, k in np.ndenumerate(keys):
+            k = int(k)
+            bits = (k & 0x7FFFFFFFFFFFFFFF) if k >> 63 else (~k & 0xFFFFFFFFFFFFFFFF)
+            out[index] = np.frombuffer(np.uint64(bits).tobytes(), dtype=np.float64)[0]
+        return out
+
+    def heun_step(self, groups_potential, groups_all):
+        """One Heun step with the dt already in self.dt (device)."""
+        U, U1 = self.state, self.stage_pool
+        self.stage(U, None, U1)
+        if self.layout.h.max_level > 0:
+            self.restrict(U1, groups_potential)
+        self.fill(U1)
+        self.stage(U1, U, U)
+        if self.layout.h.max_level > 0:
+            self.restrict(U, groups_all)
+        self.fill(U)
+
+    # host views --------------------------------------------------------------------------------
+    def view(self, pool, patch, field):
+        return self.layout.patch_view(pool, patch, field)

@@ -1,0 +1,564 @@
+"""The patch hierarchy on the device: layout of the state pools and the op lists.
+
+`AMRHierarchy` is the mesh API the solvers use, the part of patchwork's
+(``patchwork-amr`` 0.2.0, absent here) that ``carafe.mhd`` calls: levels refined by 2,
+each a list of patches with boxes in level indices, periodic axes, spacing, and
+``regrid``. `Layout` turns a hierarchy and a field set into what the kernels need:
+
+* a pool layout: every patch's fields with a halo of two, one padded node-shaped array
+  per field (``PatchDesc`` rows);
+* the work lists of the fused stage kernels (tiles) and of the rate kernel (chunks);
+* op lists that replace patchwork's ``exchange_halos`` (copies from same-level patches
+  and periodic images, coarse-to-fine interpolation, outflow / wall faces) and
+  ``restrict``, and the flux-register ops of refluxing.
+
+Node ownership: a patch computes the nodes ``[lo, hi)`` of each axis, and its upper node
+plane too unless same-level patches (or its own periodic image) provide the whole plane;
+every other point of its haloed arrays is filled by the op lists.
+"""
+
+from __future__ import annotations
+
+import itertools
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from wellbalanced_b200 import _lib
+
+HALO = 2
+
+
+@dataclass
+class Patch:
+    level: int
+    box: tuple  # ((lo, hi), ...) in level cell indices
+    index: int = -1
+    is_local: bool = True
+    ranks: list = field(default_factory=lambda: [0])
+
+    @property
+    def shape(self):
+        return tuple(hi - lo for lo, hi in self.box)
+
+
+class AMRHierarchy:
+    """Levels of patches over a Cartesian box (refinement ratio 2).
+
+    Args mirror the patchwork constructor the reference calls
+    (``AMRHierarchy(shape, bounds, periodic=..., comm=..., placement=...)``); ``split``
+    cuts the base level into that many patches per axis.
+    """
+
+    refinement_ratio = 2
+
+    def __init__(self, shape, bounds=None, periodic=None, *, comm=None, placement="all", geometry="cartesian",
+                 split=None):
+        self.shape = tuple(int(n) for n in shape)
+        self.ndim = len(self.shape)
+        if self.ndim not in (1, 2, 3):
+            raise ValueError("a hierarchy has 1 to 3 axes")
+        bounds = bounds or ((0.0, 1.0),) * self.ndim
+        self.bounds = tuple((float(lo), float(hi)) for lo, hi in bounds)
+        self.lower_bound = tuple(lo for lo, _ in self.bounds)
+        self.periodic = tuple(bool(p) for p in (periodic or (False,) * self.ndim))
+        self.cylindrical = geometry == "cylindrical"
+        self.graded = False
+        self.comm = comm
+        self.placement = placement
+        self.patches: list[Patch] = []
+        split = split or (1,) * self.ndim
+        cuts = [np.linspace(0, n, s + 1).round().astype(int) for n, s in zip(self.shape, split, strict=True)]
+        for index in itertools.product(*(range(s) for s in split)):
+            box = tuple((int(c[k]), int(c[k + 1])) for c, k in zip(cuts, index, strict=True))
+            self._append(Patch(0, box))
+
+    def _append(self, patch):
+        patch.index = len(self.patches)
+        self.patches.append(patch)
+        return patch
+
+    @property
+    def max_level(self):
+        return max(p.level for p in self.patches)
+
+    @property
+    def local_patches(self):
+        return self.patches
+
+    def level_shape(self, level):
+        return tuple(n * 2**level for n in self.shape)
+
+    def spacing(self, level):
+        return tuple((hi - lo) / n for (lo, hi), n in zip(self.bounds, self.level_shape(level), strict=True))
+
+    def patches_at_level(self, level):
+        return [p for p in self.patches if p.level == level]
+
+    def add_patch(self, level, box):
+        """A patch on ``level`` (>= 1) over ``box``, aligned to the coarse cells."""
+        box = tuple((int(lo), int(hi)) for lo, hi in box)
+        if level < 1 or level > self.max_level + 1:
+            raise ValueError("patches are added one level above an existing one")
+        shape = self.level_shape(level)
+        for (lo, hi), n in zip(box, shape, strict=True):
+            if not 0 <= lo < hi <= n:
+                raise ValueError(f"box {box} is outside level {level} of shape {shape}")
+            if lo % 2 or hi % 2:
+                raise ValueError(f"box {box} is not aligned to the cells of level {level - 1}")
+            if hi - lo < 4:
+                raise ValueError("a refined patch needs at least 4 cells per axis")
+        return self._append(Patch(level, box))
+
+    def regrid(self, tags, *, max_patch_size=None, buffer=1, min_patch_size=4):
+        """A new hierarchy with patches covering the tagged cells of each level.
+
+        ``tags[level]`` is a boolean array of that level's shape; the tagged cells grow
+        by ``buffer`` cells, are clustered into boxes of at most ``max_patch_size``
+        coarse cells per side (``cluster_tags``), and refined. Levels above the tagged
+        ones are dropped.
+        """
+        from wellbalanced_b200.regrid import cluster_tags
+
+        new = AMRHierarchy(self.shape, self.bounds, self.periodic, comm=self.comm, placement=self.placement)
+        new.patches = []
+        for patch in self.patches_at_level(0):
+            new._append(Patch(0, patch.box))
+        levels = sorted(tags)
+        for level in levels:
+            if level > new.max_level:
+                break
+            boxes = cluster_tags(
+                np.asarray(tags[level], dtype=bool),
+                buffer=buffer,
+                max_size=max_patch_size,
+                min_size=min_patch_size,
+                parents=[p.box for p in new.patches_at_level(level)],
+                periodic=self.periodic,
+            )
+            for box in boxes:
+                new._append(Patch(level + 1, tuple((2 * lo, 2 * hi) for lo, hi in box)))
+        return new
+
+
+# ---- field sets -----------------------------------------------------------------------------
+@dataclass(frozen=True)
+class FieldGroup:
+    lo: int
+    hi: int
+    node_mask: int  # bit a: axis a is node-centred
+
+
+def field_groups(ndim):
+    """The field groups of the MHD state: 2D (6 cells, A_z nodes), 3D (5 cells, 3 edges)."""
+    if ndim == 2:
+        return (FieldGroup(0, 6, 0b00), FieldGroup(6, 7, 0b11))
+    return (FieldGroup(0, 5, 0b000), FieldGroup(5, 6, 0b110), FieldGroup(6, 7, 0b101), FieldGroup(7, 8, 0b011))
+
+
+def _boxes_intersect(a, b):
+    out = []
+    for (alo, ahi), (blo, bhi) in zip(a, b, strict=True):
+        lo, hi = max(alo, blo), min(ahi, bhi)
+        if lo >= hi:
+            return None
+        out.append((lo, hi))
+    return tuple(out)
+
+
+class Layout:
+    """Pool layout, work lists and op lists of a hierarchy for the MHD state."""
+
+    def __init__(self, hierarchy: AMRHierarchy, *, walls=None, precision=32, lx=32, instances=None,
+                 align=8):
+        self.h = hierarchy
+        self.ndim = hierarchy.ndim
+        if self.ndim not in (2, 3):
+            raise ValueError("the MHD state lives on 2D or 3D hierarchies")
+        self.nfields = 7 if self.ndim == 2 else 8
+        self.groups = field_groups(self.ndim)
+        self.precision = precision
+        self.lx = lx
+        self.walls = walls or ((False, False),) * self.ndim
+        patches = hierarchy.patches
+        self.npatches = len(patches)
+        self.instances = np.zeros(self.npatches, dtype=np.int32) if instances is None else np.asarray(instances, np.int32)
+        self.ninstances = int(self.instances.max()) + 1 if self.npatches else 1
+        self._own_last()
+        self._pool(align)
+        self._tiles()
+        self._chunks()
+        self.copy_phases = self._copy_ops()
+        self.interp_levels = self._interp_ops()
+        self.restrict_levels = self._restrict_ops()
+
+    # ownership ---------------------------------------------------------------------------
+    def _own_last(self):
+        """own[p][a]: whether patch p computes its upper node plane along axis a."""
+        h = self.h
+        self.own = []
+        for p in h.patches:
+            flags = []
+            for a in range(self.ndim):
+                flags.append(not self._plane_provided(p, a))
+            self.own.append(tuple(flags))
+
+    def _plane_provided(self, p, a):
+        """Whether same-level patches' lower node planes cover p's upper plane along a."""
+        h = self.h
+        n_level = h.level_shape(p.level)[a]
+        plane = p.box[a][1]
+        # transverse node range of the plane, inclusive
+        need = [(p.box[b][0], p.box[b][1] + 1) for b in range(self.ndim) if b != a]
+        covered = np.zeros([hi - lo for lo, hi in need], dtype=bool)
+        for q in h.patches_at_level(p.level):
+            lo = q.box[a][0]
+            if lo == plane or (h.periodic[a] and lo + n_level == plane):
+                # q's computed node range along the transverse axes (its lower plane),
+                # conservatively [lo, hi) there: its upper nodes may be someone else's
+                idx = []
+                for (nlo, nhi), b in zip(need, [b for b in range(self.ndim) if b != a], strict=True):
+                    qlo, qhi = q.box[b]
+                    s, e = max(nlo, qlo), min(nhi, qhi + 1)
+                    if s >= e:
+                        break
+                    idx.append(slice(s - nlo, e - nlo))
+                else:
+                    covered[tuple(idx)] = True
+        return bool(covered.all())
+
+    # pool ----------------------------------------------------------------------------------
+    def _pool(self, align):
+        h = self.h
+        rows = np.zeros(self.npatches, dtype=_lib.PATCH)
+        offset = 0
+        bflux = 0
+        ncons = 6 if self.ndim == 2 else 5
+        self.bflux_size = 0
+        for p in h.patches:
+            n = list(p.shape) + [1] * (3 - self.ndim)
+            dims = [p.shape[a] + 5 for a in range(self.ndim)]  # node-shaped, halo 2
+            inner = dims[-1]
+            inner = (inner + align - 1) // align * align
+            if self.ndim == 2:
+                pitch0, pitch1 = inner, 0
+                size = dims[0] * inner
+            else:
+                pitch1 = inner
+                pitch0 = dims[1] * inner
+                size = dims[0] * pitch0
+            size = (size + 31) // 32 * 32
+            r = rows[p.index]
+            r["off"] = offset
+            r["fstride"] = size
+            r["pitch0"] = pitch0
+            r["pitch1"] = pitch1
+            r["n"] = n
+            r["instance"] = self.instances[p.index]
+            flags = 0
+            for a in range(self.ndim):
+                lower, upper = self._wall_sides(p, a)
+                if lower:
+                    flags |= 1 << (2 * a)
+                if upper:
+                    flags |= 1 << (2 * a + 1)
+                if self.own[p.index][a]:
+                    flags |= 1 << (8 + a)
+            r["flags"] = flags
+            r["level"] = p.level
+            r["dx"] = list(h.spacing(p.level)) + [1.0] * (3 - self.ndim)
+            r["bflux"] = bflux
+            faces = sum(2 * int(np.prod([p.shape[b] for b in range(self.ndim) if b != a])) for a in range(self.ndim))
+            bflux += faces * ncons
+            offset += self.nfields * size
+        self.rows = rows
+        self.pool_size = offset
+        self.bflux_size = bflux
+
+    def _wall_sides(self, p, a):
+        shape = self.h.level_shape(p.level)
+        lower_wall, upper_wall = self.walls[a]
+        return (lower_wall and p.box[a][0] == 0, upper_wall and p.box[a][1] == shape[a])
+
+    def patch_view(self, pool, p, f):
+        """A view of field f of patch p in `pool` (a 1-D tensor/array), haloed shape."""
+        r = self.rows[p.index]
+        start = int(r["off"] + f * r["fstride"])
+        if self.ndim == 2:
+            X, P0 = p.shape[0] + 5, int(r["pitch0"])
+            view = pool[start : start + X * P0].reshape(X, P0)
+            return view[:, : p.shape[1] + 5]
+        X, Y = p.shape[0] + 5, p.shape[1] + 5
+        P0, P1 = int(r["pitch0"]), int(r["pitch1"])
+        view = pool[start : start + X * P0].reshape(X, Y, P1)
+        return view[:, :, : p.shape[2] + 5]
+
+    # work lists ----------------------------------------------------------------------------
+    def _tiles(self):
+        lib = _lib.load()
+        import ctypes
+
+        a, b = ctypes.c_int(), ctypes.c_int()
+        _lib.call("wb_tile_shape", self.ndim, self.precision, ctypes.addressof(a), ctypes.addressof(b))
+        self.tile_shape = (a.value, b.value)
+        del lib
+        tiles = []
+        for p in self.h.patches:
+            own = [p.shape[a] + (1 if self.own[p.index][a] else 0) for a in range(self.ndim)]
+            if self.ndim == 2:
+                tx, ty = self.tile_shape
+                for x0 in range(0, own[0], tx):
+                    for y0 in range(0, own[1], ty):
+                        tiles.append((p.index, x0, y0, 0))
+            else:
+                ty, tz = self.tile_shape
+                for x0 in range(0, own[0], self.lx):
+                    for y0 in range(0, own[1], ty):
+                        for z0 in range(0, own[2], tz):
+                            tiles.append((p.index, x0, y0, z0))
+        self.tiles = np.array(tiles, dtype=np.int32).view(_lib.TILE).reshape(-1) if tiles else np.zeros(0, _lib.TILE)
+
+    def _chunks(self, per=2048):
+        patch, start = [], []
+        for p in self.h.patches:
+            cells = int(np.prod(p.shape))
+            for s in range(0, cells, per):
+                patch.append(p.index)
+                start.append(s)
+        self.chunk_patch = np.array(patch, dtype=np.int32)
+        self.chunk_start = np.array(start, dtype=np.int32)
+        # finest sum of inverse squared spacings per instance (diffusion limit)
+        inv = np.zeros(self.ninstances)
+        for p in self.h.patches:
+            s = sum(d**-2 for d in self.h.spacing(p.level))
+            inv[self.instances[p.index]] = max(inv[self.instances[p.index]], s)
+        self.inv_dx2_sum = inv
+
+    # same-level copies and physical boundaries ----------------------------------------------
+    def _computed_box(self, p, g):
+        """Computed points of patch p for field group g, as haloed index ranges."""
+        out = []
+        for a in range(self.ndim):
+            node = (g.node_mask >> a) & 1
+            n = p.shape[a]
+            hi = HALO + n + (1 if node and self.own[p.index][a] else 0)
+            out.append((HALO, hi))
+        return tuple(out)
+
+    def _haloed_size(self, p, g, a):
+        return p.shape[a] + 4 + ((g.node_mask >> a) & 1)
+
+    def _halo_slabs(self, p, g):
+        """The halo of p (haloed box minus computed box) as disjoint boxes."""
+        full = [(0, self._haloed_size(p, g, a)) for a in range(self.ndim)]
+        comp = self._computed_box(p, g)
+        slabs = []
+        for a in range(self.ndim):
+            for side in (0, 1):
+                box = []
+                for b in range(self.ndim):
+                    if b < a:
+                        box.append(comp[b])
+                    elif b == a:
+                        box.append((full[a][0], comp[a][0]) if side == 0 else (comp[a][1], full[a][1]))
+                    else:
+                        box.append(full[b])
+                if all(lo < hi for lo, hi in box):
+                    slabs.append(tuple(box))
+        return slabs
+
+    def _copy_ops(self):
+        """Per level: same-level copy ops, then boundary ops per axis (op arrays)."""
+        h = self.h
+        phases = []
+        for level in range(h.max_level + 1):
+            same = []
+            patches = h.patches_at_level(level)
+            n_level = h.level_shape(level)
+            for p in patches:
+                for g in self.groups:
+                    slabs = self._halo_slabs(p, g)
+                    for q in patches:
+                        comp_q = self._computed_box(q, g)
+                        shifts = [(0,) if not h.periodic[a] else (-n_level[a], 0, n_level[a]) for a in range(self.ndim)]
+                        for shift in itertools.product(*shifts):
+                            # q's computed points in p's haloed coordinates
+                            src = tuple(
+                                (lo + q.box[a][0] + shift[a] - p.box[a][0], hi + q.box[a][0] + shift[a] - p.box[a][0])
+                                for a, (lo, hi) in enumerate(comp_q)
+                            )
+                            for slab in slabs:
+                                box = _boxes_intersect(slab, src)
+                                if box is None:
+                                    continue
+                                op = np.zeros((), dtype=_lib.COPY_OP)
+                                op["dst"], op["src1"], op["src2"] = p.index, q.index, -1
+                                op["field_lo"], op["field_hi"], op["negate"] = g.lo, g.hi, -1
+                                n = [hi - lo for lo, hi in box] + [1] * (3 - self.ndim)
+                                d = [lo for lo, _ in box] + [0] * (3 - self.ndim)
+                                s1 = [lo - q.box[a][0] - shift[a] + p.box[a][0] for a, (lo, _) in enumerate(box)]
+                                s1 += [0] * (3 - self.ndim)
+                                op["n"], op["d"], op["s1"] = n, d, s1
+                                op["m1"] = [1, 1, 1]
+                                op["s2"], op["m2"] = [0, 0, 0], [0, 0, 0]
+                                op["w1"], op["w2"] = 1.0, 0.0
+                                same.append(op)
+            boundary = [[] for _ in range(self.ndim)]
+            for p in patches:
+                for a in range(self.ndim):
+                    if h.periodic[a]:
+                        continue
+                    lower = p.box[a][0] == 0
+                    upper = p.box[a][1] == n_level[a]
+                    wall = self.walls[a]
+                    for g in self.groups:
+                        boundary[a] += self._boundary_ops(p, g, a, lower, upper, wall)
+            phases.append((self._pack(same, _lib.COPY_OP), [self._pack(b, _lib.COPY_OP) for b in boundary]))
+        return phases
+
+    def _boundary_ops(self, p, g, a, lower, upper, wall):
+        ops = []
+        size = [self._haloed_size(p, g, b) for b in range(self.ndim)]
+        node = (g.node_mask >> a) & 1
+        N = size[a]
+
+        def make(d_lo, count, s1, m1a, w1, s2=0, m2a=0, w2=0.0, negate=-1):
+            op = np.zeros((), dtype=_lib.COPY_OP)
+            op["dst"], op["src1"], op["src2"] = p.index, p.index, p.index
+            op["field_lo"], op["field_hi"], op["negate"] = g.lo, g.hi, negate
+            n = list(size) + [1] * (3 - self.ndim)
+            n[a] = count
+            d = [0, 0, 0]
+            d[a] = d_lo
+            src1 = [0, 0, 0]
+            src1[a] = s1
+            m1 = [1, 1, 1]
+            m1[a] = m1a
+            src2 = [0, 0, 0]
+            src2[a] = s2
+            m2 = [1, 1, 1]
+            m2[a] = m2a
+            op["n"], op["d"], op["s1"], op["m1"], op["s2"], op["m2"] = n, d, src1, m1, src2, m2
+            op["w1"], op["w2"] = w1, w2
+            return op
+
+        for side, active in ((0, lower), (1, upper)):
+            if not active:
+                continue
+            is_wall = wall[side]
+            if g.node_mask == 0 or (self.ndim == 3 and not node and g.lo >= 5):
+                # cell-centred along a
+                if self.ndim == 3 and g.lo >= 5:
+                    # edge potentials along their own (cell-centred) axis: linear extrapolation
+                    ops += self._node_extrapolation(make, side, N)
+                    continue
+                negate = (1 + a) if is_wall else -1
+                if not is_wall:
+                    if side == 0:
+                        ops.append(make(0, HALO, HALO, 0, 1.0))
+                    else:
+                        ops.append(make(N - HALO, HALO, N - HALO - 1, 0, 1.0))
+                else:
+                    if side == 0:  # dst 1-k <- src 2+k
+                        ops.append(make(0, HALO, 2 * HALO - 1, -1, 1.0, negate=negate))
+                    else:  # dst N-2+k <- src N-3-k
+                        ops.append(make(N - HALO, HALO, N - HALO - 1, -1, 1.0, negate=negate))
+            else:
+                if is_wall:
+                    for k in range(1, HALO + 1):
+                        if side == 0:  # moved[h-k] = 2 moved[h] - moved[h+k]
+                            ops.append(make(HALO - k, 1, HALO, 0, 2.0, HALO + k, 0, -1.0))
+                        else:
+                            e = N - HALO - 1
+                            ops.append(make(e + k, 1, e, 0, 2.0, e - k, 0, -1.0))
+                else:
+                    ops += self._node_extrapolation(make, side, N)
+        return ops
+
+    @staticmethod
+    def _node_extrapolation(make, side, N):
+        ops = []
+        for k in range(1, HALO + 1):
+            if side == 0:  # moved[h-k] = (1+k) moved[h] - k moved[h+1]
+                ops.append(make(HALO - k, 1, HALO, 0, 1.0 + k, HALO + 1, 0, -float(k)))
+            else:
+                e = N - HALO - 1
+                ops.append(make(e + k, 1, e, 0, 1.0 + k, e - 1, 0, -float(k)))
+        return ops
+
+    # coarse-fine ---------------------------------------------------------------------------
+    def _interp_ops(self):
+        """Per level >= 1: ops interpolating every halo point of its patches from below."""
+        h = self.h
+        levels = [np.zeros(0, _lib.INTERP_OP)]
+        for level in range(1, h.max_level + 1):
+            ops = []
+            n_coarse = h.level_shape(level - 1)
+            for f in h.patches_at_level(level):
+                for g in self.groups:
+                    slabs = self._halo_slabs(f, g)
+                    for c in h.patches_at_level(level - 1):
+                        shifts = [(0,) if not h.periodic[a] else (-n_coarse[a], 0, n_coarse[a]) for a in range(self.ndim)]
+                        for shift in itertools.product(*shifts):
+                            # fine haloed points whose coarse parent lies in c (+ shift)
+                            region = []
+                            for a in range(self.ndim):
+                                node = (g.node_mask >> a) & 1
+                                clo = c.box[a][0] + shift[a]
+                                chi = c.box[a][1] + shift[a] + node  # node parents include hi
+                                # parent(g) = floor(g / 2) in [clo, chi)  <=>  g in [2 clo, 2 chi)
+                                glo, ghi = 2 * clo, 2 * chi
+                                region.append((glo - f.box[a][0] + HALO, ghi - f.box[a][0] + HALO))
+                            for slab in slabs:
+                                box = _boxes_intersect(slab, tuple(region))
+                                if box is None:
+                                    continue
+                                op = np.zeros((), dtype=_lib.INTERP_OP)
+                                op["fine"], op["coarse"] = f.index, c.index
+                                op["field_lo"], op["field_hi"] = g.lo, g.hi
+                                op["node_mask"], op["ndim"] = g.node_mask, self.ndim
+                                op["n"] = [hi - lo for lo, hi in box] + [1] * (3 - self.ndim)
+                                op["d"] = [lo for lo, _ in box] + [0] * (3 - self.ndim)
+                                op["fine_lo"] = [f.box[a][0] for a in range(self.ndim)] + [0] * (3 - self.ndim)
+                                op["coarse_lo"] = [c.box[a][0] + shift[a] for a in range(self.ndim)] + [0] * (3 - self.ndim)
+                                ops.append(op)
+            levels.append(self._pack(ops, _lib.INTERP_OP))
+        return levels
+
+    def _restrict_ops(self):
+        """Per level >= 1, ops setting the level below from it, per field group."""
+        h = self.h
+        levels = {0: {}}
+        for level in range(1, h.max_level + 1):
+            per_group = {}
+            for g in self.groups:
+                ops = []
+                for f in h.patches_at_level(level):
+                    for c in h.patches_at_level(level - 1):
+                        cbox = self._computed_box(c, g)
+                        ranges = []
+                        for a in range(self.ndim):
+                            node = (g.node_mask >> a) & 1
+                            lo = max(f.box[a][0] // 2, c.box[a][0])
+                            hi = min(f.box[a][1] // 2 + node, c.box[a][0] + cbox[a][1] - HALO)
+                            if lo >= hi:
+                                break
+                            ranges.append((lo, hi))
+                        else:
+                            op = np.zeros((), dtype=_lib.RESTRICT_OP)
+                            op["fine"], op["coarse"] = f.index, c.index
+                            op["field_lo"], op["field_hi"] = g.lo, g.hi
+                            op["node_mask"], op["ndim"] = g.node_mask, self.ndim
+                            op["n"] = [hi - lo for lo, hi in ranges] + [1] * (3 - self.ndim)
+                            op["c"] = [lo - c.box[a][0] + HALO for a, (lo, _) in enumerate(ranges)] + [0] * (3 - self.ndim)
+                            op["f"] = [2 * lo - f.box[a][0] + HALO for a, (lo, _) in enumerate(ranges)] + [0] * (3 - self.ndim)
+                            ops.append(op)
+                per_group[g] = self._pack(ops, _lib.RESTRICT_OP)
+            levels[level] = per_group
+        return levels
+
+    @staticmethod
+    def _pack(ops, dtype):
+        if not ops:
+            return np.zeros(0, dtype)
+        return np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)

@@ -23,10 +23,11 @@ import numpy as np
 
 
 def _shell_filter(shape, kmin, kmax, power):
-    axes = [np.fft.fftfreq(n, 1.0 / n) for n in shape]
-    kk = np.meshgrid(*axes, indexing="ij")
+    """sqrt(P(k)) on the half spectrum of a real FFT, zero outside kmin <= |k| <= kmax."""
+    axes = [np.fft.fftfreq(n, 1.0 / n) for n in shape[:-1]] + [np.fft.rfftfreq(shape[-1], 1.0 / shape[-1])]
+    kk = np.meshgrid(*axes, indexing="ij", sparse=True)
     k = np.sqrt(sum(c * c for c in kk))
-    weight = np.zeros(shape)
+    weight = np.zeros(k.shape)
     inside = (k >= kmin) & (k <= kmax)
     weight[inside] = k[inside] ** (power / 2.0)
     return weight, kk
@@ -35,17 +36,19 @@ def _shell_filter(shape, kmin, kmax, power):
 def _random_field(rng, shape, weight, kk, shifts):
     """A real Gaussian random field filtered by ``weight``, sampled at grid + ``shifts``.
 
-    ``shifts`` are offsets in cells along each axis (0 or 0.5).
+    ``shifts`` are offsets in cells along each axis (0 or 0.5), applied as phases.
     """
+    from scipy import fft
+
     noise = rng.standard_normal(shape)
-    spectrum = np.fft.fftn(noise) * weight
-    phase = 0.0
-    for k, shift, n in zip(kk, shifts, shape, strict=True):
-        if shift:
-            phase = phase + 2.0 * np.pi * k * shift / n
-    if np.any(np.asarray(shifts) != 0):
+    spectrum = fft.rfftn(noise, workers=-1) * weight
+    if any(shifts):
+        phase = 0.0
+        for k, shift, n in zip(kk, shifts, shape, strict=True):
+            if shift:
+                phase = phase + 2.0 * np.pi * k * shift / n
         spectrum = spectrum * np.exp(1j * phase)
-    return np.real(np.fft.ifftn(spectrum))
+    return fft.irfftn(spectrum, s=shape, workers=-1)
 
 
 def _periodic_edge(values, extra):
