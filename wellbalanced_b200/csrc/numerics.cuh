@@ -28,7 +28,34 @@ __device__ __forceinline__ R rmin(R a, R b) { return b < a ? b : a; }
 template <typename R>
 __device__ __forceinline__ R rmax(R a, R b) { return a < b ? b : a; }
 
-__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+// Arithmetic policy of the two precisions.
+//  float64 keeps every division and square root of the reference, in its order, so the
+//  float64 kernels agree with the reference to rounding (`div(a, b, inv_b)` is a / b and
+//  the precomputed reciprocal is dead code the compiler drops).
+//  float32 shares one approximate reciprocal (MUFU rcp, ~1 ulp) per denominator and takes
+//  square roots as x * rsqrt(x): ~14 special-function ops per HLLD face instead of ~40
+//  correctly rounded division / square-root sequences.
+template <typename R>
+struct Math;
+
+template <>
+struct Math<double> {
+  static __device__ __forceinline__ double inv(double b) { return 1.0 / b; }
+  static __device__ __forceinline__ double div(double a, double b, double) { return a / b; }
+  static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+  // 1 / sqrt(x) as the reference writes it: 1 / sqrt(x)
+  static __device__ __forceinline__ double over_sqrt(double a, double sq) { return a / sq; }
+};
+
+template <>
+struct Math<float> {
+  static __device__ __forceinline__ float inv(float b) { return __fdividef(1.0f, b); }
+  static __device__ __forceinline__ float div(float a, float, float inv_b) { return a * inv_b; }
+  static __device__ __forceinline__ float sqrt(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+  static __device__ __forceinline__ float over_sqrt(float a, float sq) { return a * __fdividef(1.0f, sq); }
+};
+
+__device__ __forceinline__ float rsqrt_(float x) { return Math<float>::sqrt(x); }
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 
 // Limited PLM slope of a cell from its backward (a) and forward (b) differences.
@@ -42,7 +69,7 @@ __device__ __forceinline__ R limited_slope(R a, R b) {
       slope = rabs(a) < rabs(b) ? a : b;
     } else if (LIM == 1) {
       const R product = a * b;
-      slope = R(2) * product / (a + b);
+      slope = Math<R>::div(R(2) * product, a + b, Math<R>::inv(a + b));
     } else {
       const R central = R(0.5) * (a + b);
       const R bound = R(2) * (rabs(a) < rabs(b) ? a : b);
@@ -67,11 +94,13 @@ __device__ __forceinline__ R limited_slope_rt(R a, R b, int limiter) {
 // Fast magnetosonic speed along the normal; the discriminant is clipped at zero.
 template <typename R>
 __device__ __forceinline__ R fast_speed(R rho, R p, R bn, R bt1, R bt2, R gamma) {
-  const R a2 = gamma * p / rho;
-  const R b2 = (bn * bn + bt1 * bt1 + bt2 * bt2) / rho;
-  const R disc = (a2 + b2) * (a2 + b2) - R(4) * a2 * bn * bn / rho;
-  const R root = disc > R(0) ? rsqrt_(disc) : R(0);
-  return rsqrt_(R(0.5) * (a2 + b2 + root));
+  using M = Math<R>;
+  const R inv_rho = M::inv(rho);
+  const R a2 = M::div(gamma * p, rho, inv_rho);
+  const R b2 = M::div(bn * bn + bt1 * bt1 + bt2 * bt2, rho, inv_rho);
+  const R disc = (a2 + b2) * (a2 + b2) - M::div(R(4) * a2 * bn * bn, rho, inv_rho);
+  const R root = disc > R(0) ? M::sqrt(disc) : R(0);
+  return M::sqrt(R(0.5) * (a2 + b2 + root));
 }
 
 // Conserved state U and physical flux F along the normal of a normal-frame primitive
@@ -104,18 +133,20 @@ __device__ __forceinline__ R side_state(const R (&w)[7], R bn, R inv_gm1, R (&u)
 template <typename R>
 __device__ __forceinline__ void star_tangential(const R (&w)[7], R bn, R s, R d, R pt, R sm,
                                                 R& rho_s, R& vt1, R& vt2, R& bt1, R& bt2) {
+  using M = Math<R>;
   const R vn = w[1];
-  rho_s = d / (s - sm);
+  rho_s = M::div(d, s - sm, M::inv(s - sm));
   const R den = d * (s - sm) - bn * bn;
   vt1 = w[2];
   vt2 = w[3];
   bt1 = w[5];
   bt2 = w[6];
   if (rabs(den) >= R(kDegenerate) * (pt + bn * bn)) {
-    vt1 = w[2] - bn * w[5] * (sm - vn) / den;
-    vt2 = w[3] - bn * w[6] * (sm - vn) / den;
-    bt1 = w[5] * (d * (s - vn) - bn * bn) / den;
-    bt2 = w[6] * (d * (s - vn) - bn * bn) / den;
+    const R inv_den = M::inv(den);
+    vt1 = w[2] - M::div(bn * w[5] * (sm - vn), den, inv_den);
+    vt2 = w[3] - M::div(bn * w[6] * (sm - vn), den, inv_den);
+    bt1 = M::div(w[5] * (d * (s - vn) - bn * bn), den, inv_den);
+    bt2 = M::div(w[6] * (d * (s - vn) - bn * bn), den, inv_den);
   }
 }
 
@@ -143,20 +174,23 @@ __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R b
   const R bn2 = bn * bn;
   const R ptl = L[4] + R(0.5) * (bn2 + L[5] * L[5] + L[6] * L[6]);
   const R ptr = Rt[4] + R(0.5) * (bn2 + Rt[5] * Rt[5] + Rt[6] * Rt[6]);
+  using M = Math<R>;
   const R dl = (sl - vl) * rl;
   const R dr = (sr - vr) * rr;
-  const R sm = (dr * vr - dl * vl - ptr + ptl) / (dr - dl);
-  const R pts = (dr * ptl - dl * ptr + dl * dr * (vr - vl)) / (dr - dl);
+  const R inv_dd = M::inv(dr - dl);
+  const R sm = M::div(dr * vr - dl * vl - ptr + ptl, dr - dl, inv_dd);
+  const R pts = M::div(dr * ptl - dl * ptr + dl * dr * (vr - vl), dr - dl, inv_dd);
   R rsl, vtl1, vtl2, btl1, btl2, rsr, vtr1, vtr2, btr1, btr2;
   star_tangential(L, bn, sl, dl, ptl, sm, rsl, vtl1, vtl2, btl1, btl2);
   star_tangential(Rt, bn, sr, dr, ptr, sm, rsr, vtr1, vtr2, btr1, btr2);
-  const R sql = rsqrt_(rsl);
-  const R sqr = rsqrt_(rsr);
+  const R sql = M::sqrt(rsl);
+  const R sqr = M::sqrt(rsr);
   const R sign = bn > R(0) ? R(1) : (bn < R(0) ? R(-1) : R(0));
-  const R vt2_1 = (sql * vtl1 + sqr * vtr1 + (btr1 - btl1) * sign) / (sql + sqr);
-  const R vt2_2 = (sql * vtl2 + sqr * vtr2 + (btr2 - btl2) * sign) / (sql + sqr);
-  const R bt2_1 = (sql * btr1 + sqr * btl1 + sql * sqr * (vtr1 - vtl1) * sign) / (sql + sqr);
-  const R bt2_2 = (sql * btr2 + sqr * btl2 + sql * sqr * (vtr2 - vtl2) * sign) / (sql + sqr);
+  const R inv_sum = M::inv(sql + sqr);
+  const R vt2_1 = M::div(sql * vtl1 + sqr * vtr1 + (btr1 - btl1) * sign, sql + sqr, inv_sum);
+  const R vt2_2 = M::div(sql * vtl2 + sqr * vtr2 + (btr2 - btl2) * sign, sql + sqr, inv_sum);
+  const R bt2_1 = M::div(sql * btr1 + sqr * btl1 + sql * sqr * (vtr1 - vtl1) * sign, sql + sqr, inv_sum);
+  const R bt2_2 = M::div(sql * btr2 + sqr * btl2 + sql * sqr * (vtr2 - vtl2) * sign, sql + sqr, inv_sum);
   const R vb2 = sm * bn + vt2_1 * bt2_1 + vt2_2 * bt2_2;
   // the side of the contact the face lies on
   const bool left = sm >= R(0);
@@ -171,14 +205,14 @@ __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R b
   const R bt1 = left ? btl1 : btr1;
   const R bt2 = left ? btl2 : btr2;
   const R sq = left ? sql : sqr;
-  const R ss = left ? sm - rabs(bn) / sql : sm + rabs(bn) / sqr;
+  const R ss = left ? sm - M::over_sqrt(rabs(bn), sql) : sm + M::over_sqrt(rabs(bn), sqr);
   const bool twice = left ? !(ss >= R(0)) : ss >= R(0);
   const R sense = left ? R(-1) : R(1);
   side_state(w, bn, inv_gm1, u, f);
   const R vn = w[1];
   const R vb = vn * bn + w[2] * w[5] + w[3] * w[6];
   const R vb_s = sm * bn + vt1 * bt1 + vt2 * bt2;
-  const R energy_s = ((s - vn) * u[4] - pt * vn + pts * sm + bn * (vb - vb_s)) / (s - sm);
+  const R energy_s = M::div((s - vn) * u[4] - pt * vn + pts * sm + bn * (vb - vb_s), s - sm, M::inv(s - sm));
   R us[7];
   us[0] = rho_s;
   us[1] = rho_s * sm;

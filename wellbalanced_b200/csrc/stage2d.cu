@@ -47,7 +47,9 @@ template <>
 __device__ __forceinline__ float recover_pressure<float>(float r, float m0, float m1, float m2, float e,
                                                          float bx, float by, float bz, float, float,
                                                          float, double gamma) {
-  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) / double(r);
+  double inv_r = double(__fdividef(1.0f, r));
+  inv_r = inv_r * (2.0 - double(r) * inv_r);
+  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) * inv_r;
   const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
   return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
 }
@@ -61,6 +63,7 @@ __device__ __forceinline__ bool bad_cell(S r, S u, S v, S w, S p, S bx, S by, S 
 
 template <typename S, int LIM>
 __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
+  using M = Math<S>;
   constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
   constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
   constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
@@ -78,6 +81,7 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
   const int64_t pitch = P.pitch0, fs = P.fstride;
   const S* __restrict__ src = a.src + P.off;
   const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+  const S idx = M::inv(dx), idy = M::inv(dy);
   const S b0x = S(a.b0[0]), b0y = S(a.b0[1]);
   const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
   const int x0 = tile.x0, y0 = tile.y0;
@@ -102,12 +106,13 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
       bz = src[5 * fs + c];
       const S* A = src + 6 * fs;
       const S a00 = A[c], a01 = A[c + 1], a10 = A[c + pitch], a11 = A[c + pitch + 1];
-      bxl = (a01 - a00) / dy + b0x;
-      bxh = (a11 - a10) / dy + b0x;
-      byl = -(a10 - a00) / dx + b0y;
-      byh = -(a11 - a01) / dx + b0y;
+      bxl = M::div(a01 - a00, dy, idy) + b0x;
+      bxh = M::div(a11 - a10, dy, idy) + b0x;
+      byl = -M::div(a10 - a00, dx, idx) + b0y;
+      byh = -M::div(a11 - a01, dx, idx) + b0y;
     }
-    const S u = m0 / r, v = m1 / r, w = m2 / r;
+    const S ir = M::inv(r);
+    const S u = M::div(m0, r, ir), v = M::div(m1, r, ir), w = M::div(m2, r, ir);
     const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh);
     S p = recover_pressure<S>(r, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
     if (!valid) p = S(1);
@@ -213,8 +218,8 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
       const int yrow[6] = {0, 2, 1, 3, 4, 6};
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const S div = (sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1]) / dx +
-                      (sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj]) / dy;
+        const S div = M::div(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1], dx, idx) +
+                      M::div(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj], dy, idy);
         S value = src[q * fs + cell] - dt * div;
         if (base_state) value = (value + base_state[q * fs + cell]) * S(0.5);
         dst[q * fs + cell] = value;

@@ -45,7 +45,10 @@ __device__ __forceinline__ double pressure3<double>(double r, double, double, do
 template <>
 __device__ __forceinline__ float pressure3<float>(float r, float m0, float m1, float m2, float e, float bx,
                                                   float by, float bz, float, float, float, double gamma) {
-  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) / double(r);
+  // 1 / rho: the float reciprocal refined by one Newton step in float64
+  double inv_r = double(__fdividef(1.0f, r));
+  inv_r = inv_r * (2.0 - double(r) * inv_r);
+  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) * inv_r;
   const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
   return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
 }
@@ -57,8 +60,15 @@ __device__ __forceinline__ bool bad3(S r, S u, S v, S w, S p, S bx, S by, S bz) 
            isfinite(by) && isfinite(bz));
 }
 
+// float32: two CTAs per SM (<= 113 registers a thread); float64: one (its shared memory).
+template <typename S>
+struct Occupancy3D {
+  static constexpr int kBlocks = sizeof(S) == 4 ? 2 : 1;
+};
+
 template <typename S, int LIM>
-__global__ void __launch_bounds__(288) stage3d_kernel(const StageArgs<S> a) {
+__global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(const StageArgs<S> a) {
+  using M = Math<S>;
   constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int RZ = TZ + 4, NR = (TY + 4) * (TZ + 4);  // plane region j, k in [-2, T+2)
   constexpr int GZ = TZ + 1, G = (TY + 1) * (TZ + 1);    // face / column grids
@@ -76,6 +86,7 @@ __global__ void __launch_bounds__(288) stage3d_kernel(const StageArgs<S> a) {
   const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
   const S* __restrict__ src = a.src + P.off;
   const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+  const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
   const S b0x = S(a.b0[0]), b0y = S(a.b0[1]), b0z = S(a.b0[2]);
   const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
   const int x0 = tile.x0, y0 = tile.y0, z0 = tile.z0;
@@ -146,16 +157,17 @@ __global__ void __launch_bounds__(288) stage3d_kernel(const StageArgs<S> a) {
           const S* Ay = src + 6 * fs;
           const S* Az = src + 7 * fs;
           // x-faces at nodes I and I+1: dA_z/dy - dA_y/dz + B0x
-          bxl = (Az[o + p1] - Az[o]) / dy - (Ay[o + 1] - Ay[o]) / dz + b0x;
-          bxh = (Az[o + p0 + p1] - Az[o + p0]) / dy - (Ay[o + p0 + 1] - Ay[o + p0]) / dz + b0x;
+          bxl = M::div(Az[o + p1] - Az[o], dy, idy) - M::div(Ay[o + 1] - Ay[o], dz, idz) + b0x;
+          bxh = M::div(Az[o + p0 + p1] - Az[o + p0], dy, idy) - M::div(Ay[o + p0 + 1] - Ay[o + p0], dz, idz) + b0x;
           // y-faces at nodes J and J+1: dA_x/dz - dA_z/dx + B0y
-          byl = (Ax[o + 1] - Ax[o]) / dz - (Az[o + p0] - Az[o]) / dx + b0y;
-          byh = (Ax[o + p1 + 1] - Ax[o + p1]) / dz - (Az[o + p1 + p0] - Az[o + p1]) / dx + b0y;
+          byl = M::div(Ax[o + 1] - Ax[o], dz, idz) - M::div(Az[o + p0] - Az[o], dx, idx) + b0y;
+          byh = M::div(Ax[o + p1 + 1] - Ax[o + p1], dz, idz) - M::div(Az[o + p1 + p0] - Az[o + p1], dx, idx) + b0y;
           // z-faces at nodes K and K+1: dA_y/dx - dA_x/dy + B0z
-          bzl = (Ay[o + p0] - Ay[o]) / dx - (Ax[o + p1] - Ax[o]) / dy + b0z;
-          bzh = (Ay[o + p0 + 1] - Ay[o + 1]) / dx - (Ax[o + p1 + 1] - Ax[o + 1]) / dy + b0z;
+          bzl = M::div(Ay[o + p0] - Ay[o], dx, idx) - M::div(Ax[o + p1] - Ax[o], dy, idy) + b0z;
+          bzh = M::div(Ay[o + p0 + 1] - Ay[o + 1], dx, idx) - M::div(Ax[o + p1 + 1] - Ax[o + 1], dy, idy) + b0z;
         }
-        const S u = m0 / rho, v = m1 / rho, w = m2 / rho;
+        const S irho = M::inv(rho);
+        const S u = M::div(m0, rho, irho), v = M::div(m1, rho, irho), w = M::div(m2, rho, irho);
         const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
         S pr = pressure3<S>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
         if (!valid) pr = S(1);
@@ -278,8 +290,9 @@ __global__ void __launch_bounds__(288) stage3d_kernel(const StageArgs<S> a) {
         const int zrow[5] = {0, 2, 3, 1, 4};  // z-sweep rows
 #pragma unroll
         for (int qf = 0; qf < 5; ++qf) {
-          const S div = (fnow[qf] - fprev[qf]) / dx + (Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)]) / dy +
-                        (Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)]) / dz;
+          const S div = M::div(fnow[qf] - fprev[qf], dx, idx) +
+                        M::div(Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)], dy, idy) +
+                        M::div(Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)], dz, idz);
           S value = src[qf * fs + o] - dt * div;
           if (base_state) value = (value + base_state[qf * fs + o]) * S(0.5);
           dst[qf * fs + o] = value;
