@@ -48,6 +48,7 @@ def parse():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-accuracy", action="store_true")
     parser.add_argument("--lx", type=int, default=32)
+    parser.add_argument("--no-plain", action="store_true")
     return parser.parse_args()
 
 
@@ -290,6 +291,11 @@ def main():
             "path": "MHD3D.load(pinned host pool) + MHD3D.advance(1) + MHD3D.save(pinned host pool)",
         }
 
+    # the plain float64 GPU step (the reference's dataflow, kernel by kernel) on the same box
+    plain = None
+    if rank == 0 and not args.no_plain:
+        plain = plain_step(n, rank, cells)
+
     # accuracy of the float32 step against the float64 device step from the same state
     accuracy = None
     if rank == 0 and not args.no_accuracy:
@@ -342,9 +348,38 @@ def main():
             line["e2e"] = e2e
         if accuracy is not None:
             line["accuracy"] = accuracy
+        if plain is not None:
+            line["plain_fp64"] = plain
+            line["plain_fp64"]["speedup_of_value"] = value / world / plain["value"]
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def plain_step(n, seed, cells, steps=3):
+    """zone-updates/s of the plain float64 GPU step (`wellbalanced_b200.plain.PlainMHD3D`)."""
+    import torch
+
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.plain import PlainMHD3D
+    from wellbalanced_b200.problems import turbulence_3d
+
+    rho, velocity, p, potential = turbulence_3d(n, seed=seed)
+    model = PlainMHD3D(AMRHierarchy((n,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3)
+    model.set_state(rho, velocity, p, vector_potential=potential)
+    model.step()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        model.step()
+    end.record()
+    torch.cuda.synchronize()
+    seconds = start.elapsed_time(end) / 1e3
+    del model
+    torch.cuda.empty_cache()
+    return {"value": cells * steps / seconds, "unit": UNIT, "ms_per_step": 1e3 * seconds / steps, "steps": steps,
+            "what": "PlainMHD3D: the reference MHD3D dataflow on the device, float64, per-kernel, intermediates in HBM"}
 
 
 def accuracy_check(n, seed, steps=10):

@@ -62,6 +62,13 @@ int wb_mhd_sweep(const double* prim, const double* bn, int axis, int limiter, do
 int wb_ct_contact(const double* fx_by, const double* gy_bx, const double* fx_rho, const double* gy_rho,
                   const double* ecc, int64_t X, int64_t Y, int64_t na, int64_t nb, double* ez, void* stream);
 
+/* The per-plane ct_contact calls of carafe/mhd3d.py:544-557 (MHD3D._edge_field) in one
+ * launch: `planes` stacked blocks, plane q of each array at q times its plane size
+ * (fx_* (planes, X-3, Y), gy_* (planes, X, Y-3), ecc (planes, X, Y), ez (planes, na, nb)). */
+int wb_ct_contact_planes(const double* fx_by, const double* gy_bx, const double* fx_rho, const double* gy_rho,
+                         const double* ecc, int64_t X, int64_t Y, int64_t na, int64_t nb, int64_t planes, double* ez,
+                         void* stream);
+
 /* carafe/kernels/mhd_rate/mhd_rate_pyccel.py:30-83 — mhd_rate(rho, mx, my, mz, energy, bz, az,
  * halo, dx, dy, b0x, b0y, gamma, out). out: device double[2] = (largest rate, smallest rho). */
 int wb_mhd_rate(const double* rho, const double* mx, const double* my, const double* mz,

@@ -249,3 +249,63 @@ def test_3d_negative_pressure_is_reported():
     model.engine.view(model.engine.state, patch, 4)[3, 3, 3] = -1.0
     with pytest.raises(FloatingPointError, match="pressure"):
         model.step(1e-3)
+
+
+# --- the plain float64 step (per-kernel, the reference's dataflow) -----------------------------
+def test_plain_2d_step_matches_the_reference_with_walls_gravity_resistivity(runs2d):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.plain import PlainMHD2D
+
+    model = PlainMHD2D(AMRHierarchy((32, 32), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True)))
+    b0 = 1.0 / np.sqrt(4.0 * np.pi)
+    model.set_state(
+        25.0 / (36.0 * np.pi),
+        lambda x, y: (-np.sin(2 * np.pi * y), np.sin(2 * np.pi * x), 0.0 * x),
+        5.0 / (12.0 * np.pi),
+        vector_potential=lambda x, y: b0 * (np.cos(4 * np.pi * x) / (4 * np.pi) + np.cos(2 * np.pi * y) / (2 * np.pi)),
+    )
+    dts = [model.step() for _ in range(5)]
+    np.testing.assert_allclose(dts, runs2d["ot32_5_dts"], rtol=1e-13)
+    close(model.state(), runs2d, "ot32_5", 1e-12)
+    # Rayleigh-Taylor: walls along y, gravity, a field along x (carafe/mhd.py:626-671)
+    rt = PlainMHD2D(
+        AMRHierarchy((8, 24), ((-0.25, 0.25), (-0.75, 0.75)), periodic=(True, False)),
+        gamma=1.4, mean_field=(0.05, 0.0), gravity=(0.0, -0.1), boundaries={"y": "wall"},
+    )
+
+    def density(x, y):
+        return np.where(y > 0.0, 2.0, 1.0)
+
+    rt.set_state(
+        density,
+        lambda x, y: (0.0 * x, 0.01 * (1 + np.cos(4 * np.pi * x)) * (1 + np.cos(3 * np.pi * y)) / 4.0, 0.0 * x),
+        lambda x, y: 2.5 - 0.1 * density(x, y) * y,
+    )
+    for _ in range(20):
+        rt.step()
+    close(rt.state(), runs2d, "rt8", 1e-12)
+    # resistive + Braginskii-conductive Orszag-Tang
+    model = PlainMHD2D(AMRHierarchy((16, 16), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True)),
+                       resistivity=1e-3, conduction=(1e-2, 1e-3))
+    model.set_state(
+        25.0 / (36.0 * np.pi),
+        lambda x, y: (-np.sin(2 * np.pi * y), np.sin(2 * np.pi * x), 0.0 * x),
+        5.0 / (12.0 * np.pi),
+        vector_potential=lambda x, y: b0 * (np.cos(4 * np.pi * x) / (4 * np.pi) + np.cos(2 * np.pi * y) / (2 * np.pi)),
+    )
+    for _ in range(3):
+        model.step()
+    close(model.state(), runs2d, "ot16_resistive", 1e-12)
+
+
+def test_plain_3d_step_matches_the_reference(runs3d):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.plain import PlainMHD3D
+    from wellbalanced_b200.problems import turbulence_3d
+
+    rho, velocity, p, potential = turbulence_3d(16, seed=7)
+    model = PlainMHD3D(AMRHierarchy((16,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3)
+    model.set_state(rho, velocity, p, vector_potential=potential)
+    dts = [model.step() for _ in range(4)]
+    np.testing.assert_allclose(dts, runs3d["turb16_dts"], rtol=1e-13)
+    close(model.state(), runs3d, "turb16", 1e-12)

@@ -26,6 +26,7 @@ SIGNATURES = {
     "wb_mhd_primitive": [c_dp] * 7 + [c_i64, c_i64] + [c_double] * 5 + [c_dp] * 5 + [c_dp],
     "wb_mhd_sweep": [c_dp, c_dp, c_int, c_int, c_double, c_i64, c_i64, c_dp, c_dp],
     "wb_ct_contact": [c_dp] * 5 + [c_i64] * 4 + [c_dp, c_dp],
+    "wb_ct_contact_planes": [c_dp] * 5 + [c_i64] * 5 + [c_dp, c_dp],
     "wb_mhd_rate": [c_dp] * 7 + [c_i64, c_i64, c_int] + [c_double] * 5 + [c_dp, c_dp],
     "wb_mhd_resistive": [c_dp] * 3 + [c_i64, c_i64] + [c_double] * 3 + [c_dp] * 3 + [c_dp],
     "wb_mhd_conductive": [c_dp] * 3 + [c_i64, c_i64] + [c_double] * 4 + [c_dp] * 2 + [c_dp],

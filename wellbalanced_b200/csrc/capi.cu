@@ -29,6 +29,8 @@ int launch_primitive_fp64(const double*, const double*, const double*, const dou
 int launch_sweep_fp64(const double*, const double*, int, int, double, int, int, double*, cudaStream_t);
 int launch_ct_fp64(const double*, const double*, const double*, const double*, const double*, int, int, int,
                    int, double*, cudaStream_t);
+int launch_ct_planes_fp64(const double*, const double*, const double*, const double*, const double*, int, int,
+                          int, int, int, double*, cudaStream_t);
 int launch_rate_fp64(const double*, const double*, const double*, const double*, const double*, const double*,
                      const double*, int, int, int, double, double, double, double, double, double*,
                      cudaStream_t);
@@ -115,6 +117,21 @@ int wb_ct_contact(const double* fx_by, const double* gy_bx, const double* fx_rho
     return kBadArgument;
   }
   return launch_ct_fp64(fx_by, gy_bx, fx_rho, gy_rho, ecc, int(X), int(Y), int(na), int(nb), ez, as_stream(stream));
+}
+
+int wb_ct_contact_planes(const double* fx_by, const double* gy_bx, const double* fx_rho, const double* gy_rho,
+                         const double* ecc, int64_t X, int64_t Y, int64_t na, int64_t nb, int64_t planes, double* ez,
+                         void* stream) {
+  set_error("");
+  if (!block_ok(X, Y, "ct_contact_planes") || !ptrs_ok({fx_by, gy_bx, fx_rho, gy_rho, ecc, ez}, "ct_contact_planes"))
+    return kBadArgument;
+  if (na < 0 || nb < 0 || na > X - 3 || nb > Y - 3 || planes < 0 || planes > 65535) {
+    set_error("ct_contact_planes: ez shape (%lld, %lld) x %lld planes out of range", (long long)na, (long long)nb,
+              (long long)planes);
+    return kBadArgument;
+  }
+  return launch_ct_planes_fp64(fx_by, gy_bx, fx_rho, gy_rho, ecc, int(X), int(Y), int(na), int(nb), int(planes), ez,
+                               as_stream(stream));
 }
 
 int wb_mhd_rate(const double* rho, const double* mx, const double* my, const double* mz, const double* energy,

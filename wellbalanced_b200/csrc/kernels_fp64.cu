@@ -116,6 +116,30 @@ __global__ void ct_fp64_kernel(const double* __restrict__ fx_by, const double* _
                   ecc[int64_t(i - 1) * Y + j], ecc[int64_t(i) * Y + j]);
 }
 
+// ct_contact over a stack of planes (the per-plane calls of carafe/mhd3d.py:544-557 in one
+// launch): plane q of every array starts at q times its plane size.
+__global__ void ct_fp64_planes_kernel(const double* __restrict__ fx_by, const double* __restrict__ gy_bx,
+                                      const double* __restrict__ fx_rho, const double* __restrict__ gy_rho,
+                                      const double* __restrict__ ecc, int X, int Y, int na, int nb,
+                                      double* __restrict__ ez) {
+  const int64_t q = blockIdx.y;
+  const int64_t fxs = int64_t(X - 3) * Y, gys = int64_t(X) * (Y - 3), es = int64_t(X) * Y, os = int64_t(na) * nb;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= os) return;
+  const int a = int(t / nb), b = int(t % nb);
+  const int i = a + 2, j = b + 2;
+  const int FY = Y - 3;
+  const double* fb = fx_by + q * fxs;
+  const double* fr = fx_rho + q * fxs;
+  const double* gb = gy_bx + q * gys;
+  const double* gr = gy_rho + q * gys;
+  const double* ec = ecc + q * es;
+  ez[q * os + t] = ct_node(fb[int64_t(i - 2) * Y + j - 1], fb[int64_t(i - 2) * Y + j], fr[int64_t(i - 2) * Y + j - 1],
+                           fr[int64_t(i - 2) * Y + j], gb[int64_t(i - 1) * FY + j - 2], gb[int64_t(i) * FY + j - 2],
+                           gr[int64_t(i - 1) * FY + j - 2], gr[int64_t(i) * FY + j - 2], ec[int64_t(i - 1) * Y + j - 1],
+                           ec[int64_t(i) * Y + j - 1], ec[int64_t(i - 1) * Y + j], ec[int64_t(i) * Y + j]);
+}
+
 // mhd_rate (mhd_rate_pyccel.py:30-83): max rate and min density over the block's own
 // cells, reduced with order-preserving integer keys (exact, order independent).
 __global__ void rate_fp64_kernel(const double* __restrict__ rho, const double* __restrict__ mx,
@@ -307,6 +331,16 @@ int launch_ct_fp64(const double* fx_by, const double* gy_bx, const double* fx_rh
   const int64_t n = int64_t(na) * nb;
   if (n > 0) ct_fp64_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(fx_by, gy_bx, fx_rho, gy_rho, ecc, X, Y, na, nb, ez);
   return check_launch("ct_contact");
+}
+
+int launch_ct_planes_fp64(const double* fx_by, const double* gy_bx, const double* fx_rho, const double* gy_rho,
+                          const double* ecc, int X, int Y, int na, int nb, int planes, double* ez,
+                          cudaStream_t stream) {
+  const int64_t n = int64_t(na) * nb;
+  if (n > 0 && planes > 0)
+    ct_fp64_planes_kernel<<<dim3(blocks_for(n, 256), planes), 256, 0, stream>>>(fx_by, gy_bx, fx_rho, gy_rho, ecc, X, Y,
+                                                                                na, nb, ez);
+  return check_launch("ct_contact_planes");
 }
 
 int launch_rate_fp64(const double* rho, const double* mx, const double* my, const double* mz,

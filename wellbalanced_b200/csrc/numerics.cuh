@@ -19,14 +19,16 @@ namespace wb {
 // Relative size below which the HLLD star denominator counts as zero (carafe/mhd.py:138).
 constexpr double kDegenerate = 1.0e-12;
 
-template <typename R>
-__device__ __forceinline__ R rabs(R x) { return x < R(0) ? -x : x; }
-
-template <typename R>
-__device__ __forceinline__ R rmin(R a, R b) { return b < a ? b : a; }
-
-template <typename R>
-__device__ __forceinline__ R rmax(R a, R b) { return a < b ? b : a; }
+// abs / min / max as single instructions (abs modifiers, FMNMX / DMNMX); the operands
+// here are never NaN in a valid state, where these agree with the reference's min / max.
+__device__ __forceinline__ float rabs(float x) { return fabsf(x); }
+__device__ __forceinline__ double rabs(double x) { return fabs(x); }
+__device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double rmin(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float rcopysign(float m, float s) { return copysignf(m, s); }
+__device__ __forceinline__ double rcopysign(double m, double s) { return copysign(m, s); }
 
 // Arithmetic policy of the two precisions.
 //  float64 keeps every division and square root of the reference, in its order, so the
@@ -59,25 +61,26 @@ __device__ __forceinline__ float rsqrt_(float x) { return Math<float>::sqrt(x); 
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 
 // Limited PLM slope of a cell from its backward (a) and forward (b) differences.
-// LIM: 0 minmod, 1 van Leer, 2 monotonized central, 3 none (central).
+// LIM: 0 minmod, 1 van Leer, 2 monotonized central, 3 none (central). Branch-free: where
+// a * b > 0 the slope is, for MC, sign(a) min(|a + b| / 2, 2 min(|a|, |b|)) — the
+// reference's central / bound / size selection (mhd_sweep_pyccel.py:25-48) when a and b
+// share a sign — and zero elsewhere.
 template <int LIM, typename R>
 __device__ __forceinline__ R limited_slope(R a, R b) {
   if (LIM == 3) return R(0.5) * (a + b);
-  R slope = R(0);
-  if (a * b > R(0)) {
-    if (LIM == 0) {
-      slope = rabs(a) < rabs(b) ? a : b;
-    } else if (LIM == 1) {
-      const R product = a * b;
-      slope = Math<R>::div(R(2) * product, a + b, Math<R>::inv(a + b));
-    } else {
-      const R central = R(0.5) * (a + b);
-      const R bound = R(2) * (rabs(a) < rabs(b) ? a : b);
-      const R size = rmin(rabs(central), rabs(bound));
-      slope = central > R(0) ? size : (central < R(0) ? -size : R(0));
-    }
+  const bool same = a * b > R(0);
+  R slope;
+  if (LIM == 0) {
+    slope = rabs(a) < rabs(b) ? a : b;
+  } else if (LIM == 1) {
+    const R product = a * b;
+    slope = Math<R>::div(R(2) * product, a + b, Math<R>::inv(a + b));
+  } else {
+    const R central = R(0.5) * (a + b);
+    const R bound = R(2) * rmin(rabs(a), rabs(b));
+    slope = rcopysign(rmin(rabs(central), bound), a);
   }
-  return slope;
+  return same ? slope : R(0);
 }
 
 // Runtime-limiter form (used by the per-kernel path, which takes the code as data).
@@ -141,40 +144,36 @@ __device__ __forceinline__ void star_tangential(const R (&w)[7], R bn, R s, R d,
   vt2 = w[3];
   bt1 = w[5];
   bt2 = w[6];
-  if (rabs(den) >= R(kDegenerate) * (pt + bn * bn)) {
-    const R inv_den = M::inv(den);
-    vt1 = w[2] - M::div(bn * w[5] * (sm - vn), den, inv_den);
-    vt2 = w[3] - M::div(bn * w[6] * (sm - vn), den, inv_den);
-    bt1 = M::div(w[5] * (d * (s - vn) - bn * bn), den, inv_den);
-    bt2 = M::div(w[6] * (d * (s - vn) - bn * bn), den, inv_den);
-  }
+  const bool regular = rabs(den) >= R(kDegenerate) * (pt + bn * bn);
+  const R inv_den = M::inv(den);
+  const R scale = d * (s - vn) - bn * bn;
+  const R v1 = w[2] - M::div(bn * w[5] * (sm - vn), den, inv_den);
+  const R v2 = w[3] - M::div(bn * w[6] * (sm - vn), den, inv_den);
+  const R b1 = M::div(w[5] * scale, den, inv_den);
+  const R b2 = M::div(w[6] * scale, den, inv_den);
+  vt1 = regular ? v1 : vt1;
+  vt2 = regular ? v2 : vt2;
+  bt1 = regular ? b1 : bt1;
+  bt2 = regular ? b2 : bt2;
 }
 
 // HLLD flux through a face between normal-frame states L and Rt with normal field bn.
+// Straight-line code: the star / double-star flux of the side of the contact the face
+// lies on is always formed and the supersonic and star-only cases are selected at the
+// end (no divergent branches). Where a face is supersonic (S_L >= 0 or S_R < 0) the
+// contact lies on the same side as the upwind state, so one side state serves both.
 template <typename R>
 __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R bn, R gamma,
                                           R inv_gm1, R (&F)[7]) {
+  using M = Math<R>;
   const R rl = L[0], vl = L[1], rr = Rt[0], vr = Rt[1];
   const R cf = rmax(fast_speed(rl, L[4], bn, L[5], L[6], gamma),
                     fast_speed(rr, Rt[4], bn, Rt[5], Rt[6], gamma));
   const R sl = rmin(vl, vr) - cf;
   const R sr = rmax(vl, vr) + cf;
-  R u[7], f[7];
-  if (sl >= R(0) || sr < R(0)) {
-    // supersonic: the physical flux of the upwind state
-    if (sl >= R(0)) {
-      side_state(L, bn, inv_gm1, u, f);
-    } else {
-      side_state(Rt, bn, inv_gm1, u, f);
-    }
-#pragma unroll
-    for (int c = 0; c < 7; ++c) F[c] = f[c];
-    return;
-  }
   const R bn2 = bn * bn;
   const R ptl = L[4] + R(0.5) * (bn2 + L[5] * L[5] + L[6] * L[6]);
   const R ptr = Rt[4] + R(0.5) * (bn2 + Rt[5] * Rt[5] + Rt[6] * Rt[6]);
-  using M = Math<R>;
   const R dl = (sl - vl) * rl;
   const R dr = (sr - vr) * rr;
   const R inv_dd = M::inv(dr - dl);
@@ -192,7 +191,7 @@ __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R b
   const R bt2_1 = M::div(sql * btr1 + sqr * btl1 + sql * sqr * (vtr1 - vtl1) * sign, sql + sqr, inv_sum);
   const R bt2_2 = M::div(sql * btr2 + sqr * btl2 + sql * sqr * (vtr2 - vtl2) * sign, sql + sqr, inv_sum);
   const R vb2 = sm * bn + vt2_1 * bt2_1 + vt2_2 * bt2_2;
-  // the side of the contact the face lies on
+  // the side of the contact the face lies on (also the upwind side when supersonic)
   const bool left = sm >= R(0);
   R w[7];
 #pragma unroll
@@ -207,13 +206,15 @@ __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R b
   const R sq = left ? sql : sqr;
   const R ss = left ? sm - M::over_sqrt(rabs(bn), sql) : sm + M::over_sqrt(rabs(bn), sqr);
   const bool twice = left ? !(ss >= R(0)) : ss >= R(0);
+  const bool supersonic = sl >= R(0) || sr < R(0);
   const R sense = left ? R(-1) : R(1);
+  R u[7], f[7];
   side_state(w, bn, inv_gm1, u, f);
   const R vn = w[1];
   const R vb = vn * bn + w[2] * w[5] + w[3] * w[6];
   const R vb_s = sm * bn + vt1 * bt1 + vt2 * bt2;
   const R energy_s = M::div((s - vn) * u[4] - pt * vn + pts * sm + bn * (vb - vb_s), s - sm, M::inv(s - sm));
-  R us[7];
+  R us[7], ud[7];
   us[0] = rho_s;
   us[1] = rho_s * sm;
   us[2] = rho_s * vt1;
@@ -221,19 +222,18 @@ __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R b
   us[4] = energy_s;
   us[5] = bt1;
   us[6] = bt2;
+  ud[0] = rho_s;
+  ud[1] = rho_s * sm;
+  ud[2] = rho_s * vt2_1;
+  ud[3] = rho_s * vt2_2;
+  ud[4] = energy_s + sense * sq * (vb_s - vb2) * sign;
+  ud[5] = bt2_1;
+  ud[6] = bt2_2;
 #pragma unroll
-  for (int c = 0; c < 7; ++c) F[c] = f[c] + s * (us[c] - u[c]);
-  if (twice) {
-    R ud[7];
-    ud[0] = rho_s;
-    ud[1] = rho_s * sm;
-    ud[2] = rho_s * vt2_1;
-    ud[3] = rho_s * vt2_2;
-    ud[4] = energy_s + sense * sq * (vb_s - vb2) * sign;
-    ud[5] = bt2_1;
-    ud[6] = bt2_2;
-#pragma unroll
-    for (int c = 0; c < 7; ++c) F[c] = F[c] + ss * (ud[c] - us[c]);
+  for (int c = 0; c < 7; ++c) {
+    const R star = f[c] + s * (us[c] - u[c]);
+    const R twice_star = star + ss * (ud[c] - us[c]);
+    F[c] = supersonic ? f[c] : (twice ? twice_star : star);
   }
 }
 
@@ -250,22 +250,19 @@ __device__ __forceinline__ void reconstruct(const R (&q0)[7], const R (&q1)[7], 
     L[c] = q1[c] + R(0.5) * s1;
     Rt[c] = q2[c] - R(0.5) * s2;
   }
-  if (L[0] <= R(0) || L[4] <= R(0) || Rt[0] <= R(0) || Rt[4] <= R(0)) {
+  const bool first_order = L[0] <= R(0) || L[4] <= R(0) || Rt[0] <= R(0) || Rt[4] <= R(0);
 #pragma unroll
-    for (int c = 0; c < 7; ++c) {
-      L[c] = q1[c];
-      Rt[c] = q2[c];
-    }
+  for (int c = 0; c < 7; ++c) {
+    L[c] = first_order ? q1[c] : L[c];
+    Rt[c] = first_order ? q2[c] : Rt[c];
   }
 }
 
 // CT-contact upwind pick (ct_contact_pyccel.py:17-24).
 template <typename R>
 __device__ __forceinline__ R upwind(R mass, R positive, R negative) {
-  R value = R(0.5) * (positive + negative);
-  if (mass > R(0)) value = positive;
-  if (mass < R(0)) value = negative;
-  return value;
+  const R mean = R(0.5) * (positive + negative);
+  return mass > R(0) ? positive : (mass < R(0) ? negative : mean);
 }
 
 // E at a node from its four faces and four cells (ct_contact_pyccel.py:36-61):

@@ -558,7 +558,33 @@ class Layout:
         return levels
 
     @staticmethod
-    def _pack(ops, dtype):
+    def _pack(ops, dtype, chunk=4096):
+        """Op array; ops larger than `chunk` points are split along their longest axis
+        (one CUDA block runs one op, so large halo slabs need many)."""
         if not ops:
             return np.zeros(0, dtype)
-        return np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
+        out = []
+        for o in ops:
+            o = np.asarray(o).reshape(())
+            n = [int(v) for v in o["n"]]
+            total = n[0] * n[1] * n[2]
+            if total <= chunk or dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
+                out.append(o)
+                continue
+            axis = int(np.argmax(n))
+            rows = max(1, chunk // max(1, total // n[axis]))
+            for start in range(0, n[axis], rows):
+                part = o.copy()
+                count = min(rows, n[axis] - start)
+                part["n"][axis] = count
+                if dtype == _lib.COPY_OP:
+                    part["d"][axis] += start
+                    part["s1"][axis] += part["m1"][axis] * start
+                    part["s2"][axis] += part["m2"][axis] * start
+                elif dtype == _lib.INTERP_OP:
+                    part["d"][axis] += start
+                else:  # restriction: coarse start c, fine start f (2 fine per coarse)
+                    part["c"][axis] += start
+                    part["f"][axis] += 2 * start
+                out.append(part)
+        return np.array(out, dtype=dtype)

@@ -87,7 +87,7 @@ class MHD2D:
             if kind == "wall" and mean_field[axis] != 0.0:
                 raise ValueError(f"a wall normal to {axis_name} needs a zero mean field along it")
             kinds[axis_name] = kind
-        if resistivity or max(conduction) > 0.0 or gravity[0] or gravity[1]:
+        if self._fused and (resistivity or max(conduction) > 0.0 or gravity[0] or gravity[1]):
             raise NotImplementedError(
                 "the fused device step covers ideal MHD; resistivity, conduction and gravity "
                 "run through wellbalanced_b200.plain.PlainMHD2D"
@@ -111,6 +111,9 @@ class MHD2D:
         self.steps = 0
         self.period = float("nan")
         self._ready = False
+
+    #: whether steps run the fused stage kernels (False: the per-kernel float64 path)
+    _fused = True
 
     def _build_engine(self):
         walls = tuple((w, w) for w in self.walls)

@@ -62,7 +62,7 @@ class MHD3D:
             raise ValueError("resistivity must be non-negative")
         if len(mean_field) != 3 or len(gravity) != 3:
             raise ValueError("mean_field and gravity have three components")
-        if resistivity or any(gravity):
+        if self._fused and (resistivity or any(gravity)):
             raise NotImplementedError("the fused 3D device step covers ideal MHD (no resistivity or gravity)")
         self.hierarchy = hierarchy
         self.gamma = float(gamma)
@@ -92,6 +92,9 @@ class MHD3D:
         self.steps = 0
         self.period = float("nan")
         self._ready = False
+
+    #: whether steps run the fused stage kernel (False: the per-kernel float64 path)
+    _fused = True
 
     # test problems (carafe/mhd3d.py:236-346) -----------------------------------------------------
     @classmethod
