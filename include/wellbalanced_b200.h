@@ -120,15 +120,21 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
                    double gamma, const double* inv_dx2_sum, double* time, const double* end, double* dt,
                    int advance, void* stream);
 
-/* Halo / restriction / refluxing op lists (struct CopyOp / InterpOp / RestrictOp /
- * RegisterOp / RefluxOp), replacing patchwork's exchange_halos, restrict and
- * FluxRegister (carafe/mhd.py:744-777, 906-919, 981, 989-991). */
+/* Halo and restriction op lists (struct CopyOp / InterpOp / RestrictOp), replacing
+ * patchwork's exchange_halos and restrict (carafe/mhd.py:744-777, 981, 991). */
 int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_interp_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
-int wb_register_ops(const double* bflux, const void* ops, int nops, double* reg, double scale, void* stream);
-int wb_reflux_ops(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
-                  void* stream);
+
+/* Refluxing, replacing patchwork's FluxRegister (carafe/mhd.py:906-919, 989-990): after
+ * a stage, reg += (mean of the fine faces - the coarse face) of every coarse-fine
+ * interface face, recomputed from the stage's input pool (struct FaceFluxOp); after the
+ * step, the coarse cells beside the interfaces take U -= sign * 0.5 dt * reg / dx and reg
+ * is cleared (struct RefluxOp; dt per instance on the device). */
+int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
+                     double b0y, double b0z, double gamma, int limiter, double* reg, void* stream);
+int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
+                    const double* dt, void* stream);
 
 /* Sizes of the engine structs, for callers that mirror them. */
 int wb_struct_sizes(int64_t* sizes_host, int n);

@@ -277,14 +277,25 @@ class Hierarchy:
                     self._restrict_pair(name, extra, fine, coarse)
 
     def _restrict_pair(self, name, extra, fine, coarse):
+        """Restrict ``fine`` into ``coarse``, periodic images included (a fine node plane
+        on the domain's upper face is also the coarse node plane 0)."""
+        shifts = []
+        for a in range(self.ndim):
+            n_fine = self.level_shape(fine.level)[a]
+            shifts.append((0, -n_fine, n_fine) if self.periodic[a] and extra[a] else (0,))
+        for shift in itertools.product(*shifts):
+            self._restrict_shifted(name, extra, fine, coarse, shift)
+
+    def _restrict_shifted(self, name, extra, fine, coarse, shift):
         source = fine.field(name).local
         target = coarse.field(name).local
         coarse_index, fine_parts = [], []
         for a in range(self.ndim):
-            (flo, fhi), (clo, chi) = fine.box[a], coarse.box[a]
+            flo, fhi = fine.box[a][0] + shift[a], fine.box[a][1] + shift[a]
+            clo, chi = coarse.box[a]
             e = extra[a]
             lo = max(flo // 2, clo)
-            hi = min(fhi // 2, chi) + e
+            hi = min(fhi // 2 + e, chi + e)
             if lo >= hi:
                 return
             coarse_index.append(slice(lo - clo, hi - clo))

@@ -43,7 +43,7 @@ def test_struct_layouts_match_the_library():
     lib = _lib.load()
     sizes = np.zeros(7, dtype=np.int64)
     assert lib.wb_struct_sizes(sizes.ctypes.data, 7) == 0
-    assert list(sizes) == [88, 16, 112, 72, 60, 96, 96]
+    assert list(sizes) == [88, 16, 112, 72, 60, 72, 96]
 
 
 def test_bad_arguments_are_reported_without_a_device():

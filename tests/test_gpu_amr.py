@@ -1,0 +1,146 @@
+"""Refined patches on the device: halos from coarser levels, restriction, refluxing (GPU).
+
+The device float64 step on hierarchies with refined patches against the oracle's AMR
+step (the same semantics, restated on the CPU: `oracle.mesh`), patch by patch, and the
+reference's own properties of refined runs (``tests/unit/test_mhd.py:164-211``,
+``tests/unit/test_mhd3d.py:72-80``): conserved totals to round-off, div B and the
+composite divergence at round-off, the refined solution close to the uniform one.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def _refined_state():
+    return dict(
+        density=lambda x, y: 1.0 + 0.5 * np.exp(-((x + 0.3) ** 2 + y**2) / 0.02),
+        velocity=(2.0, 1.0, 0.3),
+        pressure=lambda x, y: 1.0 + 0.2 * np.cos(np.pi * x),
+        vector_potential=lambda x, y: 0.1 * np.maximum(0.3 - np.hypot(x, y), 0.0),
+        bz=lambda x, y: 0.1 * np.sin(np.pi * x),
+    )
+
+
+def _pair(cells=16, precision=64):
+    from oracle.mesh import Hierarchy
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    box = ((cells - cells // 2, cells + cells // 2), (cells // 2, 3 * cells // 2))
+    oh = Hierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), (True, True))
+    oh.add_patch(1, box)
+    dh = AMRHierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True))
+    dh.add_patch(1, box)
+    oracle = OracleMHD2D(oh, limiter="minmod")
+    device = MHD2D(dh, limiter="minmod", precision=precision)
+    state = _refined_state()
+    oracle.set_state(state["density"], state["velocity"], state["pressure"],
+                     vector_potential=state["vector_potential"], bz=state["bz"])
+    device.set_state(state["density"], state["velocity"], state["pressure"],
+                     vector_potential=state["vector_potential"], bz=state["bz"])
+    return oracle, device
+
+
+def test_refined_2d_matches_the_oracle_patch_by_patch():
+    oracle, device = _pair()
+    for _ in range(12):
+        dt = oracle.step()
+        device.step(dt)
+    for op, dp in zip(oracle.hierarchy.patches, device.hierarchy.patches, strict=True):
+        for f, name in enumerate(oracle.names.values()):
+            np.testing.assert_allclose(device.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                       err_msg=f"level {op.level} {name}")
+        np.testing.assert_allclose(device.gather(dp, 6, node=True), op.field(oracle.potential).local,
+                                   rtol=1e-11, atol=1e-12)
+
+
+def test_refined_2d_conserves_and_keeps_div_b_zero():
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    _, model = _pair()
+    before = model.totals()
+    model.run(0.2)
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-12
+    assert model.divergence() < 1e-14
+    assert model.composite_divergence() < 1e-14
+    # close to the uniform solution (test_mhd.py:193-211)
+    _, refined = _pair()
+    refined.run(0.1)
+    uniform = MHD2D(AMRHierarchy((32, 16), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True)), limiter="minmod",
+                    precision=64)
+    s = _refined_state()
+    uniform.set_state(s["density"], s["velocity"], s["pressure"], vector_potential=s["vector_potential"], bz=s["bz"])
+    uniform.run(0.1)
+    difference = refined.dataset().density.values - uniform.dataset().density.values
+    assert float(np.abs(difference).max()) < 0.05
+
+
+def test_refined_2d_float32_drift_is_at_float32_round_off():
+    _, model = _pair(precision=32)
+    before = model.totals()
+    for _ in range(50):
+        model.step()
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-5 * max(1.0, abs(before[name])), name
+    assert model.divergence() < 1e-12
+    assert model.composite_divergence() < 1e-6
+
+
+def _alfven_pair(precision=64):
+    from oracle.mesh import Hierarchy
+    from oracle.mhd3d import MHD3D as OracleMHD3D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    wavevector = 2 * np.pi * np.array([0.5, 1.0, 1.0])
+    k = np.linalg.norm(wavevector)
+    n = wavevector / k
+    e1 = np.cross(n, [0.0, 0.0, 1.0])
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(n, e1)
+
+    def perpendicular(x, y, z):
+        phase = wavevector[0] * x + wavevector[1] * y + wavevector[2] * z
+        return [0.1 * (np.sin(phase) * e1[i] + np.cos(phase) * e2[i]) for i in range(3)]
+
+    def potential(i):
+        return lambda x, y, z: perpendicular(x, y, z)[i] / k
+
+    bounds = ((0.0, 2.0), (0.0, 1.0), (0.0, 1.0))
+    oh = Hierarchy((16, 8, 8), bounds, (True,) * 3)
+    oh.add_patch(1, ((8, 20), (4, 12), (2, 10)))
+    dh = AMRHierarchy((16, 8, 8), bounds, periodic=(True,) * 3)
+    dh.add_patch(1, ((8, 20), (4, 12), (2, 10)))
+    models = (OracleMHD3D(oh, mean_field=tuple(n)), MHD3D(dh, mean_field=tuple(n), precision=precision))
+    for m in models:
+        m.set_state(1.0, lambda x, y, z: [-b for b in perpendicular(x, y, z)], 0.1,
+                    vector_potential=(potential(0), potential(1), potential(2)))
+    return models
+
+
+def test_refined_3d_matches_the_oracle_and_conserves():
+    oracle, device = _alfven_pair()
+    before = device.totals()
+    for _ in range(6):
+        dt = oracle.step()
+        device.step(dt)
+    for op, dp in zip(oracle.hierarchy.patches, device.hierarchy.patches, strict=True):
+        names = [*oracle.names.values(), *oracle.potential]
+        for f, name in enumerate(names):
+            np.testing.assert_allclose(device.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                       err_msg=f"level {op.level} {name}")
+    after = device.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-14 * max(1.0, abs(before[name])) * 100
+    assert device.divergence() < 1e-14

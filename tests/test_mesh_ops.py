@@ -126,3 +126,34 @@ def test_tiles_cover_every_computed_node_once():
         assert np.all(count == 1)
     # the non-periodic x boundary is computed by its patch, the shared plane is not
     assert layout.own[0] == (False, False) and layout.own[1] == (True, False)
+
+
+@pytest.mark.parametrize("case", [6, 7, 8])
+def test_2d_restriction_ops_match_the_oracle(case):
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+
+    shape, bounds, periodic, split, fine, boundaries = CASES_2D[case]
+    oracle_h = Hierarchy(shape, bounds, periodic, split)
+    device_h = AMRHierarchy(shape, bounds, periodic, split=split)
+    for level, box in fine:
+        oracle_h.add_patch(level, box)
+        device_h.add_patch(level, box)
+    model = OracleMHD2D(oracle_h, boundaries=boundaries)
+    layout = Layout(device_h, precision=64)
+    pool = np.zeros(layout.pool_size)
+    extras = [(0, 0)] * 6 + [(1, 1)]
+    rng = np.random.default_rng(20 + case)
+    names = _fill_oracle_and_pool(model, layout, pool, rng, 7, extras)
+    for name in names:
+        oracle_h.restrict(name)
+    for level in range(layout.h.max_level, 0, -1):
+        for g in layout.groups:
+            _emulate.apply_restrict(pool, layout.rows, layout.restrict_levels[level][g])
+    # compare the computed points (the oracle also writes duplicate nodes the device fills)
+    for patch in oracle_h.patches:
+        dev = layout.h.patches[oracle_h.patches.index(patch)]
+        for f, name in enumerate(names):
+            expect = patch.field(name).local
+            got = layout.patch_view(pool, dev, f)[tuple(slice(2, 2 + s) for s in expect.shape)]
+            own = [s - (0 if (f < 6 or layout.own[dev.index][a]) else 1) for a, s in enumerate(expect.shape)]
+            np.testing.assert_allclose(got[: own[0], : own[1]], expect[: own[0], : own[1]], atol=1e-14)

@@ -41,8 +41,8 @@ SIGNATURES = {
     "wb_copy_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_interp_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
-    "wb_register_ops": [c_dp, c_dp, c_int, c_dp, c_double, c_dp],
-    "wb_reflux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp],
+    "wb_face_flux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp, c_dp],
+    "wb_reflux_apply": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],
     "wb_struct_sizes": [c_dp, c_int],
 }
 
@@ -75,7 +75,7 @@ def load():
     status = lib.wb_struct_sizes(sizes.ctypes.data, 7)
     if status != 0:
         raise WBError(lib.wb_last_error().decode())
-    expected = [d.itemsize for d in (PATCH, TILE, COPY_OP, INTERP_OP, RESTRICT_OP, REGISTER_OP, REFLUX_OP)]
+    expected = [d.itemsize for d in (PATCH, TILE, COPY_OP, INTERP_OP, RESTRICT_OP, FACE_FLUX_OP, REFLUX_OP)]
     if list(sizes) != expected:
         raise RuntimeError(f"struct layout mismatch between host and library: {list(sizes)} != {expected}")
     _lib = lib
@@ -129,13 +129,13 @@ RESTRICT_OP = np.dtype(
         "itemsize": 60,
     }
 )
-REGISTER_OP = np.dtype(
+FACE_FLUX_OP = np.dtype(
     {
-        "names": ["coarse_off", "fine_off", "coarse_stride", "fine_stride", "coarse_start", "fine_start",
-                  "coarse_row", "fine_row", "reg_off", "len", "width", "ncomp", "fine_a", "fine_b"],
-        "formats": ["<i8"] * 9 + ["<i4"] * 5,
-        "offsets": [0, 8, 16, 24, 32, 40, 48, 56, 64, 72, 76, 80, 84, 88],
-        "itemsize": 96,
+        "names": ["coarse", "fine", "ndim", "axis", "t1", "t2", "coarse_plane", "fine_plane", "coarse_t0", "fine_t0",
+                  "len", "width", "pad0", "pad1", "reg_off"],
+        "formats": ["<i4"] * 8 + [("<i4", 2)] * 2 + ["<i4"] * 4 + ["<i8"],
+        "offsets": [0, 4, 8, 12, 16, 20, 24, 28, 32, 40, 48, 52, 56, 60, 64],
+        "itemsize": 72,
     }
 )
 REFLUX_OP = np.dtype(

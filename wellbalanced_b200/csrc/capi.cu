@@ -286,22 +286,35 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
                                      static_cast<const RestrictOp*>(ops), nops, as_stream(stream));
 }
 
-int wb_register_ops(const double* bflux, const void* ops, int nops, double* reg, double scale, void* stream) {
+int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
+                     double b0y, double b0z, double gamma, int limiter, double* reg, void* stream) {
   set_error("");
-  if (nops > 0 && !ptrs_ok({bflux, ops, reg}, "register_ops")) return kBadArgument;
-  return launch_register_ops(bflux, static_cast<const RegisterOp*>(ops), nops, reg, scale, as_stream(stream));
+  if (!precision_ok(precision, "face_flux_ops") || (nops > 0 && !ptrs_ok({pool, patches, ops, reg}, "face_flux_ops")))
+    return kBadArgument;
+  if (limiter < 0 || limiter > 3) {
+    set_error("face_flux_ops: limiter code %d is not one of 0..3", limiter);
+    return kBadArgument;
+  }
+  const double b0[3] = {b0x, b0y, b0z};
+  if (precision == 32)
+    return launch_face_flux_ops<float>(static_cast<const float*>(pool), static_cast<const PatchDesc*>(patches),
+                                       static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, reg,
+                                       as_stream(stream));
+  return launch_face_flux_ops<double>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
+                                      static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, reg,
+                                      as_stream(stream));
 }
 
-int wb_reflux_ops(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
-                  void* stream) {
+int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
+                    const double* dt, void* stream) {
   set_error("");
-  if (!precision_ok(precision, "reflux_ops") || (nops > 0 && !ptrs_ok({pool, patches, ops, reg}, "reflux_ops")))
+  if (!precision_ok(precision, "reflux_apply") || (nops > 0 && !ptrs_ok({pool, patches, ops, reg, dt}, "reflux_apply")))
     return kBadArgument;
   if (precision == 32)
-    return launch_reflux_ops<float>(static_cast<float*>(pool), static_cast<const PatchDesc*>(patches),
-                                    static_cast<const RefluxOp*>(ops), nops, reg, as_stream(stream));
-  return launch_reflux_ops<double>(static_cast<double*>(pool), static_cast<const PatchDesc*>(patches),
-                                   static_cast<const RefluxOp*>(ops), nops, reg, as_stream(stream));
+    return launch_reflux_apply<float>(static_cast<float*>(pool), static_cast<const PatchDesc*>(patches),
+                                      static_cast<const RefluxOp*>(ops), nops, reg, dt, as_stream(stream));
+  return launch_reflux_apply<double>(static_cast<double*>(pool), static_cast<const PatchDesc*>(patches),
+                                     static_cast<const RefluxOp*>(ops), nops, reg, dt, as_stream(stream));
 }
 
 int wb_struct_sizes(int64_t* sizes_host, int n) {
@@ -315,7 +328,7 @@ int wb_struct_sizes(int64_t* sizes_host, int n) {
   sizes_host[2] = sizeof(CopyOp);
   sizes_host[3] = sizeof(InterpOp);
   sizes_host[4] = sizeof(RestrictOp);
-  sizes_host[5] = sizeof(RegisterOp);
+  sizes_host[5] = sizeof(FaceFluxOp);
   sizes_host[6] = sizeof(RefluxOp);
   return kOk;
 }

@@ -11,7 +11,6 @@
 //   cell-centred axes, coincident-or-4-point-midpoint along node axes.
 // * Restriction ops set coarse values under fine patches: the mean of the fine values
 //   along cell-centred axes, the coincident fine value along node axes.
-// * Reflux ops correct coarse cells beside fine patches with the float64 flux register.
 #include "layout.cuh"
 #include "halo.cuh"
 #include "wb_internal.cuh"
@@ -149,49 +148,6 @@ __global__ void __launch_bounds__(256) restrict_ops_kernel(S* __restrict__ pool,
   }
 }
 
-// Accumulate scale * (fine mean - coarse) boundary fluxes of an interface into the
-// register (float64): reg[r + q * len + t] += scale * (mean of fine faces - coarse face).
-__global__ void register_ops_kernel(const double* __restrict__ bflux, const RegisterOp* __restrict__ ops,
-                                    double* __restrict__ reg, double scale) {
-  const RegisterOp op = ops[blockIdx.x];
-  const int64_t count = int64_t(op.len) * op.ncomp;
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int q = int(t / op.len), s = int(t % op.len);
-    const int s1 = s / op.width, s2 = s % op.width;  // coarse face position (two transverse axes)
-    const double coarse = bflux[op.coarse_off + int64_t(q) * op.coarse_stride + op.coarse_start +
-                                int64_t(s1) * op.coarse_row + s2];
-    double fine = 0.0;
-    for (int a = 0; a < op.fine_a; ++a)
-      for (int b = 0; b < op.fine_b; ++b)
-        fine += bflux[op.fine_off + int64_t(q) * op.fine_stride + op.fine_start +
-                      int64_t(op.fine_a * s1 + a) * op.fine_row + (op.fine_b * s2 + b)];
-    fine /= double(op.fine_a * op.fine_b);
-    reg[op.reg_off + int64_t(q) * op.len + s] += scale * (fine - coarse);
-  }
-}
-
-// Apply the register to the coarse cells outside the fine patch and clear it:
-// U -= sign * reg / dx (sign +1 where the interface is the cell's upper face).
-template <typename S>
-__global__ void reflux_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                  const RefluxOp* __restrict__ ops, double* __restrict__ reg) {
-  const RefluxOp op = ops[blockIdx.x];
-  const PatchDesc C = patches[op.coarse];
-  const int64_t count = int64_t(op.len) * op.ncomp;
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int q = int(t / op.len), s = int(t % op.len);
-    const int s1 = s / op.width, s2 = s % op.width;
-    int idx[3] = {op.c[0], op.c[1], op.c[2]};
-    idx[op.t1] += s1;
-    if (op.t2 >= 0) idx[op.t2] += s2;
-    const int64_t o = offset_of(C, idx[0], idx[1], idx[2]);
-    const double r = reg[op.reg_off + int64_t(q) * op.len + s];
-    S* u = pool + C.off + int64_t(op.field[q]) * C.fstride + o;
-    *u = S(double(*u) - op.sign * r / op.dx);
-    reg[op.reg_off + int64_t(q) * op.len + s] = 0.0;
-  }
-}
-
 template <typename S>
 int launch_copy_ops(S* pool, const PatchDesc* patches, const CopyOp* ops, int nops, cudaStream_t stream) {
   if (nops > 0) copy_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops);
@@ -207,25 +163,11 @@ int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops
   if (nops > 0) restrict_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops);
   return check_launch("restrict");
 }
-int launch_register_ops(const double* bflux, const RegisterOp* ops, int nops, double* reg, double scale,
-                        cudaStream_t stream) {
-  if (nops > 0) register_ops_kernel<<<nops, 256, 0, stream>>>(bflux, ops, reg, scale);
-  return check_launch("flux register");
-}
-template <typename S>
-int launch_reflux_ops(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
-                      cudaStream_t stream) {
-  if (nops > 0) reflux_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops, reg);
-  return check_launch("reflux");
-}
-
 template int launch_copy_ops<float>(float*, const PatchDesc*, const CopyOp*, int, cudaStream_t);
 template int launch_copy_ops<double>(double*, const PatchDesc*, const CopyOp*, int, cudaStream_t);
 template int launch_interp_ops<float>(float*, const PatchDesc*, const InterpOp*, int, cudaStream_t);
 template int launch_interp_ops<double>(double*, const PatchDesc*, const InterpOp*, int, cudaStream_t);
 template int launch_restrict_ops<float>(float*, const PatchDesc*, const RestrictOp*, int, cudaStream_t);
 template int launch_restrict_ops<double>(double*, const PatchDesc*, const RestrictOp*, int, cudaStream_t);
-template int launch_reflux_ops<float>(float*, const PatchDesc*, const RefluxOp*, int, double*, cudaStream_t);
-template int launch_reflux_ops<double>(double*, const PatchDesc*, const RefluxOp*, int, double*, cudaStream_t);
 
 }  // namespace wb

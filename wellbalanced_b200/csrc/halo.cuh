@@ -43,16 +43,17 @@ struct RestrictOp {
   int32_t f[3];
 };
 
-// One coarse-fine interface side: faces of a coarse patch's boundary-flux record and
-// the fine faces over them, accumulated into the register.
-struct RegisterOp {
-  int64_t coarse_off, fine_off;  // offsets of the two patches' boundary-flux blocks
-  int64_t coarse_stride, fine_stride;  // elements between components
-  int64_t coarse_start, fine_start;    // first face of the interface within the side
-  int64_t coarse_row, fine_row;        // elements between rows of the second transverse axis
+// One coarse-fine interface side: the coarse faces (haloed index coarse_plane along
+// `axis` of the coarse patch, transverse start coarse_t0) and the fine faces over them
+// (2 per coarse face along each transverse axis), accumulated into reg[reg_off ...].
+struct FaceFluxOp {
+  int32_t coarse, fine;
+  int32_t ndim, axis, t1, t2;
+  int32_t coarse_plane, fine_plane;
+  int32_t coarse_t0[2], fine_t0[2];
+  int32_t len, width;
+  int32_t pad0, pad1;
   int64_t reg_off;
-  int32_t len, width, ncomp;           // faces (len = rows * width), components
-  int32_t fine_a, fine_b;              // fine faces per coarse face along each transverse axis
 };
 
 // Apply the register of one interface to the coarse cells beside it.
@@ -72,10 +73,11 @@ template <typename S>
 int launch_interp_ops(S* pool, const PatchDesc* patches, const InterpOp* ops, int nops, cudaStream_t stream);
 template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream);
-int launch_register_ops(const double* bflux, const RegisterOp* ops, int nops, double* reg, double scale,
-                        cudaStream_t stream);
 template <typename S>
-int launch_reflux_ops(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
-                      cudaStream_t stream);
+int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
+                         double gamma, int limiter, double* reg, cudaStream_t stream);
+template <typename S>
+int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
+                        const double* dt, cudaStream_t stream);
 
 }  // namespace wb

@@ -281,4 +281,30 @@ __device__ __forceinline__ R ct_node(R fb_lo, R fb_hi, R m_lo, R m_hi, R gb_lo, 
   return R(0.25) * (gb_hi + gb_lo - fb_hi - fb_lo + dl1 + dr1 + dl2 + dr2);
 }
 
+// Pressure recovery p = (gamma - 1)(E - rho u^2 / 2 - B^2 / 2) of a cell.
+template <typename S>
+__device__ __forceinline__ S recover_pressure(S r, S m0, S m1, S m2, S e, S bx, S by, S bz, S u, S v,
+                                              S w, double gamma);
+
+// float64: the reference's expression (mhd_primitive_pyccel.py:60-64)
+template <>
+__device__ __forceinline__ double recover_pressure<double>(double r, double, double, double, double e,
+                                                           double bx, double by, double bz, double u,
+                                                           double v, double w, double gamma) {
+  return (gamma - 1.0) * (e - 0.5 * r * (u * u + v * v + w * w) - 0.5 * (bx * bx + by * by + bz * bz));
+}
+
+// float32 state: the same difference evaluated in float64 from the stored values, so
+// the cancellation of low-beta cells costs no extra rounding.
+template <>
+__device__ __forceinline__ float recover_pressure<float>(float r, float m0, float m1, float m2, float e,
+                                                         float bx, float by, float bz, float, float,
+                                                         float, double gamma) {
+  double inv_r = double(__fdividef(1.0f, r));
+  inv_r = inv_r * (2.0 - double(r) * inv_r);
+  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) * inv_r;
+  const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
+  return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
+}
+
 }  // namespace wb

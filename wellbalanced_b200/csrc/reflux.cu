@@ -1,0 +1,215 @@
+// Refluxing on the device (Berger–Colella; patchwork's FluxRegister, whose semantics
+// tests/unit/test_fluid2d_patches.py:162-240 of the reference pins): after each RK stage
+// the fluxes through every coarse-fine interface face are recomputed from the stage's
+// input state — the coarse face and the mean of the fine faces over it, with the same
+// reconstruction and HLLD as the stage kernels — and their difference is accumulated in
+// a float64 register; after the Heun combine the coarse cells outside the fine patches
+// take the register's correction (carafe/mhd.py:906-919, 989-990).
+#include "halo.cuh"
+#include "layout.cuh"
+#include "numerics.cuh"
+#include "wb_internal.cuh"
+
+namespace wb {
+
+__device__ __forceinline__ int64_t cell_offset(const PatchDesc& P, int i, int j, int k) {
+  if (P.pitch1) return int64_t(i) * P.pitch0 + int64_t(j) * P.pitch1 + k;
+  return int64_t(i) * P.pitch0 + j;
+}
+
+// Primitive variables (rho, u, v, w, p, bx, by, bz) of haloed cell (i, j, k) and the
+// field at its lower face along `axis`, with the arithmetic of the stage kernels.
+template <typename S>
+__device__ void cell_primitive(const S* src, const PatchDesc& P, int ndim, int i, int j, int k, int axis,
+                               const double* b0, double gamma, S (&q)[8], S& bn_lower) {
+  using M = Math<S>;
+  const int64_t fs = P.fstride;
+  const int64_t o = cell_offset(P, i, j, k);
+  const S r = src[o], m0 = src[fs + o], m1 = src[2 * fs + o], m2 = src[3 * fs + o], e = src[4 * fs + o];
+  S bx, by, bz;
+  if (ndim == 2) {
+    const S* A = src + 6 * fs;
+    const int64_t p0 = P.pitch0;
+    const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+    const S idx = M::inv(dx), idy = M::inv(dy);
+    const S bxl = M::div(A[o + 1] - A[o], dy, idy) + S(b0[0]);
+    const S bxh = M::div(A[o + p0 + 1] - A[o + p0], dy, idy) + S(b0[0]);
+    const S byl = -M::div(A[o + p0] - A[o], dx, idx) + S(b0[1]);
+    const S byh = -M::div(A[o + p0 + 1] - A[o + 1], dx, idx) + S(b0[1]);
+    bx = S(0.5) * (bxl + bxh);
+    by = S(0.5) * (byl + byh);
+    bz = src[5 * fs + o];
+    bn_lower = axis == 0 ? bxl : byl;
+  } else {
+    const S* Ax = src + 5 * fs;
+    const S* Ay = src + 6 * fs;
+    const S* Az = src + 7 * fs;
+    const int64_t p0 = P.pitch0, p1 = P.pitch1;
+    const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+    const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
+    auto fx = [&](int64_t c) { return M::div(Az[c + p1] - Az[c], dy, idy) - M::div(Ay[c + 1] - Ay[c], dz, idz) + S(b0[0]); };
+    auto fy = [&](int64_t c) { return M::div(Ax[c + 1] - Ax[c], dz, idz) - M::div(Az[c + p0] - Az[c], dx, idx) + S(b0[1]); };
+    auto fz = [&](int64_t c) { return M::div(Ay[c + p0] - Ay[c], dx, idx) - M::div(Ax[c + p1] - Ax[c], dy, idy) + S(b0[2]); };
+    const S bxl = fx(o), byl = fy(o), bzl = fz(o);
+    bx = S(0.5) * (bxl + fx(o + p0));
+    by = S(0.5) * (byl + fy(o + p1));
+    bz = S(0.5) * (bzl + fz(o + 1));
+    bn_lower = axis == 0 ? bxl : (axis == 1 ? byl : bzl);
+  }
+  const S ir = M::inv(r);
+  const S u = M::div(m0, r, ir), v = M::div(m1, r, ir), w = M::div(m2, r, ir);
+  q[0] = r;
+  q[1] = u;
+  q[2] = v;
+  q[3] = w;
+  q[4] = recover_pressure<S>(r, m0, m1, m2, e, bx, by, bz, u, v, w, gamma);
+  q[5] = bx;
+  q[6] = by;
+  q[7] = bz;
+}
+
+// The flux through the lower face along `axis` of haloed cell (i, j, k), in the frame of
+// that axis; conserved rows returned in physical order (2D: rho, mx, my, mz, E, Bz; 3D:
+// rho, mx, my, mz, E), computed in the state's precision like the stage kernels.
+template <typename S, int LIM>
+__device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, int i, int j, int k,
+                          const double* b0, double gamma, double (&out)[6]) {
+  int comp[7], rows[6];
+  int ncons;
+  if (ndim == 2) {
+    ncons = 6;
+    if (axis == 0) {
+      const int c[7] = {0, 1, 2, 3, 4, 6, 7};
+      const int r[6] = {0, 1, 2, 3, 4, 6};
+      for (int t = 0; t < 7; ++t) comp[t] = c[t];
+      for (int t = 0; t < 6; ++t) rows[t] = r[t];
+    } else {
+      const int c[7] = {0, 2, 1, 3, 4, 5, 7};
+      const int r[6] = {0, 2, 1, 3, 4, 6};
+      for (int t = 0; t < 7; ++t) comp[t] = c[t];
+      for (int t = 0; t < 6; ++t) rows[t] = r[t];
+    }
+  } else {
+    ncons = 5;
+    const int s = axis, b = (axis + 1) % 3, c = (axis + 2) % 3;
+    comp[0] = 0;
+    comp[1] = 1 + s;
+    comp[2] = 1 + b;
+    comp[3] = 1 + c;
+    comp[4] = 4;
+    comp[5] = 5 + b;
+    comp[6] = 5 + c;
+    rows[0] = 0;
+    rows[1 + s] = 1;
+    rows[1 + b] = 2;
+    rows[1 + c] = 3;
+    rows[4] = 4;
+  }
+  S qs[4][7];
+  S bn = S(0);
+  for (int st = 0; st < 4; ++st) {
+    int ii = i, jj = j, kk = k;
+    if (axis == 0) ii += st - 2;
+    if (axis == 1) jj += st - 2;
+    if (axis == 2) kk += st - 2;
+    S q[8], bl;
+    cell_primitive<S>(src, P, ndim, ii, jj, kk, axis, b0, gamma, q, bl);
+    if (st == 2) bn = bl;  // the face is the lower face of the third cell
+    for (int t = 0; t < 7; ++t) qs[st][t] = q[comp[t]];
+  }
+  S L[7], Rt[7], F[7];
+  reconstruct<LIM>(qs[0], qs[1], qs[2], qs[3], L, Rt);
+  hlld_flux(L, Rt, bn, S(gamma), S(1.0 / (gamma - 1.0)), F);
+  for (int t = 0; t < ncons; ++t) out[t] = double(F[rows[t]]);
+}
+
+// One thread per coarse face of an interface: reg[slot] += mean of the fine faces over
+// it - the coarse face (each op holds both sides, so no two threads share a slot).
+template <typename S, int LIM>
+__global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                     const FaceFluxOp* __restrict__ ops, double b0x, double b0y, double b0z,
+                                     double gamma, double* __restrict__ reg) {
+  const FaceFluxOp op = ops[blockIdx.x];
+  const PatchDesc C = patches[op.coarse];
+  const PatchDesc F = patches[op.fine];
+  const double b0[3] = {b0x, b0y, b0z};
+  const int ncons = op.ndim == 2 ? 6 : 5;
+  const int fine_a = 2, fine_b = op.ndim == 3 ? 2 : 1;
+  for (int s = threadIdx.x; s < op.len; s += blockDim.x) {
+    const int s1 = s / op.width, s2 = s % op.width;
+    int idx[3] = {0, 0, 0};
+    idx[op.axis] = op.coarse_plane;
+    idx[op.t1] = op.coarse_t0[0] + s1;
+    if (op.ndim == 3) idx[op.t2] = op.coarse_t0[1] + s2;
+    double coarse[6];
+    face_flux<S, LIM>(pool + C.off, C, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, coarse);
+    double fine[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < fine_a; ++a)
+      for (int b = 0; b < fine_b; ++b) {
+        int f[3] = {0, 0, 0};
+        f[op.axis] = op.fine_plane;
+        f[op.t1] = op.fine_t0[0] + 2 * s1 + a;
+        if (op.ndim == 3) f[op.t2] = op.fine_t0[1] + 2 * s2 + b;
+        double g[6];
+        face_flux<S, LIM>(pool + F.off, F, op.ndim, op.axis, f[0], f[1], f[2], b0, gamma, g);
+        for (int q = 0; q < ncons; ++q) fine[q] += g[q];
+      }
+    const double count = double(fine_a * fine_b);
+    for (int q = 0; q < ncons; ++q) reg[op.reg_off + int64_t(q) * op.len + s] += fine[q] / count - coarse[q];
+  }
+}
+
+// Apply the register of one interface to the coarse cells beside it, then clear it:
+// U -= sign * (0.5 dt) * reg / dx (sign +1 where the interface is the cell's upper face).
+template <typename S>
+__global__ void reflux_apply_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                    const RefluxOp* __restrict__ ops, double* __restrict__ reg,
+                                    const double* __restrict__ dt) {
+  const RefluxOp op = ops[blockIdx.x];
+  const PatchDesc C = patches[op.coarse];
+  const double scale = 0.5 * dt[C.instance];
+  const int64_t count = int64_t(op.len) * op.ncomp;
+  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
+    const int q = int(t / op.len), s = int(t % op.len);
+    const int s1 = s / op.width, s2 = s % op.width;
+    int idx[3] = {op.c[0], op.c[1], op.c[2]};
+    idx[op.t1] += s1;
+    if (op.t2 >= 0) idx[op.t2] += s2;
+    const int64_t o = cell_offset(C, idx[0], idx[1], idx[2]);
+    double& r = reg[op.reg_off + int64_t(q) * op.len + s];
+    S* u = pool + C.off + int64_t(op.field[q]) * C.fstride + o;
+    *u = S(double(*u) - op.sign * scale * r / op.dx);
+    r = 0.0;
+  }
+}
+
+template <typename S>
+int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
+                         double gamma, int limiter, double* reg, cudaStream_t stream) {
+  if (nops <= 0) return kOk;
+  switch (limiter) {
+    case 0: face_flux_ops_kernel<S, 0><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
+    case 1: face_flux_ops_kernel<S, 1><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
+    case 2: face_flux_ops_kernel<S, 2><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
+    default: face_flux_ops_kernel<S, 3><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
+  }
+  return check_launch("face flux ops");
+}
+
+template <typename S>
+int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
+                        const double* dt, cudaStream_t stream) {
+  if (nops > 0) reflux_apply_kernel<S><<<nops, 128, 0, stream>>>(pool, patches, ops, reg, dt);
+  return check_launch("reflux");
+}
+
+template int launch_face_flux_ops<float>(const float*, const PatchDesc*, const FaceFluxOp*, int, const double*, double,
+                                         int, double*, cudaStream_t);
+template int launch_face_flux_ops<double>(const double*, const PatchDesc*, const FaceFluxOp*, int, const double*,
+                                          double, int, double*, cudaStream_t);
+template int launch_reflux_apply<float>(float*, const PatchDesc*, const RefluxOp*, int, double*, const double*,
+                                        cudaStream_t);
+template int launch_reflux_apply<double>(double*, const PatchDesc*, const RefluxOp*, int, double*, const double*,
+                                         cudaStream_t);
+
+}  // namespace wb

@@ -32,28 +32,6 @@ struct Tile3D {
 };
 
 template <typename S>
-__device__ __forceinline__ S pressure3(S r, S m0, S m1, S m2, S e, S bx, S by, S bz, S u, S v, S w,
-                                       double gamma);
-
-template <>
-__device__ __forceinline__ double pressure3<double>(double r, double, double, double, double e, double bx,
-                                                    double by, double bz, double u, double v, double w,
-                                                    double gamma) {
-  return (gamma - 1.0) * (e - 0.5 * r * (u * u + v * v + w * w) - 0.5 * (bx * bx + by * by + bz * bz));
-}
-
-template <>
-__device__ __forceinline__ float pressure3<float>(float r, float m0, float m1, float m2, float e, float bx,
-                                                  float by, float bz, float, float, float, double gamma) {
-  // 1 / rho: the float reciprocal refined by one Newton step in float64
-  double inv_r = double(__fdividef(1.0f, r));
-  inv_r = inv_r * (2.0 - double(r) * inv_r);
-  const double kinetic = 0.5 * (double(m0) * m0 + double(m1) * m1 + double(m2) * m2) * inv_r;
-  const double magnetic = 0.5 * (double(bx) * bx + double(by) * by + double(bz) * bz);
-  return float((gamma - 1.0) * (double(e) - kinetic - magnetic));
-}
-
-template <typename S>
 __device__ __forceinline__ bool bad3(S r, S u, S v, S w, S p, S bx, S by, S bz) {
   if (!(r > S(0) && p > S(0))) return true;
   return !(isfinite(r) && isfinite(u) && isfinite(v) && isfinite(w) && isfinite(p) && isfinite(bx) &&
@@ -169,7 +147,7 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
         const S irho = M::inv(rho);
         const S u = M::div(m0, rho, irho), v = M::div(m1, rho, irho), w = M::div(m2, rho, irho);
         const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
-        S pr = pressure3<S>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
+        S pr = recover_pressure<S>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
         if (!valid) pr = S(1);
         P8[r] = rho;
         P8[NR + r] = u;

@@ -89,7 +89,12 @@ class Engine:
         self.time = torch.zeros(n, dtype=torch.float64, device=self.device)
         self.end = torch.zeros(n, dtype=torch.float64, device=self.device)
         self.bad = torch.zeros(1, dtype=torch.int64, device=self.device)
-        self.bflux = torch.zeros(max(L.bflux_size, 1), dtype=torch.float64, device=self.device)
+        self.bflux = None
+        self.face_flux_ops = _device_bytes(L.face_flux_ops, self.device)
+        self.nface = int(L.face_flux_ops.size)
+        self.reflux_ops = _device_bytes(L.reflux_ops, self.device)
+        self.nreflux = int(L.reflux_ops.size)
+        self.register = torch.zeros(max(L.register_size, 1), dtype=torch.float64, device=self.device)
         self.stream = stream
         #: kernels launched by this engine (counted per C-ABI call)
         self.launches = 0
@@ -182,15 +187,36 @@ class Engine:
             out[index] = np.frombuffer(np.uint64(bits).tobytes(), dtype=np.float64)[0]
         return out
 
+    def face_fluxes(self, pool):
+        """Register += fine-mean minus coarse fluxes of every coarse-fine interface face."""
+        if self.nface:
+            b = self.mean_field
+            _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                      self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
+                      self.register.data_ptr(), self._s())
+            self.launches += 1
+
+    def reflux(self, pool):
+        """Coarse cells beside fine patches take the register's correction (then cleared)."""
+        if self.nreflux:
+            _lib.call("wb_reflux_apply", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                      self.reflux_ops.data_ptr(), self.nreflux, self.register.data_ptr(), self.dt.data_ptr(),
+                      self._s())
+            self.launches += 1
+
     def heun_step(self, groups_potential, groups_all):
-        """One Heun step with the dt already in self.dt (device)."""
+        """One Heun step with the dt already in self.dt (device), refluxed and restricted."""
         U, U1 = self.state, self.stage_pool
+        refined = self.layout.h.max_level > 0
         self.stage(U, None, U1)
-        if self.layout.h.max_level > 0:
+        self.face_fluxes(U)
+        if refined:
             self.restrict(U1, groups_potential)
         self.fill(U1)
         self.stage(U1, U, U)
-        if self.layout.h.max_level > 0:
+        self.face_fluxes(U1)
+        self.reflux(U)
+        if refined:
             self.restrict(U, groups_all)
         self.fill(U)
 

@@ -191,6 +191,7 @@ class Layout:
         self.copy_phases = self._copy_ops()
         self.interp_levels = self._interp_ops()
         self.restrict_levels = self._restrict_ops()
+        self.face_flux_ops, self.reflux_ops, self.register_size = self._reflux_ops()
 
     # ownership ---------------------------------------------------------------------------
     def _own_last(self):
@@ -526,36 +527,121 @@ class Layout:
         return levels
 
     def _restrict_ops(self):
-        """Per level >= 1, ops setting the level below from it, per field group."""
+        """Per level >= 1, ops setting the level below from it, per field group.
+
+        Periodic images count: on a periodic axis a fine node plane on the domain's upper
+        face is also coarse node plane 0.
+        """
         h = self.h
         levels = {0: {}}
         for level in range(1, h.max_level + 1):
+            n_fine = h.level_shape(level)
             per_group = {}
             for g in self.groups:
                 ops = []
                 for f in h.patches_at_level(level):
+                    shifts = [
+                        (0, -n_fine[a], n_fine[a]) if h.periodic[a] and (g.node_mask >> a) & 1 else (0,)
+                        for a in range(self.ndim)
+                    ]
                     for c in h.patches_at_level(level - 1):
                         cbox = self._computed_box(c, g)
+                        for shift in itertools.product(*shifts):
+                            ranges = []
+                            for a in range(self.ndim):
+                                node = (g.node_mask >> a) & 1
+                                flo, fhi = f.box[a][0] + shift[a], f.box[a][1] + shift[a]
+                                lo = max(flo // 2, c.box[a][0])
+                                hi = min(fhi // 2 + node, c.box[a][0] + cbox[a][1] - HALO)
+                                if lo >= hi:
+                                    break
+                                ranges.append((lo, hi, flo))
+                            else:
+                                op = np.zeros((), dtype=_lib.RESTRICT_OP)
+                                op["fine"], op["coarse"] = f.index, c.index
+                                op["field_lo"], op["field_hi"] = g.lo, g.hi
+                                op["node_mask"], op["ndim"] = g.node_mask, self.ndim
+                                op["n"] = [hi - lo for lo, hi, _ in ranges] + [1] * (3 - self.ndim)
+                                op["c"] = [lo - c.box[a][0] + HALO for a, (lo, _, _) in enumerate(ranges)] + [0] * (3 - self.ndim)
+                                op["f"] = [2 * lo - flo + HALO for lo, _, flo in ranges] + [0] * (3 - self.ndim)
+                                ops.append(op)
+                per_group[g] = self._pack(ops, _lib.RESTRICT_OP)
+            levels[level] = per_group
+        return levels
+
+    # refluxing ----------------------------------------------------------------------------
+    def _reflux_ops(self):
+        """Coarse-fine interfaces: one FaceFluxOp and one RefluxOp per (fine side, coarse patch).
+
+        The coarse cell outside fine patch F across its side along axis a (wrapped on a
+        periodic axis) takes the correction; its face shared with F's region is recomputed
+        in the coarse patch holding that cell, the fine faces in F.
+        """
+        h = self.h
+        ncons = 6 if self.ndim == 2 else 5
+        face_ops, reflux_ops = [], []
+        offset = 0
+        for f in h.patches:
+            if f.level == 0:
+                continue
+            n_coarse = h.level_shape(f.level - 1)
+            dx = h.spacing(f.level - 1)
+            for a in range(self.ndim):
+                trans = [b for b in range(self.ndim) if b != a]
+                for side in (0, 1):
+                    plane_f = f.box[a][side]
+                    plane_c = plane_f // 2
+                    outside = plane_c - 1 if side == 0 else plane_c
+                    if h.periodic[a]:
+                        outside_w = outside % n_coarse[a]
+                    elif 0 <= outside < n_coarse[a]:
+                        outside_w = outside
+                    else:
+                        continue
+                    face_c = outside_w + 1 if side == 0 else outside_w
+                    for c in h.patches_at_level(f.level - 1):
+                        if not c.box[a][0] <= outside_w < c.box[a][1]:
+                            continue
                         ranges = []
-                        for a in range(self.ndim):
-                            node = (g.node_mask >> a) & 1
-                            lo = max(f.box[a][0] // 2, c.box[a][0])
-                            hi = min(f.box[a][1] // 2 + node, c.box[a][0] + cbox[a][1] - HALO)
+                        for b in trans:
+                            lo = max(f.box[b][0] // 2, c.box[b][0])
+                            hi = min(f.box[b][1] // 2, c.box[b][1])
                             if lo >= hi:
                                 break
                             ranges.append((lo, hi))
                         else:
-                            op = np.zeros((), dtype=_lib.RESTRICT_OP)
-                            op["fine"], op["coarse"] = f.index, c.index
-                            op["field_lo"], op["field_hi"] = g.lo, g.hi
-                            op["node_mask"], op["ndim"] = g.node_mask, self.ndim
-                            op["n"] = [hi - lo for lo, hi in ranges] + [1] * (3 - self.ndim)
-                            op["c"] = [lo - c.box[a][0] + HALO for a, (lo, _) in enumerate(ranges)] + [0] * (3 - self.ndim)
-                            op["f"] = [2 * lo - f.box[a][0] + HALO for a, (lo, _) in enumerate(ranges)] + [0] * (3 - self.ndim)
-                            ops.append(op)
-                per_group[g] = self._pack(ops, _lib.RESTRICT_OP)
-            levels[level] = per_group
-        return levels
+                            counts = [hi - lo for lo, hi in ranges]
+                            length = int(np.prod(counts))
+                            width = counts[1] if self.ndim == 3 else 1
+                            op = np.zeros((), dtype=_lib.FACE_FLUX_OP)
+                            op["coarse"], op["fine"] = c.index, f.index
+                            op["ndim"], op["axis"] = self.ndim, a
+                            op["t1"] = trans[0]
+                            op["t2"] = trans[1] if self.ndim == 3 else -1
+                            op["coarse_plane"] = face_c - c.box[a][0] + HALO
+                            op["fine_plane"] = plane_f - f.box[a][0] + HALO
+                            op["coarse_t0"] = [lo - c.box[b][0] + HALO for b, (lo, _) in zip(trans, ranges, strict=True)] + [0] * (3 - self.ndim)
+                            op["fine_t0"] = [2 * lo - f.box[b][0] + HALO for b, (lo, _) in zip(trans, ranges, strict=True)] + [0] * (3 - self.ndim)
+                            op["len"], op["width"] = length, width
+                            op["reg_off"] = offset
+                            face_ops.append(op)
+                            rop = np.zeros((), dtype=_lib.REFLUX_OP)
+                            rop["coarse"] = c.index
+                            rop["len"], rop["width"], rop["ncomp"] = length, width, ncons
+                            cidx = [0, 0, 0]
+                            cidx[a] = outside_w - c.box[a][0] + HALO
+                            for b, (lo, _) in zip(trans, ranges, strict=True):
+                                cidx[b] = lo - c.box[b][0] + HALO
+                            rop["c"] = cidx
+                            rop["t1"] = trans[0]
+                            rop["t2"] = trans[1] if self.ndim == 3 else -1
+                            rop["field"] = list(range(ncons)) + [0] * (8 - ncons)
+                            rop["sign"] = 1.0 if side == 0 else -1.0
+                            rop["dx"] = dx[a]
+                            rop["reg_off"] = offset
+                            reflux_ops.append(rop)
+                            offset += ncons * length
+        return (self._pack(face_ops, _lib.FACE_FLUX_OP), self._pack(reflux_ops, _lib.REFLUX_OP), offset)
 
     @staticmethod
     def _pack(ops, dtype, chunk=4096):
@@ -563,6 +649,8 @@ class Layout:
         (one CUDA block runs one op, so large halo slabs need many)."""
         if not ops:
             return np.zeros(0, dtype)
+        if dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
+            return np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
         out = []
         for o in ops:
             o = np.asarray(o).reshape(())

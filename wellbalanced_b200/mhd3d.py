@@ -361,16 +361,34 @@ class MHD3D:
             largest = max(largest, float(torch.max(torch.abs(div))) * min(spacing))
         return largest
 
+    def _covered(self, patch):
+        mask = np.zeros(patch.shape, dtype=bool)
+        for fine in self.hierarchy.patches_at_level(patch.level + 1):
+            idx = []
+            for a in range(3):
+                (flo, fhi), (lo, hi) = fine.box[a], patch.box[a]
+                s, e = max(flo // 2, lo), min(fhi // 2, hi)
+                if s >= e:
+                    break
+                idx.append(slice(s - lo, e - lo))
+            else:
+                mask[tuple(idx)] = True
+        return mask
+
     def totals(self) -> dict[str, float]:
+        """Integrals of the conserved fields from the leaf cells (float64)."""
         self._check_ready()
         out = dict.fromkeys(CONSERVED_3D, 0.0)
         for patch in self.hierarchy.patches:
-            if patch.level != self.hierarchy.max_level and self.hierarchy.max_level > 0:
-                raise NotImplementedError("3D totals over refined levels are not available yet")
             volume = float(np.prod(self.hierarchy.spacing(patch.level)))
+            leaf = torch.from_numpy(~self._covered(patch)).to(self.engine.device)
             for f, name in enumerate(CONSERVED_3D):
-                out[name] += float(torch.sum(self._read(patch, f).to(torch.float64))) * volume
+                out[name] += float(torch.sum(self._read(patch, f).to(torch.float64)[leaf])) * volume
         return out
+
+    def gather(self, patch, field):
+        extra = (0, 0, 0) if field < 5 else _EXTRA[field - 5]
+        return self._read(patch, field, extra).to(torch.float64).cpu().numpy()
 
     def state(self) -> dict[str, np.ndarray]:
         (patch,) = self.hierarchy.patches_at_level(0)
