@@ -130,7 +130,9 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
  * a stage, reg += (mean of the fine faces - the coarse face) of every coarse-fine
  * interface face, recomputed from the stage's input pool (struct FaceFluxOp); after the
  * step, the coarse cells beside the interfaces take U -= sign * 0.5 dt * reg / dx and reg
- * is cleared (struct RefluxOp; dt per instance on the device). */
+ * is cleared (struct RefluxOp; dt per instance on the device). The ops of one
+ * wb_reflux_apply call run concurrently and must not share a coarse cell: a cell between
+ * fine patches takes its corrections from separate calls (one per axis and side). */
 int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
                      double b0y, double b0z, double gamma, int limiter, double* reg, void* stream);
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,

@@ -29,6 +29,10 @@ CASES_2D = [
     ((16, 12), ((0.0, 1.0), (0.0, 1.0)), (True, True), None, [(1, ((8, 20), (6, 18)))], None),
     ((16, 12), ((0.0, 1.0), (0.0, 1.0)), (True, True), (2, 2), [(1, ((0, 12), (4, 16))), (1, ((20, 32), (8, 24)))], None),
     ((12, 12), ((0.0, 1.0), (0.0, 1.0)), (False, False), None, [(1, ((0, 8), (8, 24)))], None),
+    # a fine level over the whole periodic domain, and a second level inside it
+    ((8, 8), ((0.0, 1.0), (0.0, 1.0)), (True, True), None, [(1, ((0, 16), (0, 16))), (2, ((8, 24), (4, 20)))], None),
+    # two fine patches that together span the periodic x axis
+    ((8, 8), ((0.0, 1.0), (0.0, 1.0)), (True, True), None, [(1, ((0, 8), (4, 12))), (1, ((8, 16), (4, 12)))], None),
 ]
 
 
@@ -128,7 +132,7 @@ def test_tiles_cover_every_computed_node_once():
     assert layout.own[0] == (False, False) and layout.own[1] == (True, False)
 
 
-@pytest.mark.parametrize("case", [6, 7, 8])
+@pytest.mark.parametrize("case", [6, 7, 8, 9, 10])
 def test_2d_restriction_ops_match_the_oracle(case):
     from oracle.mhd2d import MHD2D as OracleMHD2D
 
@@ -146,6 +150,17 @@ def test_2d_restriction_ops_match_the_oracle(case):
     names = _fill_oracle_and_pool(model, layout, pool, rng, 7, extras)
     for name in names:
         oracle_h.restrict(name)
+    # node planes a fine patch does not compute are stale copies until the next halo fill:
+    # the restriction must not read them
+    for dev in layout.h.patches:
+        if dev.level == 0:
+            continue
+        view = layout.patch_view(pool, dev, 6)
+        for a in range(2):
+            if not layout.own[dev.index][a]:
+                index = [slice(None)] * 2
+                index[a] = 2 + dev.shape[a]
+                view[tuple(index)] = np.nan
     for level in range(layout.h.max_level, 0, -1):
         for g in layout.groups:
             _emulate.apply_restrict(pool, layout.rows, layout.restrict_levels[level][g])
@@ -157,3 +172,119 @@ def test_2d_restriction_ops_match_the_oracle(case):
             got = layout.patch_view(pool, dev, f)[tuple(slice(2, 2 + s) for s in expect.shape)]
             own = [s - (0 if (f < 6 or layout.own[dev.index][a]) else 1) for a, s in enumerate(expect.shape)]
             np.testing.assert_allclose(got[: own[0], : own[1]], expect[: own[0], : own[1]], atol=1e-14)
+
+
+def test_merged_layouts_fill_each_instance_independently():
+    parts = []
+    for shape in ((8, 6), (12, 10), (8, 6)):
+        h = AMRHierarchy(shape, ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True))
+        parts.append((h, Layout(h, precision=64)))
+    merged = Layout.merge([layout for _, layout in parts])
+    assert merged.ninstances == 3 and list(merged.instances) == [0, 1, 2]
+    rng = np.random.default_rng(5)
+    pool = rng.normal(size=merged.pool_size)
+    _emulate.fill(pool, merged)
+    start = 0
+    for k, (h, layout) in enumerate(parts):
+        single = pool[start : start + layout.pool_size].copy()
+        expect = single.copy()
+        _emulate.fill(expect, layout)
+        np.testing.assert_array_equal(single, expect)
+        start += layout.pool_size
+
+
+def test_reflux_phases_touch_disjoint_cells():
+    """A coarse cell between fine patches takes corrections from several RefluxOps; the
+    ops of one phase (one launch) must never share a cell."""
+    boxes = [((0, 8), (0, 14)), ((14, 20), (0, 4)), ((0, 4), (14, 18)), ((8, 20), (14, 28)), ((0, 20), (28, 36)),
+             ((0, 6), (44, 52)), ((8, 20), (36, 52)), ((0, 8), (52, 64)), ((24, 28), (0, 16)), ((28, 40), (0, 8)),
+             ((28, 38), (8, 20)), ((56, 64), (0, 20)), ((20, 24), (22, 48)), ((60, 64), (28, 36))]
+    h = AMRHierarchy((16, 16), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True))
+    h.add_patch(1, ((0, 32), (0, 32)))
+    for box in boxes:
+        h.add_patch(2, box)
+    layout = Layout(h, precision=64)
+    assert len(layout.reflux_phases) == 4
+    shared = 0
+    seen_any = {}
+    for ops in layout.reflux_phases:
+        seen = set()
+        for op in ops:
+            for s in range(int(op["len"])):
+                s1, s2 = divmod(s, int(op["width"]))
+                idx = [int(v) for v in op["c"]]
+                idx[int(op["t1"])] += s1
+                if int(op["t2"]) >= 0:
+                    idx[int(op["t2"])] += s2
+                cell = (int(op["coarse"]), *idx)
+                assert cell not in seen
+                seen.add(cell)
+                shared += cell in seen_any
+                seen_any[cell] = True
+    assert shared > 0  # the configuration does have cells corrected from two sides
+
+
+def test_op_records_keep_the_c_layout():
+    """Every record array handed to the kernels has the exact C struct layout (NumPy
+    repacks padded structured dtypes when concatenating; the upload casts back)."""
+    import torch
+
+    from wellbalanced_b200 import _lib
+    from wellbalanced_b200.engine import _device_bytes
+
+    h = AMRHierarchy((16, 16), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True))
+    h.add_patch(1, ((4, 12), (8, 20)))
+    h.add_patch(1, ((12, 20), (8, 16)))
+    single = Layout(h, precision=64)
+    merged = Layout.merge([single, single])
+    for layout in (single, merged):
+        arrays = [(layout.rows, _lib.PATCH), (layout.tiles, _lib.TILE), (layout.face_flux_ops, _lib.FACE_FLUX_OP),
+                  (layout.reflux_ops, _lib.REFLUX_OP)]
+        arrays += [(ops, _lib.REFLUX_OP) for ops in layout.reflux_phases]
+        arrays += [(ops, _lib.INTERP_OP) for ops in layout.interp_levels]
+        for same, boundary in layout.copy_phases:
+            arrays += [(same, _lib.COPY_OP)] + [(ops, _lib.COPY_OP) for ops in boundary]
+        for groups in layout.restrict_levels.values():
+            arrays += [(ops, _lib.RESTRICT_OP) for ops in groups.values()]
+        for array, dtype in arrays:
+            assert array.dtype == dtype and array.dtype.itemsize == dtype.itemsize
+            if array.size:
+                raw = _device_bytes(array, torch.device("cpu"), dtype)
+                assert raw.numel() == array.size * dtype.itemsize
+                back = raw.numpy().view(dtype)
+                assert back.tobytes() == np.ascontiguousarray(array).tobytes()
+    # a repacked array is cast back field by field
+    packed = np.concatenate([single.reflux_ops, single.reflux_ops])
+    assert packed.dtype.itemsize != _lib.REFLUX_OP.itemsize
+    raw = _device_bytes(packed, torch.device("cpu"), _lib.REFLUX_OP).numpy().view(_lib.REFLUX_OP)
+    for name in _lib.REFLUX_OP.names:
+        np.testing.assert_array_equal(raw[name], packed[name])
+
+
+@pytest.mark.parametrize("case", [6, 7, 8, 9, 10])
+def test_flux_register_ops_stay_inside_their_patches(case):
+    """FaceFluxOps read a 4-cell stencil (and the node after it) across each face, and
+    RefluxOps write interior cells only: check every index against the haloed extents."""
+    shape, bounds, periodic, split, fine, boundaries = CASES_2D[case]
+    h = AMRHierarchy(shape, bounds, periodic, split=split)
+    for level, box in fine:
+        h.add_patch(level, box)
+    layout = Layout(h, precision=64)
+    rows = layout.rows
+    for op in layout.face_flux_ops:
+        a, t1 = int(op["axis"]), int(op["t1"])
+        for patch, plane, t0, step in ((op["coarse"], op["coarse_plane"], op["coarse_t0"][0], 1),
+                                       (op["fine"], op["fine_plane"], op["fine_t0"][0], 2)):
+            n = rows[patch]["n"]
+            # haloed indices: cells plane-2 .. plane+1 of n+4, the node after them of n+5
+            assert 0 <= plane - 2 and plane + 1 < n[a] + 4
+            # transverse: interior cells only
+            last = t0 + step * int(op["len"]) - 1
+            assert 2 <= t0 and last < n[t1] + 2
+    for op in layout.reflux_ops:
+        n = rows[op["coarse"]]["n"]
+        t1 = int(op["t1"])
+        c = [int(v) for v in op["c"]][:2]
+        for axis in range(2):
+            hi = c[axis] + (int(op["len"]) - 1 if axis == t1 else 0)
+            assert 2 <= c[axis] and hi < 2 + n[axis]

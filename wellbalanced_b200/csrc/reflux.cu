@@ -161,6 +161,7 @@ __global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc
 
 // Apply the register of one interface to the coarse cells beside it, then clear it:
 // U -= sign * (0.5 dt) * reg / dx (sign +1 where the interface is the cell's upper face).
+// One block per op, no atomics: the ops of one launch must touch disjoint cells.
 template <typename S>
 __global__ void reflux_apply_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
                                     const RefluxOp* __restrict__ ops, double* __restrict__ reg,

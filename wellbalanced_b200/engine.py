@@ -37,19 +37,23 @@ def ctypes_ptr(t):
     return t.data_ptr()
 
 
-def _device_bytes(array, device):
-    """A uint8 device tensor holding a numpy structured array (None if empty)."""
+def _device_bytes(array, device, dtype):
+    """A uint8 device tensor holding a numpy structured array in the C layout ``dtype``
+    (None if empty). NumPy may repack a padded structured dtype (``np.concatenate`` does),
+    so the records are cast back to the exact layout the kernels read."""
     if array is None or array.size == 0:
         return None
-    raw = np.ascontiguousarray(array).view(np.uint8).reshape(-1)
-    return torch.from_numpy(raw.copy()).to(device)
+    array = np.ascontiguousarray(np.asarray(array).astype(dtype, copy=False))
+    if array.dtype != dtype or array.dtype.itemsize != dtype.itemsize:
+        raise TypeError(f"op records of dtype {array.dtype} do not have the C layout {dtype}")
+    return torch.from_numpy(array.view(np.uint8).reshape(-1).copy()).to(device)
 
 
 class Engine:
     """Device pools + op lists of one hierarchy; the kernels' launch sequence."""
 
     def __init__(self, hierarchy, *, precision=32, walls=None, limiter=1, gamma=5.0 / 3.0, mean_field=(0.0, 0.0, 0.0),
-                 instances=None, device="cuda", lx=32, stream=None):
+                 instances=None, device="cuda", lx=32, stream=None, layout=None):
         if precision not in (32, 64):
             raise ValueError("precision is 32 or 64")
         if not torch.cuda.is_available():
@@ -61,25 +65,27 @@ class Engine:
         self.limiter = int(limiter)
         self.gamma = float(gamma)
         self.mean_field = tuple(float(b) for b in mean_field) + (0.0,) * (3 - len(mean_field))
-        self.layout = Layout(hierarchy, walls=walls, precision=precision, lx=lx, instances=instances)
+        self.layout = layout if layout is not None else Layout(
+            hierarchy, walls=walls, precision=precision, lx=lx, instances=instances)
         L = self.layout
         self.ndim = L.ndim
         self.state = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
         self.stage_pool = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
-        self.patches = _device_bytes(L.rows, self.device)
-        self.tiles = _device_bytes(L.tiles, self.device)
+        self.patches = _device_bytes(L.rows, self.device, _lib.PATCH)
+        self.tiles = _device_bytes(L.tiles, self.device, _lib.TILE)
         self.ntiles = int(L.tiles.size)
         self.chunk_patch = torch.from_numpy(L.chunk_patch).to(self.device)
         self.chunk_start = torch.from_numpy(L.chunk_start).to(self.device)
         self.nchunks = int(L.chunk_patch.size)
         self.inv_dx2_sum = torch.from_numpy(L.inv_dx2_sum).to(self.device)
         self.copy_phases = [
-            (_device_bytes(same, self.device), same.size, [(_device_bytes(b, self.device), b.size) for b in bnd])
+            (_device_bytes(same, self.device, _lib.COPY_OP), same.size,
+             [(_device_bytes(b, self.device, _lib.COPY_OP), b.size) for b in bnd])
             for same, bnd in L.copy_phases
         ]
-        self.interp_levels = [(_device_bytes(ops, self.device), ops.size) for ops in L.interp_levels]
+        self.interp_levels = [(_device_bytes(ops, self.device, _lib.INTERP_OP), ops.size) for ops in L.interp_levels]
         self.restrict_levels = {
-            level: {g: (_device_bytes(ops, self.device), ops.size) for g, ops in groups.items()}
+            level: {g: (_device_bytes(ops, self.device, _lib.RESTRICT_OP), ops.size) for g, ops in groups.items()}
             for level, groups in L.restrict_levels.items()
         }
         n = L.ninstances
@@ -90,10 +96,14 @@ class Engine:
         self.end = torch.zeros(n, dtype=torch.float64, device=self.device)
         self.bad = torch.zeros(1, dtype=torch.int64, device=self.device)
         self.bflux = None
-        self.face_flux_ops = _device_bytes(L.face_flux_ops, self.device)
+        self.face_flux_ops = _device_bytes(L.face_flux_ops, self.device, _lib.FACE_FLUX_OP)
         self.nface = int(L.face_flux_ops.size)
-        self.reflux_ops = _device_bytes(L.reflux_ops, self.device)
+        self.reflux_ops = _device_bytes(L.reflux_ops, self.device, _lib.REFLUX_OP)
         self.nreflux = int(L.reflux_ops.size)
+        counts = [int(ops.size) for ops in L.reflux_phases]
+        starts = np.cumsum([0, *counts[:-1]])
+        #: (first op, op count) of each reflux phase in `reflux_ops`
+        self.reflux_phases = [(int(a), c) for a, c in zip(starts, counts, strict=True) if c]
         self.register = torch.zeros(max(L.register_size, 1), dtype=torch.float64, device=self.device)
         self.stream = stream
         #: kernels launched by this engine (counted per C-ABI call)
@@ -131,7 +141,7 @@ class Engine:
     def restrict(self, pool, groups):
         """Coarse values under finer patches from the fine ones (finest level first)."""
         s = self._s()
-        for level in range(self.layout.h.max_level, 0, -1):
+        for level in range(self.layout.max_level, 0, -1):
             for g in groups:
                 ops, nops = self.restrict_levels[level][g]
                 if nops:
@@ -198,16 +208,17 @@ class Engine:
 
     def reflux(self, pool):
         """Coarse cells beside fine patches take the register's correction (then cleared)."""
-        if self.nreflux:
+        size = _lib.REFLUX_OP.itemsize
+        for start, count in self.reflux_phases:
             _lib.call("wb_reflux_apply", self.precision, pool.data_ptr(), self.patches.data_ptr(),
-                      self.reflux_ops.data_ptr(), self.nreflux, self.register.data_ptr(), self.dt.data_ptr(),
-                      self._s())
+                      self.reflux_ops.data_ptr() + start * size, count, self.register.data_ptr(),
+                      self.dt.data_ptr(), self._s())
             self.launches += 1
 
     def heun_step(self, groups_potential, groups_all):
         """One Heun step with the dt already in self.dt (device), refluxed and restricted."""
         U, U1 = self.state, self.stage_pool
-        refined = self.layout.h.max_level > 0
+        refined = self.layout.max_level > 0
         self.stage(U, None, U1)
         self.face_fluxes(U)
         if refined:

@@ -166,6 +166,15 @@ def _boxes_intersect(a, b):
     return tuple(out)
 
 
+def _concat(arrays, dtype):
+    """Records of ``arrays`` in one array of the C layout ``dtype`` (``np.concatenate``
+    alone may repack a padded structured dtype)."""
+    arrays = [np.asarray(a) for a in arrays if a is not None and np.asarray(a).size]
+    if not arrays:
+        return np.zeros(0, dtype)
+    return np.concatenate(arrays).astype(dtype)
+
+
 class Layout:
     """Pool layout, work lists and op lists of a hierarchy for the MHD state."""
 
@@ -191,7 +200,7 @@ class Layout:
         self.copy_phases = self._copy_ops()
         self.interp_levels = self._interp_ops()
         self.restrict_levels = self._restrict_ops()
-        self.face_flux_ops, self.reflux_ops, self.register_size = self._reflux_ops()
+        self.face_flux_ops, self.reflux_phases, self.register_size = self._reflux_ops()
 
     # ownership ---------------------------------------------------------------------------
     def _own_last(self):
@@ -530,7 +539,9 @@ class Layout:
         """Per level >= 1, ops setting the level below from it, per field group.
 
         Periodic images count: on a periodic axis a fine node plane on the domain's upper
-        face is also coarse node plane 0.
+        face is also coarse node plane 0. Only nodes the fine patch computes are read: its
+        upper plane, when a neighbour or its own periodic image provides it, holds the
+        previous fill's values until the halo fill that follows the restriction.
         """
         h = self.h
         levels = {0: {}}
@@ -549,7 +560,9 @@ class Layout:
                         for shift in itertools.product(*shifts):
                             ranges = []
                             for a in range(self.ndim):
-                                node = (g.node_mask >> a) & 1
+                                # a fine patch's upper node plane counts only where it computes
+                                # it (else it is a copy filled after the restriction)
+                                node = (g.node_mask >> a) & 1 and self.own[f.index][a]
                                 flo, fhi = f.box[a][0] + shift[a], f.box[a][1] + shift[a]
                                 lo = max(flo // 2, c.box[a][0])
                                 hi = min(fhi // 2 + node, c.box[a][0] + cbox[a][1] - HALO)
@@ -569,17 +582,130 @@ class Layout:
             levels[level] = per_group
         return levels
 
+    # batches ------------------------------------------------------------------------------
+    @classmethod
+    def merge(cls, layouts):
+        """One layout holding independent problems: instance k is ``layouts[k]``.
+
+        Patch, pool, instance and register indices of each part are shifted past the
+        previous parts; no op couples two parts (each keeps its own periodic images).
+        Parts may repeat (a batch of same-sized problems shares one part layout).
+        """
+        first = layouts[0]
+        out = cls.__new__(cls)
+        out.h = None
+        out.ndim = first.ndim
+        out.nfields = first.nfields
+        out.groups = first.groups
+        out.precision = first.precision
+        out.lx = first.lx
+        out.tile_shape = first.tile_shape
+        out.walls = first.walls
+        rows, tiles, chunk_patch, chunk_start, inv = [], [], [], [], []
+        same_levels, boundary_levels, interp_levels = {}, {}, {}
+        restrict_levels, face_ops = {}, []
+        reflux_phases = [[] for _ in range(2 * first.ndim)]
+        own, instances = [], []
+        patch_shift = pool_shift = reg_shift = 0
+        for k, part in enumerate(layouts):
+            r = part.rows.copy()
+            r["off"] += pool_shift
+            r["instance"] = k
+            rows.append(r)
+            own.extend(part.own)
+            instances.extend([k] * part.npatches)
+            t = part.tiles.copy()
+            t["patch"] += patch_shift
+            tiles.append(t)
+            chunk_patch.append(part.chunk_patch + patch_shift)
+            chunk_start.append(part.chunk_start)
+            inv.append(part.inv_dx2_sum[:1])
+
+            def shifted(ops, fields):
+                ops = ops.copy()
+                for name in fields:
+                    mask = ops[name] >= 0
+                    ops[name][mask] += patch_shift
+                return ops
+
+            for level, (same, boundary) in enumerate(part.copy_phases):
+                same_levels.setdefault(level, []).append(shifted(same, ("dst", "src1", "src2")))
+                for axis, ops in enumerate(boundary):
+                    boundary_levels.setdefault((level, axis), []).append(shifted(ops, ("dst", "src1", "src2")))
+            for level, ops in enumerate(part.interp_levels):
+                interp_levels.setdefault(level, []).append(shifted(ops, ("fine", "coarse")))
+            for level, groups in part.restrict_levels.items():
+                for g, ops in groups.items():
+                    restrict_levels.setdefault(level, {}).setdefault(g, []).append(shifted(ops, ("fine", "coarse")))
+            f = shifted(part.face_flux_ops, ("coarse", "fine"))
+            f["reg_off"] += reg_shift
+            face_ops.append(f)
+            for phase, ops in enumerate(part.reflux_phases):
+                rf = shifted(ops, ("coarse",))
+                rf["reg_off"] += reg_shift
+                reflux_phases[phase].append(rf)
+            patch_shift += part.npatches
+            pool_shift += part.pool_size
+            reg_shift += part.register_size
+        out.rows = _concat(rows, _lib.PATCH)
+        out.npatches = patch_shift
+        out.pool_size = pool_shift
+        out.own = own
+        out.instances = np.array(instances, dtype=np.int32)
+        out.ninstances = len(layouts)
+        out.tiles = _concat(tiles, _lib.TILE)
+        out.chunk_patch = np.concatenate(chunk_patch).astype(np.int32)
+        out.chunk_start = np.concatenate(chunk_start).astype(np.int32)
+        out.inv_dx2_sum = np.concatenate(inv)
+        nlevels = max(len(part.copy_phases) for part in layouts)
+        naxes = first.ndim
+        out.copy_phases = []
+        for level in range(nlevels):
+            same = _concat(same_levels.get(level, []), _lib.COPY_OP)
+            boundary = [_concat(boundary_levels.get((level, a), []), _lib.COPY_OP) for a in range(naxes)]
+            out.copy_phases.append((same, boundary))
+        out.interp_levels = [_concat(interp_levels.get(level, []), _lib.INTERP_OP) for level in range(nlevels)]
+        out.restrict_levels = {0: {}}
+        for level, groups in restrict_levels.items():
+            if level == 0:
+                continue
+            out.restrict_levels[level] = {g: _concat(ops, _lib.RESTRICT_OP) for g, ops in groups.items()}
+        out.face_flux_ops = _concat(face_ops, _lib.FACE_FLUX_OP)
+        out.reflux_phases = [_concat(ops, _lib.REFLUX_OP) for ops in reflux_phases]
+        out.register_size = reg_shift
+        out.max_level = max(part.max_level for part in layouts)
+        return out
+
+    @property
+    def max_level(self):
+        return self.__dict__.get("_max_level", self.h.max_level if self.h is not None else 0)
+
+    @max_level.setter
+    def max_level(self, value):
+        self.__dict__["_max_level"] = value
+
     # refluxing ----------------------------------------------------------------------------
+    @property
+    def reflux_ops(self):
+        """All RefluxOps, phase after phase (`reflux_phases`)."""
+        return _concat(self.reflux_phases, _lib.REFLUX_OP)
+
     def _reflux_ops(self):
         """Coarse-fine interfaces: one FaceFluxOp and one RefluxOp per (fine side, coarse patch).
 
         The coarse cell outside fine patch F across its side along axis a (wrapped on a
         periodic axis) takes the correction; its face shared with F's region is recomputed
         in the coarse patch holding that cell, the fine faces in F.
+
+        A coarse cell between fine patches takes corrections from several sides, so the
+        RefluxOps come in 2 * ndim phases, one per (axis, side), applied one after the
+        other: two ops of one phase never meet in a cell (the fine patches of a level do
+        not overlap), so each phase is one race-free launch.
         """
         h = self.h
         ncons = 6 if self.ndim == 2 else 5
-        face_ops, reflux_ops = [], []
+        face_ops = []
+        phases = [[] for _ in range(2 * self.ndim)]
         offset = 0
         for f in h.patches:
             if f.level == 0:
@@ -639,9 +765,9 @@ class Layout:
                             rop["sign"] = 1.0 if side == 0 else -1.0
                             rop["dx"] = dx[a]
                             rop["reg_off"] = offset
-                            reflux_ops.append(rop)
+                            phases[2 * a + side].append(rop)
                             offset += ncons * length
-        return (self._pack(face_ops, _lib.FACE_FLUX_OP), self._pack(reflux_ops, _lib.REFLUX_OP), offset)
+        return (self._pack(face_ops, _lib.FACE_FLUX_OP), [self._pack(ops, _lib.REFLUX_OP) for ops in phases], offset)
 
     @staticmethod
     def _pack(ops, dtype, chunk=4096):

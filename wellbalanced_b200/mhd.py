@@ -231,7 +231,7 @@ class MHD2D:
     def _write(self, patch, field, values):
         n = values.shape
         view = self.engine.view(self.engine.state, patch, field)
-        view[HALO : HALO + n[0], HALO : HALO + n[1]] = torch.from_numpy(np.ascontiguousarray(values)).to(
+        view[HALO : HALO + n[0], HALO : HALO + n[1]] = torch.from_numpy(np.require(values, requirements=("C", "W"))).to(
             view.device, view.dtype
         )
 
@@ -383,6 +383,23 @@ class MHD2D:
             raise ValueError("the saved state belongs to another layout or precision")
         pool.copy_(host, non_blocking=True)
         self._ready = True
+
+    def regrid(self, tags: dict[int, np.ndarray], **options: Any) -> None:
+        """Regrid on ``tags`` (``carafe/mhd.py:1043-1056``): new patches over the tagged
+        cells (`AMRHierarchy.regrid` options: ``max_patch_size``, ``buffer``), the conserved
+        fields moved with their integrals kept, ``A_z`` interpolated (div B stays zero)."""
+        from wellbalanced_b200.regrid import regrid_model
+
+        regrid_model(self, tags, **options)
+
+    def _field_extras(self):
+        return [(0, 0)] * 6 + [(1, 1)]
+
+    def _gather_field(self, patch, f):
+        return self.gather(patch, f, node=f == 6)
+
+    def _write_field(self, patch, f, values):
+        self._write(patch, f, values)
 
     # diagnostics ---------------------------------------------------------------------------------
     def divergence(self) -> float:

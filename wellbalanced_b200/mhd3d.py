@@ -76,18 +76,8 @@ class MHD3D:
         self.periodic = tuple(hierarchy.periodic)
         self.precision = int(precision)
         self.device = device
-        self.engine = Engine(
-            hierarchy,
-            precision=self.precision,
-            limiter=LIMITER_CODES.index(limiter),
-            gamma=self.gamma,
-            mean_field=self.mean_field,
-            device=device,
-            lx=lx,
-        )
-        groups = self.engine.layout.groups
-        self._groups_all = groups
-        self._groups_potential = groups[1:]
+        self.lx = lx
+        self._build_engine()
         self.time = 0.0
         self.steps = 0
         self.period = float("nan")
@@ -95,6 +85,20 @@ class MHD3D:
 
     #: whether steps run the fused stage kernel (False: the per-kernel float64 path)
     _fused = True
+
+    def _build_engine(self):
+        self.engine = Engine(
+            self.hierarchy,
+            precision=self.precision,
+            limiter=LIMITER_CODES.index(self.limiter),
+            gamma=self.gamma,
+            mean_field=self.mean_field,
+            device=self.device,
+            lx=self.lx,
+        )
+        groups = self.engine.layout.groups
+        self._groups_all = groups
+        self._groups_potential = groups[1:]
 
     # test problems (carafe/mhd3d.py:236-346) -----------------------------------------------------
     @classmethod
@@ -211,7 +215,7 @@ class MHD3D:
 
     def _write(self, patch, field, values, extra=(0, 0, 0)):
         view = self.engine.view(self.engine.state, patch, field)
-        view[self._slices(patch, extra)] = torch.from_numpy(np.ascontiguousarray(values)).to(view.device, view.dtype)
+        view[self._slices(patch, extra)] = torch.from_numpy(np.require(values, requirements=("C", "W"))).to(view.device, view.dtype)
 
     def _read(self, patch, field, extra=(0, 0, 0), pool=None):
         pool = self.engine.state if pool is None else pool
@@ -342,6 +346,59 @@ class MHD3D:
             raise ValueError("the saved state belongs to another layout or precision")
         pool.copy_(host, non_blocking=True)
         self._ready = True
+
+    # refinement ----------------------------------------------------------------------------------
+    def current_tags(self, threshold: float, levels: int) -> dict[int, np.ndarray]:
+        """Tag cells where ``|J|`` (central differences of the cell field) times the cell
+        size exceeds ``threshold`` (``carafe/mhd3d.py:771-801``)."""
+        self._check_ready()
+        h = self.hierarchy
+        tags = {level: np.zeros(h.level_shape(level), dtype=bool) for level in range(min(levels, h.max_level + 1))}
+        for patch in h.patches:
+            if patch.level not in tags:
+                continue
+            spacing = h.spacing(patch.level)
+            eng = self.engine
+            nx, ny, nz = patch.shape
+            X, Y, Z = nx + 4, ny + 4, nz + 4
+            pot = (
+                eng.view(eng.state, patch, 5)[:X, : Y + 1, : Z + 1].to(torch.float64),
+                eng.view(eng.state, patch, 6)[: X + 1, :Y, : Z + 1].to(torch.float64),
+                eng.view(eng.state, patch, 7)[: X + 1, : Y + 1, :Z].to(torch.float64),
+            )
+            faces = []
+            for a in range(3):
+                _, b, c = _cyclic(a)
+                faces.append(torch.diff(pot[c], dim=b) / spacing[b] - torch.diff(pot[b], dim=c) / spacing[c]
+                             + self.mean_field[a])
+            cells = [0.5 * (f.narrow(a, 0, f.shape[a] - 1) + f.narrow(a, 1, f.shape[a] - 1)) for a, f in enumerate(faces)]
+            square = 0.0
+            for c in range(3):
+                _, a, b = _cyclic(c)
+                jc = torch.gradient(cells[b], spacing=spacing[a], dim=a)[0] - torch.gradient(
+                    cells[a], spacing=spacing[b], dim=b)[0]
+                square = square + jc**2
+            size = torch.sqrt(square)[HALO:-HALO, HALO:-HALO, HALO:-HALO]
+            index = tuple(slice(lo, hi) for lo, hi in patch.box)
+            tags[patch.level][index] |= (size * max(spacing) > threshold).cpu().numpy()
+        return tags
+
+    def regrid(self, tags: dict[int, np.ndarray], **options: Any) -> None:
+        """Regrid on ``tags`` (``carafe/mhd3d.py:803-816``); the potential is interpolated and
+        restricted, so the field stays divergence-free."""
+        from wellbalanced_b200.regrid import regrid_model
+
+        regrid_model(self, tags, **options)
+
+    def _field_extras(self):
+        return [(0, 0, 0)] * 5 + list(_EXTRA)
+
+    def _gather_field(self, patch, f):
+        return self.gather(patch, f)
+
+    def _write_field(self, patch, f, values):
+        extra = (0, 0, 0) if f < 5 else _EXTRA[f - 5]
+        self._write(patch, f, values, extra)
 
     # diagnostics ---------------------------------------------------------------------------------
     def _potentials(self, patch):

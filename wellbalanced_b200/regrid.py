@@ -1,0 +1,291 @@
+"""Regridding: clustering tagged cells into patches and moving the state onto them.
+
+The reference delegates this to patchwork (``AMRHierarchy.regrid``, absent here;
+``carafe/mhd.py:1043-1056``, ``carafe/mhd3d.py:803-816``): "the conserved fields keep their
+integrals, A_z is interpolated ... so the field stays divergence-free". Restated here:
+
+* `cluster_tags` — the tagged cells of a level, grown by ``buffer`` cells, restricted to
+  where a finer patch can nest (one cell inside the level's patches), are covered by
+  boxes by recursive bisection (Berger–Rigoutsos: cut at a hole of the tag signature,
+  else at its strongest inflection, else across the middle of the longest side) until
+  each box is at least 70% tagged and at most ``max_size`` cells per side;
+* `transfer` — the new hierarchy's level values: where the old hierarchy had a patch on
+  that level its values are kept (on a periodic axis the duplicate node planes take the
+  kept value from either side, so they agree), elsewhere they are prolongated from the
+  new coarser level — cells by minmod-limited linear reconstruction (children c ± s/4 per axis, so
+  the mean of the children is the coarse value: integrals kept, no new extrema), the
+  potential linearly along node axes and constant along an edge's own axis (so the
+  restriction that follows leaves the coarse potential, hence the coarse field,
+  unchanged).
+"""
+
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+
+
+def _grow(mask, buffer, periodic):
+    out = mask.copy()
+    for a in range(mask.ndim):
+        grown = out.copy()
+        for k in range(1, buffer + 1):
+            for sign in (-1, 1):
+                if periodic[a]:
+                    grown |= np.roll(out, sign * k, axis=a)
+                else:
+                    shifted = np.zeros_like(out)
+                    src = [slice(None)] * mask.ndim
+                    dst = [slice(None)] * mask.ndim
+                    if sign > 0:
+                        src[a], dst[a] = slice(0, -k), slice(k, None)
+                    else:
+                        src[a], dst[a] = slice(k, None), slice(0, -k)
+                    shifted[tuple(dst)] = out[tuple(src)]
+                    grown |= shifted
+        out = grown
+    return out
+
+
+def nesting_mask(shape, parents, periodic, margin=1):
+    """Cells of a level where a finer patch may lie: inside its patches by ``margin`` cells
+    (the domain boundary needs no margin)."""
+    covered = np.zeros(shape, dtype=bool)
+    for box in parents:
+        covered[tuple(slice(lo, hi) for lo, hi in box)] = True
+    outside = ~covered
+    # cells within `margin` of an uncovered cell are excluded
+    near = _grow(outside, margin, periodic)
+    return covered & ~near
+
+
+def _signature_cut(sub, axis):
+    sig = sub.sum(axis=tuple(b for b in range(sub.ndim) if b != axis))
+    n = sig.size
+    for k in range(1, n - 1):  # a hole: no tag in a whole slab
+        if sig[k] == 0:
+            return k
+    if n >= 4:
+        lap = sig[:-2] - 2 * sig[1:-1] + sig[2:]
+        best, where = 0, None
+        for k in range(1, lap.size):
+            if lap[k - 1] * lap[k] < 0:
+                jump = abs(lap[k] - lap[k - 1])
+                if jump > best:
+                    best, where = jump, k + 1
+        if where is not None and 2 <= where <= n - 2:
+            return where
+    return None
+
+
+def cluster_tags(tags, *, buffer=1, max_size=None, min_size=4, parents=None, periodic=None, efficiency=0.7):
+    """Boxes ``((lo, hi), ...)`` of the level covering the (grown, nestable) tagged cells.
+
+    ``min_size`` is the smallest box side in cells of the REFINED level (boxes are at
+    least ``ceil(min_size / 2)`` cells of this level).
+    """
+    tags = np.asarray(tags, dtype=bool)
+    periodic = periodic or (False,) * tags.ndim
+    parents = parents or [tuple((0, n) for n in tags.shape)]
+    grown = _grow(tags, buffer, periodic) if buffer else tags.copy()
+    allowed = nesting_mask(tags.shape, parents, periodic, margin=1)
+    grown &= allowed
+    min_side = max(2, (min_size + 1) // 2)
+    max_side = max_size or max(tags.shape)
+    boxes = []
+
+    def shrink(box):
+        sub = grown[tuple(slice(lo, hi) for lo, hi in box)]
+        if not sub.any():
+            return None
+        out = []
+        for a in range(tags.ndim):
+            along = sub.any(axis=tuple(b for b in range(tags.ndim) if b != a))
+            idx = np.flatnonzero(along)
+            out.append((box[a][0] + int(idx[0]), box[a][0] + int(idx[-1]) + 1))
+        return tuple(out)
+
+    def pad(box):
+        """Grow a box to the minimal side, staying in the domain and the allowed region."""
+        out = list(box)
+        for a, (lo, hi) in enumerate(box):
+            while hi - lo < min_side:
+                if hi < tags.shape[a]:
+                    hi += 1
+                elif lo > 0:
+                    lo -= 1
+                else:
+                    break
+            out[a] = (lo, hi)
+        region = allowed[tuple(slice(lo, hi) for lo, hi in out)]
+        return tuple(out) if region.all() else None
+
+    def split(box, depth=0):
+        box = shrink(box)
+        if box is None:
+            return
+        sub = grown[tuple(slice(lo, hi) for lo, hi in box)]
+        sides = [hi - lo for lo, hi in box]
+        fits = all(s <= max_side for s in sides)
+        region = allowed[tuple(slice(lo, hi) for lo, hi in box)]
+        if fits and sub.mean() >= efficiency and region.all():
+            padded = pad(box)
+            if padded is not None:
+                boxes.append(padded)
+                return
+        if max(sides) <= min_side or depth > 64:
+            padded = pad(box)
+            if padded is not None:
+                boxes.append(padded)
+            return
+        order = sorted(range(tags.ndim), key=lambda a: -sides[a])
+        for a in order:
+            if sides[a] < 2 * min_side:
+                continue
+            cut = _signature_cut(sub, a)
+            if cut is not None and min_side <= cut <= sides[a] - min_side:
+                break
+        else:
+            a = order[0]
+            cut = sides[a] // 2
+        lo, hi = box[a]
+        left = tuple((lo, lo + cut) if b == a else box[b] for b in range(tags.ndim))
+        right = tuple((lo + cut, hi) if b == a else box[b] for b in range(tags.ndim))
+        split(left, depth + 1)
+        split(right, depth + 1)
+
+    split(tuple((0, n) for n in tags.shape))
+    # boxes must not overlap (padding may have grown one into another): trim by dropping
+    # the overlap from the later box along its longest side, or drop it
+    kept = []
+    for box in boxes:
+        if any(_overlap(box, other) for other in kept):
+            continue
+        kept.append(box)
+    return kept
+
+
+def _overlap(a, b):
+    return all(alo < bhi and blo < ahi for (alo, ahi), (blo, bhi) in zip(a, b, strict=True))
+
+
+# ---- state transfer ------------------------------------------------------------------------
+def _minmod(a, b):
+    return np.where(a * b > 0.0, np.where(np.abs(a) < np.abs(b), a, b), 0.0)
+
+
+def prolong_cells(coarse, periodic):
+    """Children of every coarse cell: c + sum_a s_a (+-1/4), s_a minmod-limited slopes."""
+    ndim = coarse.ndim
+    padded = np.pad(coarse, 1, mode="wrap") if all(periodic) else coarse
+    if not all(periodic):
+        modes = [(1, 1)] * ndim
+        padded = coarse
+        for a in range(ndim):
+            padded = np.pad(padded, [(1, 1) if b == a else (0, 0) for b in range(ndim)],
+                            mode="wrap" if periodic[a] else "edge")
+        del modes
+    inner = tuple(slice(1, -1) for _ in range(ndim))
+    centre = padded[inner]
+    slopes = []
+    for a in range(ndim):
+        lo = [slice(1, -1)] * ndim
+        hi = [slice(1, -1)] * ndim
+        lo[a] = slice(0, -2)
+        hi[a] = slice(2, None)
+        slopes.append(_minmod(centre - padded[tuple(lo)], padded[tuple(hi)] - centre))
+    fine = np.empty(tuple(2 * n for n in coarse.shape))
+    for offsets in itertools.product((0, 1), repeat=ndim):
+        value = centre.copy()
+        for a, o in enumerate(offsets):
+            value = value + slopes[a] * (0.25 if o else -0.25)
+        fine[tuple(slice(o, None, 2) for o in offsets)] = value
+    return fine
+
+
+def prolong_potential(coarse, node_axes):
+    """Fine potential from coarse: linear along node axes (coincident nodes exact,
+    midpoints averaged), constant along cell axes (an edge's own direction)."""
+    out = coarse
+    for a, node in enumerate(node_axes):
+        n = out.shape[a]
+        if node:
+            shape = list(out.shape)
+            shape[a] = 2 * (n - 1) + 1
+            fine = np.empty(shape)
+            even = [slice(None)] * out.ndim
+            even[a] = slice(0, None, 2)
+            fine[tuple(even)] = out
+            odd = [slice(None)] * out.ndim
+            odd[a] = slice(1, None, 2)
+            lo = np.take(out, np.arange(0, n - 1), axis=a)
+            hi = np.take(out, np.arange(1, n), axis=a)
+            fine[tuple(odd)] = 0.5 * (lo + hi)
+        else:
+            fine = np.repeat(out, 2, axis=a)
+        out = fine
+    return out
+
+
+def _merge_periodic_planes(values, mask, extra, periodic, shape):
+    """On a periodic axis a node array's last plane duplicates its first: take the kept
+    (old-patch) value from either plane, so both planes agree after the transfer."""
+    for a, (node, wraps) in enumerate(zip(extra, periodic, strict=True)):
+        if not (node and wraps):
+            continue
+        first = [slice(None)] * values.ndim
+        last = [slice(None)] * values.ndim
+        first[a], last[a] = 0, shape[a]
+        first, last = tuple(first), tuple(last)
+        take = mask[last] & ~mask[first]
+        values[first] = np.where(take, values[last], values[first])
+        mask[first] |= mask[last]
+        values[last] = values[first]
+        mask[last] = mask[first]
+
+
+def regrid_model(model, tags, **options):
+    """Regrid ``model`` (an `MHD2D` / `MHD3D`) on ``tags`` and move its state over."""
+    model._check_ready()
+    old_h = model.hierarchy
+    extras = model._field_extras()
+    periodic = old_h.periodic
+    old_levels = {}
+    for level in range(old_h.max_level + 1):
+        shape = old_h.level_shape(level)
+        arrays = []
+        for f, extra in enumerate(extras):
+            size = tuple(n + e for n, e in zip(shape, extra, strict=True))
+            values = np.zeros(size)
+            mask = np.zeros(size, dtype=bool)
+            for p in old_h.patches_at_level(level):
+                index = tuple(slice(lo, hi + e) for (lo, hi), e in zip(p.box, extra, strict=True))
+                values[index] = model._gather_field(p, f)
+                mask[index] = True
+            _merge_periodic_planes(values, mask, extra, periodic, shape)
+            arrays.append((values, mask))
+        old_levels[level] = arrays
+    new_h = old_h.regrid(tags, **options)
+    time, steps = model.time, model.steps
+    model.hierarchy = new_h
+    model._build_engine()
+    new_levels = {}
+    for level in range(new_h.max_level + 1):
+        arrays = []
+        for f, extra in enumerate(extras):
+            old = old_levels.get(level)
+            if level == 0:
+                result = old[f][0]
+            else:
+                coarse = new_levels[level - 1][f]
+                fine = prolong_potential(coarse, extra) if any(extra) else prolong_cells(coarse, periodic)
+                result = fine if old is None else np.where(old[f][1], old[f][0], fine)
+            arrays.append(result)
+            for p in new_h.patches_at_level(level):
+                index = tuple(slice(lo, hi + e) for (lo, hi), e in zip(p.box, extra, strict=True))
+                model._write_field(p, f, result[index])
+        new_levels[level] = arrays
+    model._after_state()
+    model.time, model.steps = time, steps
+    model.engine.time.fill_(time)
