@@ -141,6 +141,22 @@ int wb_reflux_apply(int precision, void* pool, const void* patches, const void* 
 /* Sizes of the engine structs, for callers that mirror them. */
 int wb_struct_sizes(int64_t* sizes_host, int n);
 
+/* wb_rate without a caller-provided key buffer: allocates nothing. No counterpart in the
+ * reference (its rate kernel returns into a caller-allocated out[2]). Same work list and
+ * state as wb_rate; the per-instance keys live in a static device array of 4096
+ * instances (64 KiB per device), and the result is decoded into `out` (device float64,
+ * 2 * ninstances): out[2k] = largest rate, out[2k+1] = smallest density of instance k.
+ * - ninstances > 4096 returns WB_TOO_LARGE with a message (use wb_rate for more);
+ * - every patch's instance index must be below ninstances (as for wb_rate);
+ * - nothing must start at zero: each call initialises the slots it uses;
+ * - the first call on a device resolves the scratch address (cudaGetSymbolAddress) and
+ *   caches it; make that call before any stream capture that includes this function;
+ * - all calls on a device share the scratch: calls in flight at the same time (other
+ *   streams, other threads) race and may return wrong values. */
+int wb_rate_static(int precision, int ndim, const void* state, const void* patches, int npatches,
+                   const int* chunk_patch, const int* chunk_start, int nchunks, double b0x, double b0y,
+                   double b0z, double gamma, int ninstances, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,8 @@ SIGNATURES = {
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],
     "wb_finalize_dt": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_rate_static": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double,
+                       c_int, c_dp, c_dp],
     "wb_copy_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_interp_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
