@@ -306,6 +306,8 @@ def main():
         launch_s = statistics.mean(stage_ms) / 1e3 if stage_ms else float("nan")
         achieved = BYTES_PER_ZONE_UPDATE / 2 * cells / launch_s / 1e9
         traffic = profile_traffic()
+        if traffic is not None:
+            traffic *= cells / 256**3  # the summary's figure is per launch at 256^3
         line = {
             "metric": METRIC,
             "value": value,
