@@ -33,24 +33,30 @@ __global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool,
   const int nx = P.n[0], ny = P.n[1];
   const S* src = pool + P.off;
   const int64_t pitch = P.pitch0, fs = P.fstride;
+  using M = Math<S>;
   const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+  const S idx = M::inv(dx), idy = M::inv(dy);
   const S g = S(gamma), bx0 = S(b0x), by0 = S(b0y);
   double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
-  const int64_t total = int64_t(nx) * ny;
-  const int64_t start = chunk_start[blockIdx.x];
+  // work-list indices are 32-bit (chunk_start is int): 32-bit index arithmetic
+  const unsigned total = unsigned(nx) * unsigned(ny);
+  const unsigned start = unsigned(chunk_start[blockIdx.x]);
   for (int s = 0; s < 8; ++s) {
-    const int64_t t = start + int64_t(s) * blockDim.x + threadIdx.x;
+    const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
     if (t >= total) break;
-    const int i = int(t / ny) + kHalo, j = int(t % ny) + kHalo;
+    const unsigned row = t / unsigned(ny);
+    const int i = int(row) + kHalo, j = int(t - row * unsigned(ny)) + kHalo;
     const int64_t c = int64_t(i) * pitch + j;
     const S* A = src + 6 * fs;
     const S r = src[c];
-    const S u = src[fs + c] / r, v = src[2 * fs + c] / r, w = src[3 * fs + c] / r;
-    const S bx = S(0.5) * ((A[c + 1] - A[c]) / dy + bx0 + ((A[c + pitch + 1] - A[c + pitch]) / dy + bx0));
-    const S by = S(0.5) * (-(A[c + pitch] - A[c]) / dx + by0 + (-(A[c + pitch + 1] - A[c + 1]) / dx + by0));
+    const S ir = M::inv(r);
+    const S u = M::div(src[fs + c], r, ir), v = M::div(src[2 * fs + c], r, ir), w = M::div(src[3 * fs + c], r, ir);
+    const S bx = S(0.5) * (M::div(A[c + 1] - A[c], dy, idy) + bx0 + (M::div(A[c + pitch + 1] - A[c + pitch], dy, idy) + bx0));
+    const S by = S(0.5) * (-M::div(A[c + pitch] - A[c], dx, idx) + by0 + (-M::div(A[c + pitch + 1] - A[c + 1], dx, idx) + by0));
     const S bz = src[5 * fs + c];
     const S p = (g - S(1)) * (src[4 * fs + c] - S(0.5) * r * (u * u + v * v + w * w) - S(0.5) * (bx * bx + by * by + bz * bz));
-    const S rate = (rabs(u) + fast_speed(r, p, bx, by, bz, g)) / dx + (rabs(v) + fast_speed(r, p, by, bx, bz, g)) / dy;
+    const S rate = M::div(rabs(u) + fast_speed(r, p, bx, by, bz, g), dx, idx) +
+                   M::div(rabs(v) + fast_speed(r, p, by, bx, bz, g), dy, idy);
     largest = fmax(largest, double(rate));
     smallest = fmin(smallest, double(r));
   }
@@ -67,33 +73,40 @@ __global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool,
   const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
   const S* src = pool + P.off;
   const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
+  using M = Math<S>;
   const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+  const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
   const S g = S(gamma);
   double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
-  const int64_t total = int64_t(nx) * ny * nz;
-  const int64_t start = chunk_start[blockIdx.x];
+  // work-list indices are 32-bit (chunk_start is int): 32-bit index arithmetic
+  const unsigned total = unsigned(nx) * unsigned(ny) * unsigned(nz);
+  const unsigned start = unsigned(chunk_start[blockIdx.x]);
   for (int s = 0; s < 8; ++s) {
-    const int64_t t = start + int64_t(s) * blockDim.x + threadIdx.x;
+    const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
     if (t >= total) break;
-    const int i = int(t / (int64_t(ny) * nz)) + kHalo;
-    const int j = int((t / nz) % ny) + kHalo;
-    const int k = int(t % nz) + kHalo;
+    const unsigned line = t / unsigned(nz);
+    const unsigned plane = line / unsigned(ny);
+    const int i = int(plane) + kHalo;
+    const int j = int(line - plane * unsigned(ny)) + kHalo;
+    const int k = int(t - line * unsigned(nz)) + kHalo;
     const int64_t o = int64_t(i) * p0 + int64_t(j) * p1 + k;
     const S* Ax = src + 5 * fs;
     const S* Ay = src + 6 * fs;
     const S* Az = src + 7 * fs;
-    const S bxl = (Az[o + p1] - Az[o]) / dy - (Ay[o + 1] - Ay[o]) / dz + S(b0x);
-    const S bxh = (Az[o + p0 + p1] - Az[o + p0]) / dy - (Ay[o + p0 + 1] - Ay[o + p0]) / dz + S(b0x);
-    const S byl = (Ax[o + 1] - Ax[o]) / dz - (Az[o + p0] - Az[o]) / dx + S(b0y);
-    const S byh = (Ax[o + p1 + 1] - Ax[o + p1]) / dz - (Az[o + p1 + p0] - Az[o + p1]) / dx + S(b0y);
-    const S bzl = (Ay[o + p0] - Ay[o]) / dx - (Ax[o + p1] - Ax[o]) / dy + S(b0z);
-    const S bzh = (Ay[o + p0 + 1] - Ay[o + 1]) / dx - (Ax[o + p1 + 1] - Ax[o + 1]) / dy + S(b0z);
+    const S bxl = M::div(Az[o + p1] - Az[o], dy, idy) - M::div(Ay[o + 1] - Ay[o], dz, idz) + S(b0x);
+    const S bxh = M::div(Az[o + p0 + p1] - Az[o + p0], dy, idy) - M::div(Ay[o + p0 + 1] - Ay[o + p0], dz, idz) + S(b0x);
+    const S byl = M::div(Ax[o + 1] - Ax[o], dz, idz) - M::div(Az[o + p0] - Az[o], dx, idx) + S(b0y);
+    const S byh = M::div(Ax[o + p1 + 1] - Ax[o + p1], dz, idz) - M::div(Az[o + p1 + p0] - Az[o + p1], dx, idx) + S(b0y);
+    const S bzl = M::div(Ay[o + p0] - Ay[o], dx, idx) - M::div(Ax[o + p1] - Ax[o], dy, idy) + S(b0z);
+    const S bzh = M::div(Ay[o + p0 + 1] - Ay[o + 1], dx, idx) - M::div(Ax[o + p1 + 1] - Ax[o + 1], dy, idy) + S(b0z);
     const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
     const S r = src[o];
-    const S u = src[fs + o] / r, v = src[2 * fs + o] / r, w = src[3 * fs + o] / r;
+    const S ir = M::inv(r);
+    const S u = M::div(src[fs + o], r, ir), v = M::div(src[2 * fs + o], r, ir), w = M::div(src[3 * fs + o], r, ir);
     const S p = (g - S(1)) * (src[4 * fs + o] - S(0.5) * r * (u * u + v * v + w * w) - S(0.5) * (bx * bx + by * by + bz * bz));
-    const S rate = (rabs(u) + fast_speed(r, p, bx, by, bz, g)) / dx + (rabs(v) + fast_speed(r, p, by, bz, bx, g)) / dy +
-                   (rabs(w) + fast_speed(r, p, bz, bx, by, g)) / dz;
+    const S rate = M::div(rabs(u) + fast_speed(r, p, bx, by, bz, g), dx, idx) +
+                   M::div(rabs(v) + fast_speed(r, p, by, bz, bx, g), dy, idy) +
+                   M::div(rabs(w) + fast_speed(r, p, bz, bx, by, g), dz, idz);
     largest = fmax(largest, double(rate));
     smallest = fmin(smallest, double(r));
   }

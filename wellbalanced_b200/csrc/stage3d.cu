@@ -31,6 +31,11 @@ struct Tile3D {
   static constexpr int TY = 16, TZ = 16;
 };
 
+// Hint that a global value will be read soon: fetch its line into L2.
+__device__ __forceinline__ void prefetch_l2(const void* ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 template <typename S>
 __device__ __forceinline__ bool bad3(S r, S u, S v, S w, S p, S bx, S by, S bz) {
   if (!(r > S(0) && p > S(0))) return true;
@@ -109,6 +114,17 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   unsigned bad = 0;
 
   for (int p = x0 - 3; p <= xe; ++p) {
+    // prefetch into L2 what phase C of the next plane reads from global memory: the
+    // cells and edges of its column in the input state (read two planes ago, usually
+    // still cached) and in the Heun base state (not read before)
+    if (tid < NCORE && p + 1 >= x0 && p < xe) {
+      const int gj = y0 + cj, gk = z0 + ck;
+      const int64_t o = int64_t(p + kHalo) * p0 + int64_t(gj + kHalo) * p1 + (gk + kHalo);
+      if (base_state) {
+#pragma unroll
+        for (int f = 0; f < 8; ++f) prefetch_l2(base_state + f * fs + o);
+      }
+    }
     // A: load cell plane c = p + 1 ------------------------------------------------------
     {
       const int c = p + 1;

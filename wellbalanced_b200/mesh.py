@@ -332,6 +332,8 @@ class Layout:
         patch, start = [], []
         for p in self.h.patches:
             cells = int(np.prod(p.shape))
+            if cells + per >= 2**31:  # the rate kernels index a patch's cells in 32 bits
+                raise ValueError(f"patch {p.box} has {cells} cells; split the level into patches below 2**31 cells")
             for s in range(0, cells, per):
                 patch.append(p.index)
                 start.append(s)
