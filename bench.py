@@ -1,19 +1,30 @@
-"""Benchmark of the B200 ideal-MHD step: zone-updates/s of the 3D decaying-turbulence box.
+"""Benchmark of the B200 ideal-MHD step: zone-updates/s.
 
-Workload (one GPU): 3D decaying turbulence on a periodic 256^3 grid, MC-limited PLM +
-HLLD + CT-contact vector-potential constrained transport, SSP-RK2 at CFL 0.3, float32
-state (pressure recovery in float64); seeded Gaussian random velocity and potential
-fields with a k^-2 spectrum on 1 <= |k| <= 8, rms Mach 1, rms |B| = 1. One zone-update is
-one cell advanced by one full RK2 step; a bench step is one RK2 step of the whole box.
-With N GPUs (torchrun) every rank advances its own box (replicas, seeded by rank: weak
-scaling, no data-path collective); `value` is the zone-updates of all ranks over the
-slowest rank's time.
+Workloads (``--workload``; one zone-update = one cell advanced by one full RK2 step):
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--cells 256] [--impl reference]
+* ``turbulence`` (default): 3D decaying turbulence on a periodic 256^3 grid,
+  MC-limited PLM + HLLD + CT-contact vector-potential constrained transport, SSP-RK2 at
+  CFL 0.3, float32 state (pressure recovery in float64); seeded Gaussian random velocity
+  and potential fields with a k^-2 spectrum on 1 <= |k| <= 8, rms Mach 1, rms |B| = 1.
+* ``batch``: 4096 independent periodic 2D Orszag-Tang problems (sides drawn from
+  {32, 48, ..., 256}, field and velocity amplitudes scaled by seeded factors in
+  [0.5, 1.5]), each at its own CFL 0.4 step, float32; all instances advanced by one launch
+  per kernel (the timed steps launch directly; the same steps replayed from a CUDA graph
+  are reported beside them).
+* ``harris``: a 2D Harris current sheet on [-1, 1] x [-2, 2], base 128 x 256, periodic in
+  x and outflow in y, refined three times on the current (|J| dx > 0.01, patches of at
+  most 32 cells a side: 177 patches), float32 with float64 refluxing; every level
+  advances at the finest CFL 0.4 step, all patches in one launch per kernel.
 
-`--impl reference` times the CPU implementation of the same step (the NumPy
-restatement of the reference's MHD3D step, the reference being pure Python) on all
-host cores, each process a bounded 32^3 sample of the workload.
+With N GPUs (torchrun) every rank advances its own copy of the workload (replicas,
+seeded by rank: weak scaling, no data-path collective); `value` is the zone-updates of
+all ranks over the slowest rank's time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload turbulence|batch|harris]
+
+`--impl reference` times the CPU implementation of the same step (the NumPy restatement
+of the reference's step, the reference being pure Python) on all host cores, each process
+a bounded sample of the workload per bench step.
 """
 
 from __future__ import annotations
@@ -32,54 +43,360 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "zone-updates/s on 1 B200 (batched FP32 vs plain FP64) at stated L1 err; % HBM roofline"
 UNIT = "zone-updates/s"
-BYTES_PER_ZONE_UPDATE = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
-WORKLOAD = ("3D decaying turbulence, periodic {n}^3, MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, "
-            "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1")
 
 
 def parse():
-    parser = argparse.ArgumentParser()
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=100)
     parser.add_argument("--warmup", type=int, default=5)
-    parser.add_argument("--cells", type=int, default=256)
+    parser.add_argument("--workload", default="turbulence", choices=["turbulence", "batch", "harris"])
+    parser.add_argument("--cells", type=int, default=256, help="turbulence: cells per side")
+    parser.add_argument("--count", type=int, default=4096, help="batch: number of instances")
     parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-accuracy", action="store_true")
-    parser.add_argument("--lx", type=int, default=32)
     parser.add_argument("--no-plain", action="store_true")
+    parser.add_argument("--lx", type=int, default=32, help="turbulence: x-planes per tile")
     return parser.parse_args()
 
 
-# ---- CPU side ---------------------------------------------------------------------------------
-def _cpu_sample(args):
-    """One process's bounded sample: the oracle MHD3D step on a small turbulence box."""
-    n, steps, seed = args
-    from oracle.mesh import Hierarchy
-    from oracle.mhd3d import MHD3D
-    from wellbalanced_b200.problems import turbulence_3d
+# ---- workloads ---------------------------------------------------------------------------------
+HARRIS_BASE = (128, 256)
+HARRIS_BOUNDS = ((-1.0, 1.0), (-2.0, 2.0))
+HARRIS_LEVELS = 3
+HARRIS_THRESHOLD = 0.01
+HARRIS_PATCH = 16  # coarse cells a side, so refined patches of at most 32 cells
 
-    rho, velocity, p, potential = turbulence_3d(n, seed=seed)
-    model = MHD3D(Hierarchy((n,) * 3, ((0.0, 1.0),) * 3, (True,) * 3), limiter="mc", cfl=0.3)
-    model.set_state(rho, velocity, p, vector_potential=potential)
+
+def _harris_model(cls, precision, seed, *, levels=HARRIS_LEVELS, base=HARRIS_BASE, **options):
+    """The Harris-sheet workload: set on the base level, then refined on the current."""
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.problems import harris_sheet
+
+    density, pressure, potential = harris_sheet(*base, seed=seed, bounds=HARRIS_BOUNDS)
+    mesh = AMRHierarchy(base, HARRIS_BOUNDS, periodic=(True, False))
+    model = cls(mesh, limiter="mc", cfl=0.4, precision=precision, **options)
+    model.set_state(density, (0.0, 0.0, 0.0), pressure, vector_potential=potential)
+    for _ in range(levels):
+        model.regrid(model.current_tags(HARRIS_THRESHOLD, levels=levels), max_patch_size=HARRIS_PATCH)
+    return model
+
+
+def _harris_on(mesh, cls, precision, seed, **options):
+    """The Harris-sheet state set directly on a given hierarchy (all levels)."""
+    from wellbalanced_b200.problems import harris_sheet
+
+    density, pressure, potential = harris_sheet(*mesh.shape, seed=seed, bounds=HARRIS_BOUNDS)
+    model = cls(mesh, limiter="mc", cfl=0.4, precision=precision, **options)
+    model.set_state(density, (0.0, 0.0, 0.0), pressure, vector_potential=potential)
+    return model
+
+
+def _copy_mesh(mesh):
+    from wellbalanced_b200.mesh import AMRHierarchy
+
+    out = AMRHierarchy(mesh.shape, mesh.bounds, mesh.periodic)
+    for p in mesh.patches:
+        if p.level:
+            out.add_patch(p.level, p.box)
+    return out
+
+
+def _time_steps(step, steps):
+    """Device seconds of `steps` calls of `step` after one warm-up call (CUDA events)."""
+    import torch
+
+    step()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        step()
+    end.record()
+    torch.cuda.synchronize()
+    return start.elapsed_time(end) / 1e3
+
+
+def _rel_l1(ref, low, patches, steps):
+    """Relative L1 of density and energy of `low` against `ref` over the given patches."""
+    import torch
+
+    out = {"steps": steps,
+           "against": "float64 device step from the same state (float64 step == reference to 1e-12 in the tests)"}
+    for key, f in (("density", 0), ("energy", 4)):
+        num = den = 0.0
+        for pr, pl in patches:
+            a = ref._read(pr, f).to(torch.float64)
+            b = low._read(pl, f).to(torch.float64)
+            num += float(torch.sum(torch.abs(b - a)))
+            den += float(torch.sum(torch.abs(a)))
+        out[f"rel_l1_{key}"] = num / den
+    return out
+
+
+class Turbulence:
+    kernel = "wb::stage3d_kernel<float, 2>"
+    bytes_per_zone_update = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
+
+    def __init__(self, args, rank):
+        from wellbalanced_b200.mhd3d import MHD3D
+
+        self.n = args.cells
+        self.rank = rank
+        self.lx = args.lx
+        self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=args.lx)
+        self.engine = self.model.engine
+        self.cells = self.n**3
+
+    def advance(self, steps):
+        self.model.advance(steps, check=False)
+
+    def config(self):
+        eng = self.engine
+        return {
+            "workload": (f"3D decaying turbulence, periodic {self.n}^3, MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, "
+                         "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1"),
+            "cells_per_gpu": self.cells,
+            "tile": {"y": eng.layout.tile_shape[0], "z": eng.layout.tile_shape[1], "x_planes": self.lx},
+        }
+
+    def plain(self, steps=3):
+        """zone-updates/s of the plain float64 GPU step (`wellbalanced_b200.plain.PlainMHD3D`)."""
+        from wellbalanced_b200.mesh import AMRHierarchy
+        from wellbalanced_b200.plain import PlainMHD3D
+        from wellbalanced_b200.problems import turbulence_3d
+
+        n = self.n
+        rho, velocity, p, potential = turbulence_3d(n, seed=self.rank)
+        model = PlainMHD3D(AMRHierarchy((n,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3)
+        model.set_state(rho, velocity, p, vector_potential=potential)
+        seconds = _time_steps(model.step, steps)
+        return {"value": self.cells * steps / seconds, "unit": UNIT, "ms_per_step": 1e3 * seconds / steps,
+                "steps": steps,
+                "what": "PlainMHD3D: the reference MHD3D dataflow on the device, float64, per-kernel, intermediates in HBM"}
+
+    def accuracy(self, steps=10):
+        import torch
+
+        from wellbalanced_b200.mhd3d import MHD3D
+
+        ref = MHD3D.turbulence(self.n, seed=self.rank, precision=64)
+        low = MHD3D.turbulence(self.n, seed=self.rank, precision=32)
+        for _ in range(steps):
+            low.step(ref.step())
+        out = _rel_l1(ref, low, list(zip(ref.hierarchy.patches, low.hierarchy.patches, strict=True)), steps)
+        out["div_b"] = low.divergence()
+        del ref, low
+        torch.cuda.empty_cache()
+        return out
+
+
+class BatchWorkload:
+    kernel = "wb::stage2d_kernel<float, 2>"
+    bytes_per_zone_update = 5 * 7 * 4  # 5 state passes x 7 values (6 cell + 1 node) x float32
+
+    def __init__(self, args, rank):
+        from wellbalanced_b200.batch import Batch
+
+        self.count = args.count
+        self.rank = rank
+        self.batch = Batch.orszag_tang(self.count, seed=rank, precision=32)
+        self.engine = self.batch.engine
+        self.cells = self.batch.cells
+
+    def advance(self, steps):
+        for _ in range(steps):
+            self.batch._step_launches()
+        self.batch.steps += steps
+
+    def graph_timing(self, steps):
+        """ms per step of the same steps replayed from one captured CUDA graph."""
+        self.batch.capture()
+        seconds = _time_steps(lambda: self.batch.advance(1, check=False), steps)
+        self.batch._graph = None
+        return 1e3 * seconds / steps
+
+    def config(self):
+        sides = [s for s, _ in self.batch.sides]
+        return {
+            "workload": (f"{self.count} independent periodic 2D Orszag-Tang problems, sides from {{32, 48, ..., 256}} "
+                         f"(seed {self.rank}), amplitudes x U[0.5, 1.5], MC-PLM + HLLD + CT, SSP-RK2, per-instance "
+                         "CFL 0.4 dt, float32 state, one launch per kernel for all instances"),
+            "cells_per_gpu": self.cells,
+            "instances": self.count,
+            "mean_side": float(sum(sides) / len(sides)),
+            "tile": {"x": self.engine.layout.tile_shape[0], "y": self.engine.layout.tile_shape[1]},
+        }
+
+    def plain(self, count=8, steps=2):
+        """The plain float64 GPU step looped over a seeded subset of the instances."""
+        from wellbalanced_b200.mesh import AMRHierarchy
+        from wellbalanced_b200.plain import PlainMHD2D
+        from wellbalanced_b200.problems import orszag_tang_2d, orszag_tang_sizes
+
+        sides, bf, vf = orszag_tang_sizes(self.count, seed=self.rank)
+        models, cells = [], 0
+        for k in range(count):
+            n = int(sides[k])
+            model = PlainMHD2D(AMRHierarchy((n, n), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True)), limiter="mc",
+                               cfl=0.4)
+            model.set_conserved(*orszag_tang_2d(n, bf[k], vf[k]))
+            models.append(model)
+            cells += n * n
+
+        def step_all():
+            for model in models:
+                model.step()
+
+        seconds = _time_steps(step_all, steps)
+        return {"value": cells * steps / seconds, "unit": UNIT, "ms_per_step": 1e3 * seconds / steps, "steps": steps,
+                "what": f"PlainMHD2D (the reference MHD2D dataflow per kernel, float64) looped over the first {count} "
+                        "instances of the batch"}
+
+    def accuracy(self, steps=10):
+        import torch
+
+        from wellbalanced_b200.mesh import AMRHierarchy
+        from wellbalanced_b200.mhd import MHD2D
+        from wellbalanced_b200.problems import orszag_tang_2d, orszag_tang_sizes
+
+        sides, bf, vf = orszag_tang_sizes(self.count, seed=self.rank)
+        k = int(max(range(len(sides)), key=lambda i: sides[i]))
+        n = int(sides[k])
+        models = []
+        for precision in (64, 32):
+            model = MHD2D(AMRHierarchy((n, n), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True)), limiter="mc",
+                          cfl=0.4, precision=precision)
+            model.set_conserved(*orszag_tang_2d(n, bf[k], vf[k]))
+            models.append(model)
+        ref, low = models
+        for _ in range(steps):
+            low.step(ref.step())
+        out = _rel_l1(ref, low, list(zip(ref.hierarchy.patches, low.hierarchy.patches, strict=True)), steps)
+        out["instance"] = f"{n}^2 (instance {k})"
+        out["div_b"] = low.divergence()
+        del ref, low, models
+        torch.cuda.empty_cache()
+        return out
+
+
+class Harris:
+    kernel = "wb::stage2d_kernel<float, 2>"
+    bytes_per_zone_update = 5 * 7 * 4
+
+    def __init__(self, args, rank):
+        from wellbalanced_b200.mhd import MHD2D
+
+        self.rank = rank
+        self.model = _harris_model(MHD2D, 32, rank)
+        self.engine = self.model.engine
+        self.cells = int(sum(p.shape[0] * p.shape[1] for p in self.model.hierarchy.patches))
+
+    def advance(self, steps):
+        self.model.advance(steps, check=False)
+
+    def config(self):
+        h = self.model.hierarchy
+        refined = [p.shape for p in h.patches if p.level]
+        return {
+            "workload": (f"2D Harris sheet on [-1,1]x[-2,2], base {HARRIS_BASE[0]}x{HARRIS_BASE[1]}, periodic x, "
+                         f"outflow y, {h.max_level} refined levels on |J| dx > {HARRIS_THRESHOLD} (patches <= "
+                         f"{2 * HARRIS_PATCH} cells a side), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.4 at the finest dx, "
+                         "float32 state with float64 refluxing, all patches in one launch per kernel"),
+            "cells_per_gpu": self.cells,
+            "patches": len(h.patches),
+            "patches_per_level": {str(lv): len(h.patches_at_level(lv)) for lv in range(h.max_level + 1)},
+            "refined_patch_sides": [min(min(s) for s in refined), max(max(s) for s in refined)] if refined else None,
+            "tile": {"x": self.engine.layout.tile_shape[0], "y": self.engine.layout.tile_shape[1]},
+        }
+
+    def plain(self, steps=2):
+        from wellbalanced_b200.plain import PlainMHD2D
+
+        model = _harris_on(_copy_mesh(self.model.hierarchy), PlainMHD2D, 64, self.rank)
+        seconds = _time_steps(model.step, steps)
+        return {"value": self.cells * steps / seconds, "unit": UNIT, "ms_per_step": 1e3 * seconds / steps,
+                "steps": steps,
+                "what": "PlainMHD2D (the reference MHD2D dataflow per kernel, float64) on the same hierarchy"}
+
+    def accuracy(self, steps=10):
+        import torch
+
+        from wellbalanced_b200.mhd import MHD2D
+
+        ref = _harris_on(_copy_mesh(self.model.hierarchy), MHD2D, 64, self.rank)
+        low = _harris_on(_copy_mesh(self.model.hierarchy), MHD2D, 32, self.rank)
+        for _ in range(steps):
+            low.step(ref.step())
+        base = list(zip(ref.hierarchy.patches_at_level(0), low.hierarchy.patches_at_level(0), strict=True))
+        out = _rel_l1(ref, low, base, steps)
+        out["against"] = "float64 device step from the same state on the same hierarchy (base level, restricted)"
+        out["div_b"] = low.divergence()
+        out["composite_div_b"] = low.composite_divergence()
+        del ref, low
+        torch.cuda.empty_cache()
+        return out
+
+
+WORKLOADS = {"turbulence": Turbulence, "batch": BatchWorkload, "harris": Harris}
+
+
+# ---- CPU legs (the oracle: NumPy restatement of the reference's step) ---------------------------
+def _cpu_sample(job):
+    """One process's bounded sample: (zone-updates, seconds) of `steps` oracle steps."""
+    workload, seed, steps, n3d = job
+    if workload == "turbulence":
+        from oracle.mesh import Hierarchy
+        from oracle.mhd3d import MHD3D
+        from wellbalanced_b200.problems import turbulence_3d
+
+        rho, velocity, p, potential = turbulence_3d(n3d, seed=seed)
+        model = MHD3D(Hierarchy((n3d,) * 3, ((0.0, 1.0),) * 3, (True,) * 3), limiter="mc", cfl=0.3)
+        model.set_state(rho, velocity, p, vector_potential=potential)
+        cells = n3d**3
+    elif workload == "batch":
+        from oracle.mesh import Hierarchy
+        from oracle.mhd2d import MHD2D
+        from wellbalanced_b200.problems import orszag_tang_2d, orszag_tang_sizes
+
+        sides, bf, vf = orszag_tang_sizes(seed + 1, seed=0)
+        n = int(sides[seed])
+        model = MHD2D(Hierarchy((n, n), ((0.0, 1.0), (0.0, 1.0)), (True, True)), limiter="mc", cfl=0.4)
+        model.set_conserved(*orszag_tang_2d(n, bf[seed], vf[seed]))
+        cells = n * n
+    else:
+        from oracle.mesh import Hierarchy
+        from oracle.mhd2d import MHD2D
+        from wellbalanced_b200.problems import harris_sheet
+
+        density, pressure, potential = harris_sheet(*HARRIS_BASE, seed=seed, bounds=HARRIS_BOUNDS)
+        model = MHD2D(Hierarchy(HARRIS_BASE, HARRIS_BOUNDS, (True, False)), limiter="mc", cfl=0.4)
+        model.set_state(density, (0.0, 0.0, 0.0), pressure, vector_potential=potential)
+        cells = HARRIS_BASE[0] * HARRIS_BASE[1]
+    if steps == 0:
+        return 0, 0.0
     model.step()  # warm-up
     start = time.perf_counter()
     for _ in range(steps):
         model.step()
-    return n**3 * steps, time.perf_counter() - start
+    return cells * steps, time.perf_counter() - start
 
 
-def cpu_baseline(n=64, steps=3):
-    """The oracle's NumPy 3D step on one core (zone-updates/s)."""
-    cells, seconds = _cpu_sample((n, steps, 0))
-    return {
-        "value": cells / seconds,
-        "unit": UNIT,
-        "cores": 1,
-        "kind": "port",
-        "sample": f"NumPy restatement of the reference MHD3D step, 3D turbulence {n}^3, {steps} RK2 steps after 1 warm-up, 1 process",
-    }
+CPU_SAMPLES = {
+    "turbulence": "3D turbulence 64^3",
+    "batch": "the batch's first Orszag-Tang instance",
+    "harris": "the Harris sheet's 128x256 base level (unrefined)",
+}
+
+
+def cpu_baseline(workload):
+    """The oracle's step on one core (zone-updates/s), a bounded sample of the workload."""
+    cells, seconds = _cpu_sample((workload, 0, 3, 64))
+    return {"value": cells / seconds, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"NumPy restatement of the reference step, {CPU_SAMPLES[workload]}, 3 RK2 steps after 1 warm-up, "
+                      "1 process"}
 
 
 def reference_arm(args):
@@ -89,20 +406,21 @@ def reference_arm(args):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    n = 32
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        pool.map(_cpu_sample, [(n, 0, s) for s in range(cores)])  # spin up, import
+        pool.map(_cpu_sample, [(args.workload, s, 0, 32) for s in range(cores)])  # spin up, import
         per_step = []
         for step in range(args.warmup + args.steps):
             start = time.perf_counter()
-            results = pool.map(_cpu_sample, [(n, 1, s) for s in range(cores)])
+            results = pool.map(_cpu_sample, [(args.workload, s, 1, 32) for s in range(cores)])
             wall = time.perf_counter() - start
             if step >= args.warmup:
                 per_step.append((sum(c for c, _ in results), wall))
     total_cells = sum(c for c, _ in per_step)
     total_time = sum(t for _, t in per_step)
     value = total_cells / total_time
+    sample = {"turbulence": "a 32^3 turbulence box", "batch": "one Orszag-Tang instance of the batch",
+              "harris": "the 128x256 Harris base level"}[args.workload]
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -117,14 +435,14 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD.format(n=args.cells) + f"; CPU sample {n}^3 per process"},
+        "config": {"workload": f"{args.workload}; CPU sample per process: {sample}"},
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
             "cores": cores,
             "kind": "port",
-            "sample": f"{cores} processes, each one RK2 step of a {n}^3 box of the workload per bench step "
-                      "(NumPy restatement of the reference MHD3D step; the reference is pure Python)",
+            "sample": f"{cores} processes, each one RK2 step of {sample} per bench step (after a warm-up step; "
+                      "NumPy restatement of the reference step; the reference is pure Python)",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -187,15 +505,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per stage launch from the committed ncu summary, if present."""
-    path = ROOT / "profiles" / "stage3d_turbulence.md"
+PROFILES = {"turbulence": "stage3d_turbulence.md", "batch": "stage2d_batch.md", "harris": "stage2d_harris.md"}
+
+
+def profile_traffic(workload, cells):
+    """DRAM bytes per stage launch from the committed ncu summary of the workload (its
+    per-cell figure times this run's cells), or None."""
+    path = ROOT / "profiles" / PROFILES[workload]
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_launch_256:"):
+        if line.strip().startswith("traffic_bytes_per_cell_launch:"):
             try:
-                return float(line.split(":", 1)[1].split()[0])
+                return float(line.split(":", 1)[1].split()[0]) * cells
             except ValueError:
                 return None
     return None
@@ -211,9 +533,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        baseline = cpu_baseline()  # before any GPU work
+        baseline = cpu_baseline(args.workload)  # before any GPU work
 
-    import numpy as np
     import torch
     import torch.distributed as dist
 
@@ -225,12 +546,9 @@ def main():
         if world > 1:
             dist.barrier()
 
-    from wellbalanced_b200.mhd3d import MHD3D
-
-    n = args.cells
-    model = MHD3D.turbulence(n, seed=rank, precision=32, lx=args.lx)
-    eng = model.engine
-    model.advance(args.warmup)
+    work = WORKLOADS[args.workload](args, rank)
+    eng = work.engine
+    work.advance(args.warmup)
     torch.cuda.synchronize()
 
     # timed region: K RK2 steps, state resident in HBM
@@ -243,7 +561,7 @@ def main():
     time.sleep(0.3)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record()
-    model.advance(args.steps, check=False)
+    work.advance(args.steps)
     end.record()
     torch.cuda.synchronize()
     barrier()
@@ -258,14 +576,18 @@ def main():
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     seconds = float(t.item())
-    cells = n**3
+    cells = work.cells
     value = world * cells * args.steps / seconds
 
-    # end to end through the public API with host buffers: per step, the state pool is
-    # copied from pinned host memory, advanced one step and copied back
+    graph_ms = work.graph_timing(min(args.steps, 50)) if isinstance(work, BatchWorkload) else None
+
+    # end to end with host buffers: per step, the state pool is copied in from pinned host
+    # memory, advanced one step and copied back
     e2e = None
     if not args.no_e2e:
-        host = model.save()
+        pool = eng.state
+        host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
+        host.copy_(pool)
         torch.cuda.synchronize()
         e2e_steps = max(3, min(args.steps, 20))
         barrier()
@@ -273,9 +595,9 @@ def main():
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s2.record()
         for _ in range(e2e_steps):
-            model.load(host)
-            model.advance(1, check=False)
-            model.save(host)
+            pool.copy_(host, non_blocking=True)
+            work.advance(1)
+            host.copy_(pool, non_blocking=True)
         e2.record()
         torch.cuda.synchronize()
         barrier()
@@ -288,26 +610,21 @@ def main():
             "unit": UNIT,
             "h2d_bytes_per_step": int(nbytes),
             "d2h_bytes_per_step": int(nbytes),
-            "path": "MHD3D.load(pinned host pool) + MHD3D.advance(1) + MHD3D.save(pinned host pool)",
+            "path": "state pool copied in from pinned host memory, one step, copied back (every step)",
         }
 
-    # the plain float64 GPU step (the reference's dataflow, kernel by kernel) on the same box
-    plain = None
-    if rank == 0 and not args.no_plain:
-        plain = plain_step(n, rank, cells)
-
-    # accuracy of the float32 step against the float64 device step from the same state
-    accuracy = None
-    if rank == 0 and not args.no_accuracy:
-        accuracy = accuracy_check(n, rank)
+    plain = work.plain() if rank == 0 and not args.no_plain else None
+    accuracy = work.accuracy() if rank == 0 and not args.no_accuracy else None
 
     if rank == 0:
         peak, peak_kind = peaks()
         launch_s = statistics.mean(stage_ms) / 1e3 if stage_ms else float("nan")
-        achieved = BYTES_PER_ZONE_UPDATE / 2 * cells / launch_s / 1e9
-        traffic = profile_traffic()
-        if traffic is not None:
-            traffic *= cells / 256**3  # the summary's figure is per launch at 256^3
+        per_launch = work.bytes_per_zone_update / 2 * cells
+        achieved = per_launch / launch_s / 1e9
+        config = work.config()
+        config["parallelism"] = f"replicas x{world}"
+        config["l2"] = "inputs larger than L2 (state pool {:.2f} GB per copy)".format(
+            eng.state.numel() * eng.state.element_size() / 1e9)
         line = {
             "metric": METRIC,
             "value": value,
@@ -321,29 +638,25 @@ def main():
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {
-                "workload": WORKLOAD.format(n=n),
-                "cells_per_gpu": cells,
-                "parallelism": f"replicas x{world}",
-                "l2": "inputs larger than L2 (state pool {:.2f} GB per copy)".format(
-                    eng.state.numel() * eng.state.element_size() / 1e9),
-                "tile": {"y": eng.layout.tile_shape[0], "z": eng.layout.tile_shape[1], "x_planes": args.lx},
-            },
+            "config": config,
             "roofline": {
                 "bound": "hbm",
                 "achieved": achieved,
                 "peak": peak,
                 "unit": "GB/s",
                 "frac": achieved / peak,
-                "traffic": traffic,
-                "kernel": "wb::stage3d_kernel<float, 2>",
-                "algorithmic_bytes_per_launch": BYTES_PER_ZONE_UPDATE / 2 * cells,
+                "traffic": profile_traffic(args.workload, cells),
+                "kernel": work.kernel,
+                "algorithmic_bytes_per_launch": per_launch,
                 "mean_launch_ms": 1e3 * launch_s,
                 "peak_kind": peak_kind,
             },
             "gpu_launches": launches,
             "clocks": clock_info,
         }
+        if graph_ms is not None:
+            line["graph"] = {"ms_per_step": graph_ms, "value": world * cells / (graph_ms / 1e3),
+                             "what": "the same steps replayed from one captured CUDA graph"}
         if baseline is not None:
             line["cpu_baseline"] = baseline
         if e2e is not None:
@@ -356,57 +669,6 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
-
-
-def plain_step(n, seed, cells, steps=3):
-    """zone-updates/s of the plain float64 GPU step (`wellbalanced_b200.plain.PlainMHD3D`)."""
-    import torch
-
-    from wellbalanced_b200.mesh import AMRHierarchy
-    from wellbalanced_b200.plain import PlainMHD3D
-    from wellbalanced_b200.problems import turbulence_3d
-
-    rho, velocity, p, potential = turbulence_3d(n, seed=seed)
-    model = PlainMHD3D(AMRHierarchy((n,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3)
-    model.set_state(rho, velocity, p, vector_potential=potential)
-    model.step()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    for _ in range(steps):
-        model.step()
-    end.record()
-    torch.cuda.synchronize()
-    seconds = start.elapsed_time(end) / 1e3
-    del model
-    torch.cuda.empty_cache()
-    return {"value": cells * steps / seconds, "unit": UNIT, "ms_per_step": 1e3 * seconds / steps, "steps": steps,
-            "what": "PlainMHD3D: the reference MHD3D dataflow on the device, float64, per-kernel, intermediates in HBM"}
-
-
-def accuracy_check(n, seed, steps=10):
-    """Relative L1 errors of float32 against float64 device steps from the same state."""
-    import numpy as np
-    import torch
-
-    from wellbalanced_b200.mhd3d import MHD3D
-
-    ref = MHD3D.turbulence(n, seed=seed, precision=64)
-    low = MHD3D.turbulence(n, seed=seed, precision=32)
-    for _ in range(steps):
-        dt = ref.step()
-        low.step(dt)
-    torch.cuda.synchronize()
-    out = {"steps": steps, "against": "float64 device step from the same state (float64 step == reference to 1e-12 in the tests)"}
-    for key, f in (("density", 0), ("energy", 4)):
-        (patch,) = ref.hierarchy.patches
-        a = ref._read(patch, f).to(torch.float64)
-        b = low._read(patch, f).to(torch.float64)
-        out[f"rel_l1_{key}"] = float(torch.sum(torch.abs(b - a)) / torch.sum(torch.abs(a)))
-    out["div_b"] = low.divergence()
-    del ref, low
-    torch.cuda.empty_cache()
-    return out
 
 
 if __name__ == "__main__":

@@ -292,6 +292,17 @@ class MHD2D:
         self.steps = 0
         self._ready = True
 
+    def set_conserved(self, fields, az):
+        """A one-patch level 0 from conserved cell arrays (rho, m_x, m_y, m_z, E, B_z) and
+        nodal A_z (a test-side setter; the reference sets states through `set_state`)."""
+        (patch,) = self.hierarchy.patches_at_level(0)
+        for name, value in zip(CONSERVED, fields, strict=True):
+            patch.field(self.names[name]).local[...] = value
+        patch.field(self.potential).local[...] = az
+        self.time = 0.0
+        self.steps = 0
+        self._ready = True
+
     def _check_ready(self):
         if not self._ready:
             raise RuntimeError("set the state first (set_state)")

@@ -139,6 +139,34 @@ def test_float32_orszag_tang_error_against_the_float64_reference(runs2d):
     assert model.divergence() < 1e-12
 
 
+def test_float32_near_degenerate_harris_sheet_tracks_float64():
+    """A Harris sheet at rest has HLLD faces whose star denominator
+    rho (S - u)(S - S_M) - B_n^2 nearly vanishes (Alfven speed close to the fast speed,
+    small tangential field). Evaluated in float32 it cancels to noise: the float32 step
+    drifted by 1e-3 per step and went negative. The float32 kernels redo those faces'
+    wave speeds and star states in float64; float32 must then track float64 closely."""
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+    from wellbalanced_b200.problems import harris_sheet
+
+    bounds = ((-1.0, 1.0), (-2.0, 2.0))
+    density, pressure, potential = harris_sheet(256, 512, seed=0, bounds=bounds)
+    models = []
+    for precision in (64, 32):
+        model = MHD2D(AMRHierarchy((256, 512), bounds, periodic=(True, False)), limiter="mc", cfl=0.4,
+                      precision=precision)
+        model.set_state(density, (0.0, 0.0, 0.0), pressure, vector_potential=potential)
+        models.append(model)
+    ref, low = models
+    for _ in range(6):
+        low.step(ref.step())
+    (pr,), (pl,) = ref.hierarchy.patches, low.hierarchy.patches
+    for f in (0, 2, 4):
+        a, b = ref.gather(pr, f), low.gather(pl, f)
+        assert np.max(np.abs(b - a)) < 2e-5, f
+        assert np.sum(np.abs(b - a)) / np.sum(np.abs(a)) < 1e-6, f
+
+
 def test_negative_pressure_is_reported():
     from wellbalanced_b200.mesh import AMRHierarchy
     from wellbalanced_b200.mhd import MHD2D

@@ -58,11 +58,23 @@ class Batch:
     def orszag_tang(cls, count, *, seed=0, precision=32, **options):
         sides, b_factor, v_factor = orszag_tang_sizes(count, seed=seed)
         batch = cls(sides, precision=precision, **options)
+        host = np.zeros(batch.layout.pool_size, dtype=np.float32 if batch.precision == 32 else np.float64)
         for k in range(count):
             fields, az = orszag_tang_2d(int(sides[k]), b_factor[k], v_factor[k], gamma=batch.gamma)
-            batch.set_instance(k, fields, az)
+            batch._write_host(host, k, fields, az)
+        batch.engine.state.copy_(torch.from_numpy(host))
         batch.finish_state()
         return batch
+
+    def _write_host(self, host, k, fields, az):
+        """Instance k's conserved cells and A_z into a host copy of the pool."""
+        from wellbalanced_b200.mesh import Patch
+
+        nx, ny = self.sides[k]
+        patch = Patch(0, ((0, nx), (0, ny)), index=k)
+        for f, value in enumerate(fields):
+            self.layout.patch_view(host, patch, f)[HALO : HALO + nx, HALO : HALO + ny] = value
+        self.layout.patch_view(host, patch, 6)[HALO : HALO + nx + 1, HALO : HALO + ny + 1] = az
 
     # state ---------------------------------------------------------------------------------------
     def _view(self, k, f, node=False):

@@ -57,6 +57,24 @@ struct Math<float> {
   static __device__ __forceinline__ float over_sqrt(float a, float sq) { return a * __fdividef(1.0f, sq); }
 };
 
+// float64 arithmetic seeded from the float32 special-function units: the reciprocal and
+// the reciprocal square root of the float32 value refined by one Newton step in float64
+// (relative error ~1e-13). Used by the float32 kernels where float32 is not enough (the
+// near-degenerate HLLD star states below).
+struct MathRefined {
+  static __device__ __forceinline__ double inv(double b) {
+    const double r = double(__fdividef(1.0f, float(b)));
+    return r * (2.0 - b * r);
+  }
+  static __device__ __forceinline__ double div(double a, double, double inv_b) { return a * inv_b; }
+  static __device__ __forceinline__ double sqrt(double x) {
+    if (!(x > 0.0)) return 0.0;
+    const double r0 = double(rsqrtf(float(x)));
+    return x * (r0 * (1.5 - 0.5 * x * r0 * r0));
+  }
+  static __device__ __forceinline__ double over_sqrt(double a, double sq) { return a * inv(sq); }
+};
+
 __device__ __forceinline__ float rsqrt_(float x) { return Math<float>::sqrt(x); }
 __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
 
@@ -95,9 +113,8 @@ __device__ __forceinline__ R limited_slope_rt(R a, R b, int limiter) {
 }
 
 // Fast magnetosonic speed along the normal; the discriminant is clipped at zero.
-template <typename R>
+template <typename R, typename M = Math<R>>
 __device__ __forceinline__ R fast_speed(R rho, R p, R bn, R bt1, R bt2, R gamma) {
-  using M = Math<R>;
   const R inv_rho = M::inv(rho);
   const R a2 = M::div(gamma * p, rho, inv_rho);
   const R b2 = M::div(bn * bn + bt1 * bt1 + bt2 * bt2, rho, inv_rho);
@@ -132,14 +149,14 @@ __device__ __forceinline__ R side_state(const R (&w)[7], R bn, R inv_gm1, R (&u)
   return pt;
 }
 
-// Star tangential velocity and field of one side (star_state without the energy).
-template <typename R>
+// Star tangential velocity and field of one side (star_state without the energy); `den`
+// returns the star denominator d (s - s_M) - B_n^2.
+template <typename R, typename M = Math<R>>
 __device__ __forceinline__ void star_tangential(const R (&w)[7], R bn, R s, R d, R pt, R sm,
-                                                R& rho_s, R& vt1, R& vt2, R& bt1, R& bt2) {
-  using M = Math<R>;
+                                                R& rho_s, R& vt1, R& vt2, R& bt1, R& bt2, R& den) {
   const R vn = w[1];
   rho_s = M::div(d, s - sm, M::inv(s - sm));
-  const R den = d * (s - sm) - bn * bn;
+  den = d * (s - sm) - bn * bn;
   vt1 = w[2];
   vt2 = w[3];
   bt1 = w[5];
@@ -157,6 +174,75 @@ __device__ __forceinline__ void star_tangential(const R (&w)[7], R bn, R s, R d,
   bt2 = regular ? b2 : bt2;
 }
 
+// The wave speeds, S_M, p_T* and both sides' star density, tangential velocity and field.
+template <typename R>
+struct HlldFront {
+  R sl, sr, ptl, ptr, dl, dr, sm, pts;
+  R rsl, vtl1, vtl2, btl1, btl2, den_l;
+  R rsr, vtr1, vtr2, btr1, btr2, den_r;
+};
+
+template <typename R, typename M>
+__device__ __forceinline__ void hlld_front(const R (&L)[7], const R (&Rt)[7], R bn, R gamma, HlldFront<R>& o) {
+  const R rl = L[0], vl = L[1], rr = Rt[0], vr = Rt[1];
+  const R cf = rmax(fast_speed<R, M>(rl, L[4], bn, L[5], L[6], gamma),
+                    fast_speed<R, M>(rr, Rt[4], bn, Rt[5], Rt[6], gamma));
+  o.sl = rmin(vl, vr) - cf;
+  o.sr = rmax(vl, vr) + cf;
+  const R bn2 = bn * bn;
+  o.ptl = L[4] + R(0.5) * (bn2 + L[5] * L[5] + L[6] * L[6]);
+  o.ptr = Rt[4] + R(0.5) * (bn2 + Rt[5] * Rt[5] + Rt[6] * Rt[6]);
+  o.dl = (o.sl - vl) * rl;
+  o.dr = (o.sr - vr) * rr;
+  const R inv_dd = M::inv(o.dr - o.dl);
+  o.sm = M::div(o.dr * vr - o.dl * vl - o.ptr + o.ptl, o.dr - o.dl, inv_dd);
+  o.pts = M::div(o.dr * o.ptl - o.dl * o.ptr + o.dl * o.dr * (vr - vl), o.dr - o.dl, inv_dd);
+  star_tangential<R, M>(L, bn, o.sl, o.dl, o.ptl, o.sm, o.rsl, o.vtl1, o.vtl2, o.btl1, o.btl2, o.den_l);
+  star_tangential<R, M>(Rt, bn, o.sr, o.dr, o.ptr, o.sm, o.rsr, o.vtr1, o.vtr2, o.btr1, o.btr2, o.den_r);
+}
+
+// Relative size of the star denominator below which a float32 evaluation is redone in
+// float64: the float32 fast speeds carry relative errors ~1e-7, so d (s - s_M) - B_n^2 has
+// absolute errors up to ~1e-6 (p_T + B_n^2) where it cancels (Alfven speed close to the
+// fast speed, small tangential field); above 1e-3 the float32 value is good to ~0.1%.
+constexpr float kNearDegenerate32 = 1.0e-3f;
+
+// The float64 evaluation of a float32 face's front half (taken rarely: only where the
+// float32 star denominator is near zero).
+__device__ __forceinline__ void hlld_front_wide(const float (&L)[7], const float (&Rt)[7], float bn, float gamma,
+                                             HlldFront<float>& o) {
+  double Ld[7], Rd[7];
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    Ld[c] = L[c];
+    Rd[c] = Rt[c];
+  }
+  HlldFront<double> d;
+  hlld_front<double, MathRefined>(Ld, Rd, double(bn), double(gamma), d);
+  o.sl = float(d.sl), o.sr = float(d.sr), o.ptl = float(d.ptl), o.ptr = float(d.ptr);
+  o.dl = float(d.dl), o.dr = float(d.dr), o.sm = float(d.sm), o.pts = float(d.pts);
+  o.rsl = float(d.rsl), o.vtl1 = float(d.vtl1), o.vtl2 = float(d.vtl2);
+  o.btl1 = float(d.btl1), o.btl2 = float(d.btl2), o.den_l = float(d.den_l);
+  o.rsr = float(d.rsr), o.vtr1 = float(d.vtr1), o.vtr2 = float(d.vtr2);
+  o.btr1 = float(d.btr1), o.btr2 = float(d.btr2), o.den_r = float(d.den_r);
+}
+
+template <typename R>
+__device__ __forceinline__ void hlld_front_checked(const R (&L)[7], const R (&Rt)[7], R bn, R gamma,
+                                                   HlldFront<R>& o) {
+  hlld_front<R, Math<R>>(L, Rt, bn, gamma, o);
+}
+
+template <>
+__device__ __forceinline__ void hlld_front_checked<float>(const float (&L)[7], const float (&Rt)[7], float bn,
+                                                          float gamma, HlldFront<float>& o) {
+  hlld_front<float, Math<float>>(L, Rt, bn, gamma, o);
+  const float bn2 = bn * bn;
+  const bool near = rabs(o.den_l) < kNearDegenerate32 * (o.ptl + bn2) ||
+                    rabs(o.den_r) < kNearDegenerate32 * (o.ptr + bn2);
+  if (near) hlld_front_wide(L, Rt, bn, gamma, o);
+}
+
 // HLLD flux through a face between normal-frame states L and Rt with normal field bn.
 // Straight-line code: the star / double-star flux of the side of the contact the face
 // lies on is always formed and the supersonic and star-only cases are selected at the
@@ -166,22 +252,11 @@ template <typename R>
 __device__ __forceinline__ void hlld_flux(const R (&L)[7], const R (&Rt)[7], R bn, R gamma,
                                           R inv_gm1, R (&F)[7]) {
   using M = Math<R>;
-  const R rl = L[0], vl = L[1], rr = Rt[0], vr = Rt[1];
-  const R cf = rmax(fast_speed(rl, L[4], bn, L[5], L[6], gamma),
-                    fast_speed(rr, Rt[4], bn, Rt[5], Rt[6], gamma));
-  const R sl = rmin(vl, vr) - cf;
-  const R sr = rmax(vl, vr) + cf;
-  const R bn2 = bn * bn;
-  const R ptl = L[4] + R(0.5) * (bn2 + L[5] * L[5] + L[6] * L[6]);
-  const R ptr = Rt[4] + R(0.5) * (bn2 + Rt[5] * Rt[5] + Rt[6] * Rt[6]);
-  const R dl = (sl - vl) * rl;
-  const R dr = (sr - vr) * rr;
-  const R inv_dd = M::inv(dr - dl);
-  const R sm = M::div(dr * vr - dl * vl - ptr + ptl, dr - dl, inv_dd);
-  const R pts = M::div(dr * ptl - dl * ptr + dl * dr * (vr - vl), dr - dl, inv_dd);
-  R rsl, vtl1, vtl2, btl1, btl2, rsr, vtr1, vtr2, btr1, btr2;
-  star_tangential(L, bn, sl, dl, ptl, sm, rsl, vtl1, vtl2, btl1, btl2);
-  star_tangential(Rt, bn, sr, dr, ptr, sm, rsr, vtr1, vtr2, btr1, btr2);
+  HlldFront<R> fr;
+  hlld_front_checked<R>(L, Rt, bn, gamma, fr);
+  const R sl = fr.sl, sr = fr.sr, ptl = fr.ptl, ptr = fr.ptr, sm = fr.sm, pts = fr.pts;
+  const R rsl = fr.rsl, vtl1 = fr.vtl1, vtl2 = fr.vtl2, btl1 = fr.btl1, btl2 = fr.btl2;
+  const R rsr = fr.rsr, vtr1 = fr.vtr1, vtr2 = fr.vtr2, btr1 = fr.btr1, btr2 = fr.btr2;
   const R sql = M::sqrt(rsl);
   const R sqr = M::sqrt(rsr);
   const R sign = bn > R(0) ? R(1) : (bn < R(0) ? R(-1) : R(0));

@@ -330,8 +330,9 @@ class MHD2D:
             taken += 1
         return taken
 
-    def advance(self, steps: int) -> None:
-        """``steps`` steps at the stable dt with no host synchronisation (checked at the end)."""
+    def advance(self, steps: int, *, check: bool = True) -> None:
+        """``steps`` steps at the stable dt with no host synchronisation (checked at the end
+        unless ``check`` is false; the bad-cell count then stays in ``engine.bad``)."""
         self._check_ready()
         eng = self.engine
         eng.bad.zero_()
@@ -339,9 +340,10 @@ class MHD2D:
             eng.rate()
             eng.finalize_dt(self.cfl, self.resistivity, max(self.conduction), advance=True)
             eng.heun_step(self._groups_potential, self._groups_all)
-        self.time = float(eng.time[0].item())
         self.steps += steps
-        self._raise_if_bad()
+        if check:
+            self.time = float(eng.time[0].item())
+            self._raise_if_bad()
 
     # refinement ----------------------------------------------------------------------------------
     def current_tags(self, threshold: float, levels: int) -> dict[int, np.ndarray]:
