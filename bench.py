@@ -297,6 +297,13 @@ class Harris:
     def advance(self, steps):
         self.model.advance(steps, check=False)
 
+    def graph_timing(self, steps):
+        """ms per step of the same steps replayed from one captured CUDA graph."""
+        self.model.capture()
+        seconds = _time_steps(lambda: self.model.advance(1, check=False), steps)
+        self.model._graph = None
+        return 1e3 * seconds / steps
+
     def config(self):
         h = self.model.hierarchy
         refined = [p.shape for p in h.patches if p.level]
@@ -579,7 +586,7 @@ def main():
     cells = work.cells
     value = world * cells * args.steps / seconds
 
-    graph_ms = work.graph_timing(min(args.steps, 50)) if isinstance(work, BatchWorkload) else None
+    graph_ms = work.graph_timing(min(args.steps, 50)) if hasattr(work, "graph_timing") else None
 
     # end to end with host buffers: per step, the state pool is copied in from pinned host
     # memory, advanced one step and copied back

@@ -144,3 +144,18 @@ def test_refined_3d_matches_the_oracle_and_conserves():
     for name in before:
         assert abs(after[name] - before[name]) < 1e-14 * max(1.0, abs(before[name])) * 100
     assert device.divergence() < 1e-14
+
+
+def test_graph_replay_equals_direct_steps_on_a_refined_hierarchy():
+    """`capture` records one step of the whole hierarchy; replays equal direct launches."""
+    import torch
+
+    _, a = _pair(precision=32)
+    _, b = _pair(precision=32)
+    a.advance(5)
+    b.capture()
+    b.advance(4)
+    torch.cuda.synchronize()
+    assert a.steps == b.steps == 5
+    assert a.time == b.time
+    np.testing.assert_array_equal(a.engine.state.cpu().numpy(), b.engine.state.cpu().numpy())

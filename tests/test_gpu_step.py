@@ -161,10 +161,11 @@ def test_float32_near_degenerate_harris_sheet_tracks_float64():
     for _ in range(6):
         low.step(ref.step())
     (pr,), (pl,) = ref.hierarchy.patches, low.hierarchy.patches
-    for f in (0, 2, 4):
+    for f in (0, 2, 4):  # density, m_y (near zero: absolute only), energy
         a, b = ref.gather(pr, f), low.gather(pl, f)
         assert np.max(np.abs(b - a)) < 2e-5, f
-        assert np.sum(np.abs(b - a)) / np.sum(np.abs(a)) < 1e-6, f
+        if f != 2:
+            assert np.sum(np.abs(b - a)) / np.sum(np.abs(a)) < 1e-6, f
 
 
 def test_negative_pressure_is_reported():

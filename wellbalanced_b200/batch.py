@@ -116,18 +116,9 @@ class Batch:
         eng.heun_step(groups[1:], groups)
 
     def capture(self):
-        """Capture one step (all launches) in a CUDA graph; `advance` then replays it."""
-        stream = torch.cuda.Stream()
-        stream.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(stream):
-            self._step_launches()  # warm-up outside the graph (function attributes, lazy loads)
-        torch.cuda.current_stream().wait_stream(stream)
-        torch.cuda.synchronize()
-        graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(graph):
-            self._step_launches()
-        torch.cuda.synchronize()
-        self._graph = graph
+        """Capture one step (all launches) in a CUDA graph; `advance` then replays it. The
+        recording takes one step of every instance."""
+        self._graph = self.engine.capture(self._step_launches)
         self.steps += 1
 
     def advance(self, steps, *, check=True):

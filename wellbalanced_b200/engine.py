@@ -215,6 +215,21 @@ class Engine:
                       self.dt.data_ptr(), self._s())
             self.launches += 1
 
+    def capture(self, step):
+        """A CUDA graph of the launches `step()` issues. `step` runs once outside the graph
+        first (lazy loading and launch attributes happen there, not in the recording)."""
+        stream = torch.cuda.Stream(self.device)
+        stream.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(stream):
+            step()
+        torch.cuda.current_stream(self.device).wait_stream(stream)
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            step()
+        torch.cuda.synchronize(self.device)
+        return graph
+
     def heun_step(self, groups_potential, groups_all):
         """One Heun step with the dt already in self.dt (device), refluxed and restricted."""
         U, U1 = self.state, self.stage_pool

@@ -116,6 +116,7 @@ class MHD2D:
     _fused = True
 
     def _build_engine(self):
+        self._graph = None
         walls = tuple((w, w) for w in self.walls)
         self.engine = Engine(
             self.hierarchy,
@@ -330,6 +331,21 @@ class MHD2D:
             taken += 1
         return taken
 
+    def _one_step(self):
+        """The launches of one step at the stable dt (dt, time and state on the device)."""
+        eng = self.engine
+        eng.rate()
+        eng.finalize_dt(self.cfl, self.resistivity, max(self.conduction), advance=True)
+        eng.heun_step(self._groups_potential, self._groups_all)
+
+    def capture(self) -> None:
+        """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
+        graph that `advance` replays. The recording takes one step. A regrid drops it."""
+        self._check_ready()
+        self._graph = self.engine.capture(self._one_step)
+        self.steps += 1
+        self.time = float(self.engine.time[0].item())
+
     def advance(self, steps: int, *, check: bool = True) -> None:
         """``steps`` steps at the stable dt with no host synchronisation (checked at the end
         unless ``check`` is false; the bad-cell count then stays in ``engine.bad``)."""
@@ -337,9 +353,10 @@ class MHD2D:
         eng = self.engine
         eng.bad.zero_()
         for _ in range(steps):
-            eng.rate()
-            eng.finalize_dt(self.cfl, self.resistivity, max(self.conduction), advance=True)
-            eng.heun_step(self._groups_potential, self._groups_all)
+            if self._graph is not None:
+                self._graph.replay()
+            else:
+                self._one_step()
         self.steps += steps
         if check:
             self.time = float(eng.time[0].item())
