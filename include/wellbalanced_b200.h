@@ -141,6 +141,26 @@ int wb_reflux_apply(int precision, void* pool, const void* patches, const void* 
 /* Sizes of the engine structs, for callers that mirror them. */
 int wb_struct_sizes(int64_t* sizes_host, int n);
 
+/* Learned refinement tagger. No counterpart in the reference: it predicts the cells the
+ * current tagger (|J| dx > threshold, carafe/mhd3d.py:771-801) flags a few steps ahead.
+ * Parameters are one float32 vector of 5313 values (W1 [64][16] | b1 | W2 [64][64] | b2 |
+ * W3 [64] | b3); the kernels use them rounded to bfloat16, with float32 accumulation.
+ * - wb_tag_features: 16 stencil features of every interior cell of the 3D patches of a
+ *   pool, written as float32 rows out[(row_start[p] + t) * 16 + c] (t the cell's index
+ *   in (i, j, k) order), normalised as (f - mean[c]) * inv_std[c]; work list as wb_rate;
+ * - wb_mlp_forward: logits of n feature rows (tensor-core mma, bf16 x float32);
+ * - wb_mlp_backward: adds the gradient of the summed weighted binary cross-entropy
+ *   (weight pos_weight where targets[r] = 1) to grads and the loss to *loss;
+ * - wb_mlp_adam: one Adam step with the gradients scaled by `scale`; clears grads. */
+int wb_tag_features(int precision, const void* pool, const void* patches, const int* chunk_patch,
+                    const int* chunk_start, int nchunks, const int64_t* row_start, double b0x, double b0y,
+                    double b0z, double gamma, const float* mean, const float* inv_std, float* out, void* stream);
+int wb_mlp_forward(const float* features, int64_t n, const float* params, float* logits, void* stream);
+int wb_mlp_backward(const float* features, const float* targets, int64_t n, const float* params, float pos_weight,
+                    float* grads, double* loss, void* stream);
+int wb_mlp_adam(float* params, float* grads, float* m, float* v, int count, float lr, float beta1, float beta2,
+                float eps, int step, float scale, void* stream);
+
 /* wb_rate without a caller-provided key buffer: allocates nothing. No counterpart in the
  * reference (its rate kernel returns into a caller-allocated out[2]). Same work list and
  * state as wb_rate; the per-instance keys live in a static device array of 4096

@@ -38,6 +38,12 @@ SIGNATURES = {
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],
     "wb_finalize_dt": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_tag_features": [c_int, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_double, c_dp,
+                        c_dp, c_dp, c_dp],
+    "wb_mlp_forward": [c_dp, ctypes.c_int64, c_dp, c_dp, c_dp],
+    "wb_mlp_backward": [c_dp, c_dp, ctypes.c_int64, c_dp, ctypes.c_float, c_dp, c_dp, c_dp],
+    "wb_mlp_adam": [c_dp, c_dp, c_dp, c_dp, c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                    c_int, ctypes.c_float, c_dp],
     "wb_rate_static": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double,
                        c_int, c_dp, c_dp],
     "wb_copy_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
