@@ -58,7 +58,7 @@ def parse():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-accuracy", action="store_true")
     parser.add_argument("--no-plain", action="store_true")
-    parser.add_argument("--lx", type=int, default=32, help="turbulence: x-planes per tile")
+    parser.add_argument("--lx", default="auto", help="turbulence: x-planes per tile (an integer, or auto: tuned)")
     return parser.parse_args()
 
 
@@ -136,6 +136,10 @@ def _rel_l1(ref, low, patches, steps):
     return out
 
 
+def describe(timings):
+    return {str(k): round(float(v), 4) for k, v in sorted(timings.items())} if timings else None
+
+
 class Turbulence:
     kernel = "wb::stage3d_kernel<float, 2>"
     bytes_per_zone_update = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
@@ -145,9 +149,10 @@ class Turbulence:
 
         self.n = args.cells
         self.rank = rank
-        self.lx = args.lx
-        self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=args.lx)
+        lx = args.lx if args.lx == "auto" else int(args.lx)
+        self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=lx)
         self.engine = self.model.engine
+        self.lx = self.model.lx
         self.cells = self.n**3
 
     def advance(self, steps):
@@ -160,6 +165,7 @@ class Turbulence:
                          "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1"),
             "cells_per_gpu": self.cells,
             "tile": {"y": eng.layout.tile_shape[0], "z": eng.layout.tile_shape[1], "x_planes": self.lx},
+            "autotune_ms_per_launch": describe(self.model.lx_timings),
         }
 
     def plain(self, steps=3):

@@ -338,3 +338,20 @@ def test_plain_3d_step_matches_the_reference(runs3d):
     dts = [model.step() for _ in range(4)]
     np.testing.assert_allclose(dts, runs3d["turb16_dts"], rtol=1e-13)
     close(model.state(), runs3d, "turb16", 1e-12)
+
+
+def test_autotuned_x_march_gives_the_same_steps():
+    """`lx="auto"` times the stage kernel for each x-march length and keeps the fastest;
+    the tiling changes no arithmetic, so every choice gives bitwise the same steps."""
+    import torch
+
+    from wellbalanced_b200.autotune import CANDIDATES
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    tuned = MHD3D.turbulence(24, seed=2, precision=32, lx="auto")
+    fixed = MHD3D.turbulence(24, seed=2, precision=32, lx=8)
+    assert tuned.lx in CANDIDATES and tuned.lx_timings and tuned.lx == min(tuned.lx_timings, key=tuned.lx_timings.get)
+    for _ in range(3):
+        fixed.step(tuned.step())
+    torch.cuda.synchronize()
+    assert torch.equal(tuned.engine.state, fixed.engine.state)

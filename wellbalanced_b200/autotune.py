@@ -1,0 +1,72 @@
+"""Autotuner of the stage kernels' schedule.
+
+The 3D stage kernel marches each 16 x 16 (y, z) column over ``lx`` x-planes per tile: a
+longer march reads fewer halo planes per cell (two extra planes per tile) but gives fewer
+tiles to spread over the 148 SMs, so the best ``lx`` depends on the patch sizes. `tune_lx`
+times the stage kernel (its stage-1 form, which writes only the scratch pool) on an
+engine's own layout and state for each candidate and keeps the fastest; results are
+remembered per (precision, patch shapes) for the process. ``MHD3D(..., lx="auto")`` tunes
+when its state is first set.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from wellbalanced_b200 import _lib
+
+CANDIDATES = (8, 16, 32, 64, 128)
+_CACHE: dict[tuple, int] = {}
+
+
+def _key(engine):
+    shapes = tuple(sorted({tuple(int(v) for v in r["n"]) for r in engine.layout.rows}))
+    return (engine.precision, engine.limiter, shapes)
+
+
+def _set_lx(engine, lx):
+    layout = engine.layout
+    layout.lx = int(lx)
+    layout._tiles()
+    from wellbalanced_b200.engine import _device_bytes
+
+    engine.tiles = _device_bytes(layout.tiles, engine.device, _lib.TILE)
+    engine.ntiles = int(layout.tiles.size)
+
+
+def tune_lx(engine, candidates=CANDIDATES, repeats=5, use_cache=True):
+    """The fastest x-march length for `engine` (3D); the engine is left set to it.
+
+    Returns ``(lx, {lx: mean ms per stage launch})`` (an empty dict when cached)."""
+    if engine.ndim != 3:
+        raise ValueError("the x-march length applies to the 3D stage kernel")
+    key = _key(engine)
+    if use_cache and key in _CACHE:
+        _set_lx(engine, _CACHE[key])
+        return _CACHE[key], {}
+    longest = max(int(r["n"][0]) + 1 for r in engine.layout.rows)
+    timings = {}
+    bad = engine.bad.clone()
+    for lx in candidates:
+        if lx > 2 * longest and lx != candidates[0]:
+            continue
+        _set_lx(engine, lx)
+        engine.stage(engine.state, None, engine.stage_pool)  # warm-up
+        torch.cuda.synchronize(engine.device)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(repeats):
+            engine.stage(engine.state, None, engine.stage_pool)
+        end.record()
+        torch.cuda.synchronize(engine.device)
+        timings[lx] = start.elapsed_time(end) / repeats
+    engine.bad.copy_(bad)
+    best = min(timings, key=timings.get)
+    _set_lx(engine, best)
+    _CACHE[key] = best
+    return best, timings
+
+
+def describe(timings):
+    return {str(k): round(float(v), 4) for k, v in sorted(timings.items())} if timings else None
+

@@ -46,7 +46,7 @@ class MHD3D:
         prefix: str = "mhd_",
         precision: int = 64,
         device: str = "cuda",
-        lx: int = 32,
+        lx: int | str = 32,
     ) -> None:
         if hierarchy.ndim != 3:
             raise ValueError("MHD3D needs a 3D hierarchy")
@@ -76,7 +76,10 @@ class MHD3D:
         self.periodic = tuple(hierarchy.periodic)
         self.precision = int(precision)
         self.device = device
-        self.lx = lx
+        # x-planes per tile of the stage kernel; "auto": tuned when the state is first set
+        self._auto_lx = lx == "auto"
+        self.lx = 32 if self._auto_lx else int(lx)
+        self.lx_timings = None
         self._build_engine()
         self.time = 0.0
         self.steps = 0
@@ -269,6 +272,11 @@ class MHD3D:
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
+        if self._auto_lx:
+            from wellbalanced_b200.autotune import tune_lx
+
+            self.lx, timings = tune_lx(eng)
+            self.lx_timings = timings or self.lx_timings
         self.time = 0.0
         self.steps = 0
         eng.time.zero_()
