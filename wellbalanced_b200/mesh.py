@@ -169,7 +169,7 @@ def _boxes_intersect(a, b):
 def _concat(arrays, dtype):
     """Records of ``arrays`` in one array of the C layout ``dtype`` (``np.concatenate``
     alone may repack a padded structured dtype)."""
-    arrays = [np.asarray(a) for a in arrays if a is not None and np.asarray(a).size]
+    arrays = [np.atleast_1d(np.asarray(a)) for a in arrays if a is not None and np.asarray(a).size]
     if not arrays:
         return np.zeros(0, dtype)
     return np.concatenate(arrays).astype(dtype)
