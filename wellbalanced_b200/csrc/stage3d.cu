@@ -59,8 +59,8 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sP = reinterpret_cast<S*>(smem_raw);  // [2 slots][8][NR] primitive variables
   S* sBn = sP + 2 * 8 * NR;                 // [2 slots][3][NR] field at each cell's lower faces
-  S* sEc = sBn + 2 * 3 * NR;                // [3 slots][3][G] cell E_x, E_y, E_z
-  S* sYZ = sEc + 3 * 3 * G;                 // [2 slots][2 dirs][7][G] y- and z-face fluxes
+  S* sEc = sBn + 2 * 3 * NR;                // [4 slots][3][G] cell E_x, E_y, E_z
+  S* sYZ = sEc + 4 * 3 * G;                 // [2 slots][2 dirs][7][G] y- and z-face fluxes
   S* sX = sYZ + 2 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
 
   const Tile tile = a.tiles[blockIdx.x];
@@ -129,10 +129,10 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
     {
       const int c = p + 1;
       const int slot = (c + 4) & 1;
-      const int slot3 = (c + 6) % 3;
+      const int slot4 = (c + 8) & 3;
       S* P8 = sP + slot * 8 * NR;
       S* B3 = sBn + slot * 3 * NR;
-      S* E3 = sEc + slot3 * 3 * G;
+      S* E3 = sEc + slot4 * 3 * G;
       const int I = c + kHalo;
       for (int r = tid; r < NR; r += blockDim.x) {
         const int j = r / RZ - 2, k = r % RZ - 2;
@@ -271,8 +271,8 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       const S* Zc = sYZ + (sc * 2 + 1) * 7 * G;
       const S* Yp = sYZ + (sp * 2 + 0) * 7 * G;
       const S* Zp = sYZ + (sp * 2 + 1) * 7 * G;
-      const S* Ec = sEc + ((p + 6) % 3) * 3 * G;
-      const S* Ep = sEc + ((p + 5) % 3) * 3 * G;
+      const S* Ec = sEc + ((p + 8) & 3) * 3 * G;
+      const S* Ep = sEc + ((p + 7) & 3) * 3 * G;
       auto yi = [&](int fj, int kk) { return fj * GZ + (kk + 1); };
       auto zi = [&](int jj, int fk) { return (jj + 1) * GZ + fk; };
       auto gi = [&](int jj, int kk) { return (jj + 1) * GZ + (kk + 1); };
@@ -328,7 +328,10 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
 #pragma unroll
       for (int cc = 0; cc < 5; ++cc) fprev[cc] = fnow[cc];
     }
-    __syncthreads();
+    // no barrier here: phase A of the next plane writes only the primitive, face-field and
+    // cell-E slots of plane p + 2 (the E ring has 4 slots, phase C reads those of p and
+    // p - 1), and phase B of the next plane, which overwrites the faces read above, comes
+    // after the next barrier
   }
   if (bad) atomicAdd(a.bad, (unsigned long long)bad);
 }
@@ -337,7 +340,7 @@ template <typename S>
 int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
   constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int NR = (TY + 4) * (TZ + 4), G = (TY + 1) * (TZ + 1);
-  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 3 * 3 * G + 2 * 2 * 7 * G + 3 * G);
+  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 4 * 3 * G + 2 * 2 * 7 * G + 3 * G);
   if (ntiles <= 0) return kOk;
   if (args.lx <= 0) {
     set_error("stage3d: lx must be positive");
