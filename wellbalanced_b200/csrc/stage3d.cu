@@ -1,7 +1,7 @@
 // Fused 3D stage kernel: one RK stage of the 3D step over a work list of tiles.
 //
 // A tile is TY x TZ columns (y, z) of a patch, marched along x over `lx` cell planes.
-// 288 threads, each with fixed roles per plane:
+// 288 threads, each with fixed roles per plane (two barriers per plane):
 //   * one x-face column (j, k) of the L-shaped set the tile needs — its thread keeps
 //     the four cell planes of the x-stencil of that column in registers;
 //   * one y-face and one z-face of the current plane;
@@ -11,8 +11,10 @@
 //      potential, carafe/mhd3d.py:361-386), forms the primitive variables (pressure in
 //      float64 for a float32 state) and the cell electric fields, counts bad cells
 //      (carafe/mhd3d.py:475-509);
-//   B: MUSCL + HLLD on x-face p and on the y- and z-faces of plane p, each in the cyclic
-//      frame of its axis (carafe/mhd3d.py:511-528, mhd_sweep_pyccel.py:254-319);
+//   B1: MUSCL + HLLD on the y- and z-faces of plane p (loaded one plane earlier), in the
+//      same barrier interval as A, so the uneven load rounds of A overlap face work;
+//   B2 (after a barrier): the x-face p, whose stencil reaches plane p+1; each face in
+//      the cyclic frame of its axis (carafe/mhd3d.py:511-528, mhd_sweep_pyccel.py:254-319);
 //   C: CT-contact edge fields (carafe/mhd3d.py:530-559; ct_contact_pyccel.py:36-61):
 //      E_x on the x-edges of cell plane p, E_y and E_z on node plane p; updates A there
 //      (A -= dt E) and the cells of plane p-1 (U -= dt div F), with the Heun combine in
@@ -60,8 +62,8 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   S* sP = reinterpret_cast<S*>(smem_raw);  // [2 slots][8][NR] primitive variables
   S* sBn = sP + 2 * 8 * NR;                 // [2 slots][3][NR] field at each cell's lower faces
   S* sEc = sBn + 2 * 3 * NR;                // [4 slots][3][G] cell E_x, E_y, E_z
-  S* sYZ = sEc + 4 * 3 * G;                 // [2 slots][2 dirs][7][G] y- and z-face fluxes
-  S* sX = sYZ + 2 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
+  S* sYZ = sEc + 4 * 3 * G;                 // [3 slots][2 dirs][7][G] y- and z-face fluxes
+  S* sX = sYZ + 3 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
 
   const Tile tile = a.tiles[blockIdx.x];
   const PatchDesc P = a.patches[tile.patch];
@@ -187,39 +189,16 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
           ++bad;
       }
     }
-    __syncthreads();
-
-    // B: faces -----------------------------------------------------------------------------
+    // B1: y- and z-faces of plane p (plane p was loaded before the previous barrier), in
+    // the same barrier interval as the loads of plane p + 1 ------------------------------
     {
-      const int c = p + 1;
-      const S* Pn = sP + ((c + 4) & 1) * 8 * NR;
-#pragma unroll
-      for (int s = 0; s < 3; ++s)
-#pragma unroll
-        for (int cc = 0; cc < 7; ++cc) q[s][cc] = q[s + 1][cc];
-      {
-        const int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
-#pragma unroll
-        for (int cc = 0; cc < 7; ++cc) q[3][cc] = Pn[xrow[cc] * NR + col_r];
-      }
-      const int slot = (p + 4) & 1;
+      const int slot = (p + 4) & 1, slot3 = (p + 6) % 3;
       const S* Pp = sP + slot * 8 * NR;
       const S* Bp = sBn + slot * 3 * NR;
-      if (p >= x0) {
-        S L[7], Rt[7], F[7];
-        reconstruct<LIM>(q[0], q[1], q[2], q[3], L, Rt);
-        hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
-        // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
-        sX[col_g] = F[0];
-        sX[G + col_g] = F[5];
-        sX[2 * G + col_g] = F[6];
-#pragma unroll
-        for (int cc = 0; cc < 5; ++cc) fnow[cc] = F[cc];
-      }
       const bool need_yz = p >= x0 - 1 && (p < xe || xn > xe);
       if (need_yz) {
-        S* Y7 = sYZ + (slot * 2 + 0) * 7 * G;
-        S* Z7 = sYZ + (slot * 2 + 1) * 7 * G;
+        S* Y7 = sYZ + (slot3 * 2 + 0) * 7 * G;
+        S* Z7 = sYZ + (slot3 * 2 + 1) * 7 * G;
         {
           // y-face between cells (yj-1, yk) and (yj, yk): frame (y, z, x)
           const int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
@@ -262,11 +241,39 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
     }
     __syncthreads();
 
+    // B2: x-face of plane p (needs plane p + 1 for its stencil) --------------------------
+    {
+      const int c = p + 1;
+      const S* Pn = sP + ((c + 4) & 1) * 8 * NR;
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) q[s][cc] = q[s + 1][cc];
+      {
+        const int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) q[3][cc] = Pn[xrow[cc] * NR + col_r];
+      }
+      const S* Bp = sBn + ((p + 4) & 1) * 3 * NR;
+      if (p >= x0) {
+        S L[7], Rt[7], F[7];
+        reconstruct<LIM>(q[0], q[1], q[2], q[3], L, Rt);
+        hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
+        // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
+        sX[col_g] = F[0];
+        sX[G + col_g] = F[5];
+        sX[2 * G + col_g] = F[6];
+#pragma unroll
+        for (int cc = 0; cc < 5; ++cc) fnow[cc] = F[cc];
+      }
+    }
+    __syncthreads();
+
     // C: edges and cells ----------------------------------------------------------------
     if (p >= x0 && tid < NCORE) {
       const int j = cj, k = ck;
       const int gj = y0 + j, gk = z0 + k;
-      const int sc = (p + 4) & 1, sp = (p + 3) & 1;  // slots of planes p and p-1
+      const int sc = (p + 6) % 3, sp = (p + 5) % 3;  // flux slots of planes p and p-1
       const S* Yc = sYZ + (sc * 2 + 0) * 7 * G;
       const S* Zc = sYZ + (sc * 2 + 1) * 7 * G;
       const S* Yp = sYZ + (sp * 2 + 0) * 7 * G;
@@ -340,7 +347,7 @@ template <typename S>
 int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
   constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int NR = (TY + 4) * (TZ + 4), G = (TY + 1) * (TZ + 1);
-  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 4 * 3 * G + 2 * 2 * 7 * G + 3 * G);
+  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 4 * 3 * G + 3 * 2 * 7 * G + 3 * G);
   if (ntiles <= 0) return kOk;
   if (args.lx <= 0) {
     set_error("stage3d: lx must be positive");
