@@ -333,6 +333,25 @@ __device__ __forceinline__ void reconstruct(const R (&q0)[7], const R (&q1)[7], 
   }
 }
 
+// The same left/right states from the two cells beside the face (q1 | q2) and their
+// limited slopes, already formed (s1 of q1, s2 of q2) -- for a caller that keeps each
+// cell's slope for both of its faces.
+template <typename R>
+__device__ __forceinline__ void reconstruct_sloped(const R (&q1)[7], const R (&q2)[7], const R (&s1)[7],
+                                                   const R (&s2)[7], R (&L)[7], R (&Rt)[7]) {
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    L[c] = q1[c] + R(0.5) * s1[c];
+    Rt[c] = q2[c] - R(0.5) * s2[c];
+  }
+  const bool first_order = L[0] <= R(0) || L[4] <= R(0) || Rt[0] <= R(0) || Rt[4] <= R(0);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    L[c] = first_order ? q1[c] : L[c];
+    Rt[c] = first_order ? q2[c] : Rt[c];
+  }
+}
+
 // CT-contact upwind pick (ct_contact_pyccel.py:17-24).
 template <typename R>
 __device__ __forceinline__ R upwind(R mass, R positive, R negative) {

@@ -103,11 +103,14 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   const int y_g = yj * GZ + (yk + 1);
   const int z_g = (zj + 1) * GZ + zk;
 
-  S q[4][7];  // x-stencil of the column: planes p-2 .. p+1 (x-frame rows)
+  S q[3][7];    // x-stencil of the column: planes p-1 .. p+1 (x-frame rows)
+  S slope[7];   // limited x-slope of plane p-1 (computed one plane earlier)
 #pragma unroll
-  for (int s = 0; s < 4; ++s)
+  for (int s = 0; s < 3; ++s)
 #pragma unroll
     for (int c = 0; c < 7; ++c) q[s][c] = S(1);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) slope[c] = S(0);
   S fprev[5] = {S(0), S(0), S(0), S(0), S(0)};
   S fnow[5] = {S(0), S(0), S(0), S(0), S(0)};
   const S dt = S(a.dt[P.instance]);
@@ -246,18 +249,22 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       const int c = p + 1;
       const S* Pn = sP + ((c + 4) & 1) * 8 * NR;
 #pragma unroll
-      for (int s = 0; s < 3; ++s)
+      for (int s = 0; s < 2; ++s)
 #pragma unroll
         for (int cc = 0; cc < 7; ++cc) q[s][cc] = q[s + 1][cc];
       {
         const int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
 #pragma unroll
-        for (int cc = 0; cc < 7; ++cc) q[3][cc] = Pn[xrow[cc] * NR + col_r];
+        for (int cc = 0; cc < 7; ++cc) q[2][cc] = Pn[xrow[cc] * NR + col_r];
       }
+      // the slope of plane p, kept for face p + 1: each cell's x-slope is formed once
+      S now[7];
+#pragma unroll
+      for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q[1][cc] - q[0][cc], q[2][cc] - q[1][cc]);
       const S* Bp = sBn + ((p + 4) & 1) * 3 * NR;
       if (p >= x0) {
         S L[7], Rt[7], F[7];
-        reconstruct<LIM>(q[0], q[1], q[2], q[3], L, Rt);
+        reconstruct_sloped(q[0], q[1], slope, now, L, Rt);
         hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
         // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
         sX[col_g] = F[0];
@@ -266,6 +273,8 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
 #pragma unroll
         for (int cc = 0; cc < 5; ++cc) fnow[cc] = F[cc];
       }
+#pragma unroll
+      for (int cc = 0; cc < 7; ++cc) slope[cc] = now[cc];
     }
     __syncthreads();
 
