@@ -103,6 +103,15 @@ int wb_stage3d(int precision, const void* src, const void* base, void* dst, cons
                const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
                double b0z, int limiter, int lx, unsigned long long* bad, double* bflux, void* stream);
 
+/* wb_stage2d with the reference's non-ideal terms in the same pass (carafe/mhd.py:844-927):
+ * resistivity eta (carafe/kernels/mhd_resistive/mhd_resistive_pyccel.py:21-67), Braginskii
+ * conduction along / across the field (mhd_conductive_pyccel.py:38-100) and gravity
+ * (gx, gy); all zero gives the ideal kernel. */
+int wb_stage2d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
+                       const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+                       int limiter, double eta, double kappa_par, double kappa_perp, double gx, double gy,
+                       unsigned long long* bad, void* stream);
+
 /* Tile shape of the stage kernels: 2D (TX, TY); 3D (TY, TZ). */
 int wb_tile_shape(int ndim, int precision, int* a, int* b);
 

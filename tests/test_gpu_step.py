@@ -168,6 +168,31 @@ def test_float32_near_degenerate_harris_sheet_tracks_float64():
             assert np.sum(np.abs(b - a)) / np.sum(np.abs(a)) < 1e-6, f
 
 
+def test_fused_step_with_gravity_resistivity_and_conduction_matches_the_reference(runs2d):
+    """The non-ideal terms inside the fused 2D stage kernel (walls + gravity, resistivity,
+    Braginskii conduction) against the reference's own runs; float32 close to them."""
+    from wellbalanced_b200.mhd import MHD2D
+
+    cases = [
+        ("rt8", lambda p: MHD2D.rayleigh_taylor(8, field=0.05, precision=p), 20),
+        ("ot16_resistive", lambda p: MHD2D.orszag_tang(16, resistivity=1e-3, conduction=(1e-2, 1e-3), precision=p), 3),
+        ("rt8_resistive", lambda p: MHD2D.rayleigh_taylor(8, resistivity=1e-3, conduction=(1e-3, 0.0), field=0.05,
+                                                          precision=p), 3),
+    ]
+    for name, make, steps in cases:
+        model = make(64)
+        assert model.engine.physics is not None
+        for _ in range(steps):
+            model.step()
+        close(model.state(), runs2d, name, 1e-12)
+        low = make(32)
+        for _ in range(steps):
+            low.step()
+        state = low.state()
+        for key in ("density", "energy"):
+            assert rel_l1(state[key], runs2d[f"{name}_{key}"]) < 1e-6, (name, key)
+
+
 def test_negative_pressure_is_reported():
     from wellbalanced_b200.mesh import AMRHierarchy
     from wellbalanced_b200.mhd import MHD2D

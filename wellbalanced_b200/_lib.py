@@ -34,6 +34,8 @@ SIGNATURES = {
                    c_dp, c_dp],
     "wb_stage3d": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_double,
                    c_int, c_int, c_dp, c_dp, c_dp],
+    "wb_stage2d_physics": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_int,
+                           c_double, c_double, c_double, c_double, c_double, c_dp, c_dp],
     "wb_tile_shape": [c_int, c_int, c_dp, c_dp],
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],

@@ -187,6 +187,32 @@ int wb_stage2d(int precision, const void* src, const void* base, void* dst, cons
   return launch_stage2d<double>(a, ntiles, limiter, as_stream(stream));
 }
 
+int wb_stage2d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
+                       const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, int limiter,
+                       double eta, double kappa_par, double kappa_perp, double gx, double gy,
+                       unsigned long long* bad, void* stream) {
+  set_error("");
+  if (!precision_ok(precision, "stage2d_physics") ||
+      !ptrs_ok({src, dst, patches, tiles, dt, bad}, "stage2d_physics"))
+    return kBadArgument;
+  if (ntiles < 0 || !(gamma > 1.0) || !(eta >= 0.0) || !(kappa_par >= 0.0) || !(kappa_perp >= 0.0)) {
+    set_error("stage2d_physics: ntiles must be >= 0, gamma > 1, and eta and the conductivities >= 0");
+    return kBadArgument;
+  }
+  if (precision == 32) {
+    StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
+                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
+                       1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, nullptr, 0};
+    a.eta = eta, a.kappa_par = kappa_par, a.kappa_perp = kappa_perp, a.gravity[0] = gx, a.gravity[1] = gy;
+    return launch_stage2d<float>(a, ntiles, limiter, as_stream(stream));
+  }
+  StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
+                      static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
+                      1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, nullptr, 0};
+  a.eta = eta, a.kappa_par = kappa_par, a.kappa_perp = kappa_perp, a.gravity[0] = gx, a.gravity[1] = gy;
+  return launch_stage2d<double>(a, ntiles, limiter, as_stream(stream));
+}
+
 int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
                int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z, int limiter, int lx,
                unsigned long long* bad, double* bflux, void* stream) {

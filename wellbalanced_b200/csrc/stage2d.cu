@@ -36,7 +36,26 @@ __device__ __forceinline__ bool bad_cell(S r, S u, S v, S w, S p, S bx, S by, S 
            isfinite(by) && isfinite(bz));
 }
 
-template <typename S, int LIM>
+// J_z at interior node (ni, nj) of the tile from the face fields in shared memory:
+// dB_y/dx - dB_x/dy (carafe/kernels/mhd_resistive/mhd_resistive_pyccel.py:21-67).
+template <typename S, int CY>
+__device__ __forceinline__ S node_current(const S* sBx, const S* sBy, int ni, int nj, S dx, S idx, S dy, S idy) {
+  using M = Math<S>;
+  return M::div(sBy[(ni + 2) * CY + nj + 2] - sBy[(ni + 1) * CY + nj + 2], dx, idx) -
+         M::div(sBx[(ni + 2) * CY + nj + 2] - sBx[(ni + 2) * CY + nj + 1], dy, idy);
+}
+
+// Temperature p / rho of local cell t.
+template <typename S, int NC>
+__device__ __forceinline__ S temperature(const S* sP, int t) {
+  using M = Math<S>;
+  const S r = sP[t];
+  return M::div(sP[4 * NC + t], r, M::inv(r));
+}
+
+// PHYS: the resistive and Braginskii-conductive face terms and gravity sources of the
+// reference (carafe/mhd.py:844-927) in the same kernel; false for ideal MHD.
+template <typename S, int LIM, bool PHYS>
 __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
   constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
@@ -145,6 +164,56 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
     S L[7], Rt[7], F[7];
     reconstruct<LIM>(q0, q1, q2, q3, L, Rt);
     hlld_flux(L, Rt, bn, gamma, inv_gm1, F);
+    if (PHYS) {
+      // the cells beside the face (local indices) and the step to their transverse neighbours
+      const int ca = base + step, cb = base + 2 * step, across = xface ? 1 : CY;
+      const S hn = xface ? dx : dy, ihn = xface ? idx : idy;   // spacing along the normal
+      const S ht = xface ? dy : dx, iht = xface ? idy : idx;   // and across it
+      const S kpar = S(a.kappa_par), kperp = S(a.kappa_perp), eta = S(a.eta);
+      if (kpar != S(0) || kperp != S(0)) {
+        // heat flux (carafe/kernels/mhd_conductive/mhd_conductive_pyccel.py:38-100):
+        // q = kpar b_n (b_n dT/dn + b_t dT/dt) + kperp dT/dn, dT/dt the MC mean of the two
+        // cells' MC-limited transverse slopes
+        S slope[2];
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          const int c = side == 0 ? ca : cb;
+          const S t0 = temperature<S, NC>(sP, c - across), t1 = temperature<S, NC>(sP, c),
+                  t2 = temperature<S, NC>(sP, c + across);
+          slope[side] = limited_slope<2>(M::div(t2 - t1, ht, iht), M::div(t1 - t0, ht, iht));
+        }
+        const S transverse = limited_slope<2>(slope[0], slope[1]);
+        const int bt_row = xface ? 6 : 5;  // the in-plane tangential field
+        const S bt = S(0.5) * (sP[bt_row * NC + ca] + sP[bt_row * NC + cb]);
+        const S bzf = S(0.5) * (sP[7 * NC + ca] + sP[7 * NC + cb]);
+        const S tiny = sizeof(S) == 4 ? S(1.17549435e-38f) : S(2.2250738585072014e-308);
+        const S magnitude = rmax(rsqrt_(bn * bn + bt * bt + bzf * bzf), tiny);
+        const S im = M::inv(magnitude);
+        const S b_n = M::div(bn, magnitude, im), b_t = M::div(bt, magnitude, im);
+        const S normal = M::div(temperature<S, NC>(sP, cb) - temperature<S, NC>(sP, ca), hn, ihn);
+        F[4] -= kpar * b_n * (b_n * normal + b_t * transverse) + kperp * normal;
+      }
+      if (eta != S(0)) {
+        const S bza = sP[7 * NC + ca], bzb = sP[7 * NC + cb];
+        const S bz_f = S(0.5) * (bza + bzb);
+        if (xface) {
+          // J_y = -dB_z/dx; J_z from the nodes at the face's two ends
+          const S jy = -M::div(bzb - bza, dx, idx);
+          const S by_f = S(0.5) * (sP[6 * NC + ca] + sP[6 * NC + cb]);
+          const S jz_f = S(0.5) * (node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy) +
+                                   node_current<S, CY>(sBx, sBy, fi, fj + 1, dx, idx, dy, idy));
+          F[6] += eta * jy;
+          F[4] += eta * (jy * bz_f - jz_f * by_f);
+        } else {
+          const S jx = M::div(bzb - bza, dy, idy);
+          const S bx_f = S(0.5) * (sP[5 * NC + ca] + sP[5 * NC + cb]);
+          const S jz_f = S(0.5) * (node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy) +
+                                   node_current<S, CY>(sBx, sBy, fi + 1, fj, dx, idx, dy, idy));
+          F[6] += -eta * jx;
+          F[4] += eta * (jz_f * bx_f - jx * bz_f);
+        }
+      }
+    }
     // walls: nothing but the pressure crosses (carafe/mhd.py:874-886)
     bool wall;
     if (xface) {
@@ -179,6 +248,7 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
                      sFx[ni * FY + nj + 1], sFy[5 * NF + ni * FY + nj], sFy[5 * NF + (ni + 1) * FY + nj],
                      sFy[ni * FY + nj], sFy[(ni + 1) * FY + nj], sE[(ni + 1) * CY + nj + 1],
                      sE[(ni + 2) * CY + nj + 1], sE[(ni + 1) * CY + nj + 2], sE[(ni + 2) * CY + nj + 2]);
+      if (PHYS && a.eta != 0.0) ez += S(a.eta) * node_current<S, CY>(sBx, sBy, ni, nj, dx, idx, dy, idy);
       const bool wall = ((P.flags & kWallLo0) && gx == 0) || ((P.flags & kWallHi0) && gx == nx) ||
                         ((P.flags & kWallLo1) && gy == 0) || ((P.flags & kWallHi1) && gy == ny);
       if (wall) ez = S(0);
@@ -196,6 +266,13 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
         const S div = M::div(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1], dx, idx) +
                       M::div(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj], dy, idy);
         S value = src[q * fs + cell] - dt * div;
+        if (PHYS) {
+          // gravity: rho g on the momentum, m . g on the energy, from the stage's input
+          const S gx = S(a.gravity[0]), gy = S(a.gravity[1]);
+          if (q == 1) value += dt * (src[cell] * gx);
+          if (q == 2) value += dt * (src[cell] * gy);
+          if (q == 4) value += dt * (src[fs + cell] * gx + src[2 * fs + cell] * gy);
+        }
         if (base_state) value = (value + base_state[q * fs + cell]) * S(0.5);
         dst[q * fs + cell] = value;
       }
@@ -226,11 +303,18 @@ int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream
   constexpr int NC = (TX + 4) * (TY + 4), NF = (TX + 1) * (TY + 1);
   const size_t smem = sizeof(S) * (11 * NC + 14 * NF);
   if (ntiles <= 0) return kOk;
+  const bool phys = args.eta != 0.0 || args.kappa_par != 0.0 || args.kappa_perp != 0.0 || args.gravity[0] != 0.0 ||
+                    args.gravity[1] != 0.0;
   switch (limiter) {
-#define WB_CASE(L)                                                                                   \
-  case L:                                                                                            \
-    cudaFuncSetAttribute(stage2d_kernel<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-    stage2d_kernel<S, L><<<ntiles, 256, smem, stream>>>(args);                                       \
+#define WB_CASE(L)                                                                                           \
+  case L:                                                                                                    \
+    if (phys) {                                                                                              \
+      cudaFuncSetAttribute(stage2d_kernel<S, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+      stage2d_kernel<S, L, true><<<ntiles, 256, smem, stream>>>(args);                                       \
+    } else {                                                                                                 \
+      cudaFuncSetAttribute(stage2d_kernel<S, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+      stage2d_kernel<S, L, false><<<ntiles, 256, smem, stream>>>(args);                                      \
+    }                                                                                                        \
     break;
     WB_CASE(0)
     WB_CASE(1)

@@ -110,6 +110,8 @@ class Engine:
         self.launches = 0
         #: optional list collecting (start, end) CUDA events around each stage kernel
         self.stage_events = None
+        #: 2D non-ideal terms (eta, kappa_par, kappa_perp, gx, gy), None for ideal MHD
+        self.physics = None
 
     # low-level launches ----------------------------------------------------------------------
     def _s(self):
@@ -159,7 +161,11 @@ class Engine:
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             start.record(torch.cuda.current_stream(self.device) if self.stream is None else self.stream)
         self.launches += 1
-        if self.ndim == 2:
+        if self.ndim == 2 and self.physics is not None:
+            _lib.call("wb_stage2d_physics", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
+                      dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
+                      self.gamma, b[0], b[1], self.limiter, *self.physics, self.bad.data_ptr(), s)
+        elif self.ndim == 2:
             _lib.call("wb_stage2d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
                       self.gamma, b[0], b[1], self.limiter, self.bad.data_ptr(),

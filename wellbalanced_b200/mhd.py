@@ -87,11 +87,6 @@ class MHD2D:
             if kind == "wall" and mean_field[axis] != 0.0:
                 raise ValueError(f"a wall normal to {axis_name} needs a zero mean field along it")
             kinds[axis_name] = kind
-        if self._fused and (resistivity or max(conduction) > 0.0 or gravity[0] or gravity[1]):
-            raise NotImplementedError(
-                "the fused device step covers ideal MHD; resistivity, conduction and gravity "
-                "run through wellbalanced_b200.plain.PlainMHD2D"
-            )
         self.hierarchy = hierarchy
         self.gamma = float(gamma)
         self.mean_field = (float(mean_field[0]), float(mean_field[1]))
@@ -130,6 +125,14 @@ class MHD2D:
         groups = self.engine.layout.groups
         self._groups_all = groups
         self._groups_potential = groups[1:]
+        physics = (self.resistivity, self.conduction[0], self.conduction[1], self.gravity[0], self.gravity[1])
+        if any(physics):
+            if self._fused and self.hierarchy.max_level > 0:
+                raise NotImplementedError(
+                    "resistivity, conduction and gravity run on one level: the flux register does not "
+                    "carry their face terms yet"
+                )
+            self.engine.physics = tuple(float(v) for v in physics)
 
     # construction of common cases (carafe/mhd.py:486-671) -----------------------------------------
     @classmethod
@@ -157,6 +160,26 @@ class MHD2D:
         )
         model.period = float(wavelength)
         return model, model.dataset()
+
+    @classmethod
+    def rayleigh_taylor(cls, cells: int, *, field: float = 0.0, amplitude: float = 0.01, **options: Any) -> MHD2D:
+        """Single-mode Rayleigh-Taylor instability on ``cells x 3 cells`` (``carafe/mhd.py:626-671``):
+        density 2 over 1 on [-0.25, 0.25] x [-0.75, 0.75], periodic in x, walls in y, gravity
+        -0.1 along y, pressure 2.5 - 0.1 rho y, gamma 1.4, v_y = amplitude (1 + cos 4 pi x)
+        (1 + cos 3 pi y) / 4, uniform field ``field`` along x."""
+        hierarchy = AMRHierarchy((cells, 3 * cells), ((-0.25, 0.25), (-0.75, 0.75)), periodic=(True, False))
+        options = {"gamma": 1.4, **options}
+        model = cls(hierarchy, mean_field=(field, 0.0), gravity=(0.0, -0.1), boundaries={"y": "wall"}, **options)
+
+        def density(x, y):
+            return np.where(y > 0.0, 2.0, 1.0)
+
+        def velocity(x, y):
+            rise = amplitude * (1.0 + np.cos(4.0 * np.pi * x)) * (1.0 + np.cos(3.0 * np.pi * y)) / 4.0
+            return (0.0 * x, rise, 0.0 * x)
+
+        model.set_state(density, velocity, lambda x, y: 2.5 - 0.1 * density(x, y) * y)
+        return model
 
     @classmethod
     def orszag_tang(cls, cells: int, **options: Any) -> MHD2D:
