@@ -380,3 +380,36 @@ def test_autotuned_x_march_gives_the_same_steps():
         fixed.step(tuned.step())
     torch.cuda.synchronize()
     assert torch.equal(tuned.engine.state, fixed.engine.state)
+
+
+def test_plain_3d_resistivity_and_gravity_match_the_reference(runs3d):
+    """The per-kernel float64 3D path with resistivity (the reference's own run) and with
+    gravity (against the oracle's 3D step, which restates carafe/mhd3d.py:635-671)."""
+    from oracle.mesh import Hierarchy
+    from oracle.mhd3d import MHD3D as OracleMHD3D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.plain import PlainMHD3D
+
+    k = 2.0 * np.pi
+    model = PlainMHD3D(AMRHierarchy((4, 4, 16), ((0.0, 1.0),) * 3, periodic=(True,) * 3), resistivity=0.01)
+    model.set_state(1.0, (0.0, 0.0, 0.0), 1.0,
+                    vector_potential=(lambda x, y, z: np.cos(k * z) / k, lambda x, y, z: np.sin(k * z) / k, 0.0))
+    for _ in range(5):
+        model.step()
+    close(model.state(), runs3d, "resistive3d", 1e-12)
+
+    def state(m):
+        m.set_state(lambda x, y, z: 1.0 + 0.3 * (z > 0.5), (0.0, 0.0, lambda x, y, z: 0.05 * np.sin(k * x)),
+                    lambda x, y, z: 2.0 - 0.2 * z,
+                    vector_potential=(0.0, lambda x, y, z: 0.05 * np.cos(k * x) / k, 0.0))
+        return m
+
+    options = dict(gravity=(0.0, 0.0, -0.2), resistivity=0.005, limiter="minmod", mean_field=(0.0, 0.0, 0.1))
+    device = state(PlainMHD3D(AMRHierarchy((6, 6, 8), ((0.0, 1.0),) * 3, periodic=(True,) * 3), **options))
+    oracle = state(OracleMHD3D(Hierarchy((6, 6, 8), ((0.0, 1.0),) * 3, (True,) * 3), **options))
+    for _ in range(4):
+        device.step(oracle.step())
+    want = oracle.state()
+    got = device.state()
+    for key in want:
+        np.testing.assert_allclose(got[key], want[key], rtol=1e-12, atol=1e-12, err_msg=key)

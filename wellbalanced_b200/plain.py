@@ -262,12 +262,63 @@ class PlainMHD3D(MHD3D):
             for row, axis in zip((1, 2, 3), frame, strict=True):
                 fluxes[("momentum_x", "momentum_y", "momentum_z")[axis]].append(block[row])
             fluxes["energy"].append(block[4])
+        if self.resistivity:
+            self._resistive(faces, patch, edges, fluxes["energy"])
         return fluxes, edges
+
+    def _resistive(self, faces, patch, edges, energy):
+        """eta J on the edge field, eta J x B on the energy fluxes (carafe/mhd3d.py:561-602).
+
+        J_c = d_a B_b - d_b B_a on the c-edges of the block from the haloed face fields; a
+        face normal to s gains eta (J_b B_c - J_c B_b), J the mean of the face's two edges
+        along each direction and B the mean of the four faces around it.
+        """
+        h = HALO
+        eta = self.resistivity
+        spacing = self.hierarchy.spacing(patch.level)
+        shape = patch.shape
+        current = []
+        for c in range(3):
+            _, a, b = _cyclic(c)
+            total = 0.0
+            for axis, field, sign in ((a, faces[b], 1.0), (b, faces[a], -1.0)):
+                derivative = torch.diff(field, dim=axis) / spacing[axis]
+                index = [slice(h, h + shape[i]) for i in range(3)]
+                index[a] = slice(h, h + shape[a] + 1)
+                index[b] = slice(h, h + shape[b] + 1)
+                index[axis] = slice(h - 1, h + shape[axis])
+                total = total + sign * derivative[tuple(index)]
+            current.append(total)
+        for c in range(3):
+            edges[c] = edges[c] + eta * current[c]
+
+        def pair_mean(t, axis, start, count):
+            return 0.5 * (t.narrow(axis, start, count) + t.narrow(axis, start + 1, count))
+
+        def field_at_face(face, normal, node):
+            face = pair_mean(face, normal, h - 1, shape[normal] + 1)  # cells -> nodes along the normal
+            face = pair_mean(face, node, h, shape[node])  # nodes -> cells along the face's own axis
+            other = 3 - normal - node
+            return face.narrow(other, h, shape[other])
+
+        for s in range(3):
+            _, b, c = _cyclic(s)
+            jb = pair_mean(current[b], c, 0, shape[c])
+            jc = pair_mean(current[c], b, 0, shape[b])
+            energy[s] = energy[s] + eta * (jb * field_at_face(faces[c], s, c) - jc * field_at_face(faces[b], s, b))
 
     def _advance(self, dt, scale):
         eng = self.engine
         eng.fill(eng.state)
         results = {p.index: self._patch_fluxes(p) for p in self.hierarchy.patches}
+        g = self.gravity
+        sources = {}
+        if any(g):
+            # rho g on the momentum and m . g on the energy, from the stage's input state
+            for p in self.hierarchy.patches:
+                rho = self._read(p, 0).clone()
+                work = sum(self._read(p, 1 + a) * ga for a, ga in enumerate(g))
+                sources[p.index] = (rho, work.clone())
         for p in self.hierarchy.patches:
             spacing = self.hierarchy.spacing(p.level)
             fluxes, edges = results[p.index]
@@ -279,6 +330,12 @@ class PlainMHD3D(MHD3D):
             for c in range(3):
                 extra = ((0, 1, 1), (1, 0, 1), (1, 1, 0))[c]
                 self._read(p, 5 + c, extra).sub_(dt * edges[c])
+            if any(g):
+                rho, work = sources[p.index]
+                for a, ga in enumerate(g):
+                    if ga:
+                        self._read(p, 1 + a).add_(dt * ga * rho)
+                self._read(p, 4).add_(dt * work)
 
     def stable_step(self):
         self._check_ready()
