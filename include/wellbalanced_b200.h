@@ -144,6 +144,13 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
  * fine patches takes its corrections from separate calls (one per axis and side). */
 int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
                      double b0y, double b0z, double gamma, int limiter, double* reg, void* stream);
+/* The same register update for a 2D hierarchy with the non-ideal face terms of
+ * wb_stage2d_physics: each recomputed face flux carries the resistive eta J terms and the
+ * Braginskii heat flux, as the reference's fluxes do when its register records them
+ * (carafe/mhd.py:866-872, 906-919). Every op must be a 2D interface. */
+int wb_face_flux_ops_physics(int precision, const void* pool, const void* patches, const void* ops, int nops,
+                             double b0x, double b0y, double gamma, int limiter, double eta, double kappa_par,
+                             double kappa_perp, double* reg, void* stream);
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
                     const double* dt, void* stream);
 

@@ -27,7 +27,7 @@ def _refined_state():
     )
 
 
-def _pair(cells=16, precision=64):
+def _pair(cells=16, precision=64, **options):
     from oracle.mesh import Hierarchy
     from oracle.mhd2d import MHD2D as OracleMHD2D
     from wellbalanced_b200.mesh import AMRHierarchy
@@ -38,8 +38,8 @@ def _pair(cells=16, precision=64):
     oh.add_patch(1, box)
     dh = AMRHierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True))
     dh.add_patch(1, box)
-    oracle = OracleMHD2D(oh, limiter="minmod")
-    device = MHD2D(dh, limiter="minmod", precision=precision)
+    oracle = OracleMHD2D(oh, limiter="minmod", **options)
+    device = MHD2D(dh, limiter="minmod", precision=precision, **options)
     state = _refined_state()
     oracle.set_state(state["density"], state["velocity"], state["pressure"],
                      vector_potential=state["vector_potential"], bz=state["bz"])
@@ -59,6 +59,32 @@ def test_refined_2d_matches_the_oracle_patch_by_patch():
                                        err_msg=f"level {op.level} {name}")
         np.testing.assert_allclose(device.gather(dp, 6, node=True), op.field(oracle.potential).local,
                                    rtol=1e-11, atol=1e-12)
+
+
+def test_refined_2d_with_resistivity_conduction_and_gravity_matches_the_oracle():
+    """The flux register carries the resistive and conductive face terms (the reference
+    records its fluxes after adding them, carafe/mhd.py:866-872, 906-919): the refined
+    non-ideal step matches the oracle's patch by patch, and without gravity the composite
+    totals stay at round-off."""
+    physics = dict(resistivity=2e-3, conduction=(2e-2, 1e-3), mean_field=(0.1, 0.05))
+    oracle, device = _pair(gravity=(0.05, -0.1), **physics)
+    for _ in range(12):
+        dt = oracle.step()
+        device.step(dt)
+    for op, dp in zip(oracle.hierarchy.patches, device.hierarchy.patches, strict=True):
+        for f, name in enumerate(oracle.names.values()):
+            np.testing.assert_allclose(device.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                       err_msg=f"level {op.level} {name}")
+        np.testing.assert_allclose(device.gather(dp, 6, node=True), op.field(oracle.potential).local,
+                                   rtol=1e-11, atol=1e-12)
+    _, model = _pair(**physics)
+    before = model.totals()
+    for _ in range(20):
+        model.step()
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-12, name
+    assert model.divergence() < 1e-14
 
 
 def test_refined_2d_conserves_and_keeps_div_b_zero():

@@ -312,23 +312,43 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
                                      static_cast<const RestrictOp*>(ops), nops, as_stream(stream));
 }
 
-int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
-                     double b0y, double b0z, double gamma, int limiter, double* reg, void* stream) {
-  set_error("");
+static int face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops,
+                         const double* b0, double gamma, int limiter, const double* physics, double* reg,
+                         void* stream) {
   if (!precision_ok(precision, "face_flux_ops") || (nops > 0 && !ptrs_ok({pool, patches, ops, reg}, "face_flux_ops")))
     return kBadArgument;
   if (limiter < 0 || limiter > 3) {
     set_error("face_flux_ops: limiter code %d is not one of 0..3", limiter);
     return kBadArgument;
   }
-  const double b0[3] = {b0x, b0y, b0z};
   if (precision == 32)
     return launch_face_flux_ops<float>(static_cast<const float*>(pool), static_cast<const PatchDesc*>(patches),
-                                       static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, reg,
+                                       static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, reg,
                                        as_stream(stream));
   return launch_face_flux_ops<double>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
-                                      static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, reg,
+                                      static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, reg,
                                       as_stream(stream));
+}
+
+int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
+                     double b0y, double b0z, double gamma, int limiter, double* reg, void* stream) {
+  set_error("");
+  const double b0[3] = {b0x, b0y, b0z};
+  return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, nullptr, reg, stream);
+}
+
+int wb_face_flux_ops_physics(int precision, const void* pool, const void* patches, const void* ops, int nops,
+                             double b0x, double b0y, double gamma, int limiter, double eta, double kappa_par,
+                             double kappa_perp, double* reg, void* stream) {
+  set_error("");
+  if (!(eta >= 0.0) || !(kappa_par >= 0.0) || !(kappa_perp >= 0.0)) {
+    set_error("face_flux_ops_physics: eta %g, kappa_par %g, kappa_perp %g must be non-negative", eta, kappa_par,
+              kappa_perp);
+    return kBadArgument;
+  }
+  const double b0[3] = {b0x, b0y, 0.0};
+  const double physics[3] = {eta, kappa_par, kappa_perp};
+  return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, physics, reg, stream);
 }
 
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,

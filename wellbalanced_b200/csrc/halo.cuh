@@ -75,7 +75,7 @@ template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream);
 template <typename S>
 int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
-                         double gamma, int limiter, double* reg, cudaStream_t stream);
+                         double gamma, int limiter, const double* physics, double* reg, cudaStream_t stream);
 template <typename S>
 int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
                         const double* dt, cudaStream_t stream);

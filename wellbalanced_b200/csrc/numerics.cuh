@@ -352,6 +352,46 @@ __device__ __forceinline__ void reconstruct_sloped(const R (&q1)[7], const R (&q
   }
 }
 
+// The resistive and Braginskii-conductive terms of a 2D face, added to its HLLD flux F
+// (frame of the face; rows 4 energy, 6 B_z), in the reference's order: the heat flux
+// q = kpar b_n (b_n dT/dn + b_t dT/dt) + kperp dT/dn is subtracted
+// (carafe/kernels/mhd_conductive/mhd_conductive_pyccel.py:38-100), then eta J terms are
+// added (mhd_resistive_pyccel.py:21-67). Inputs: the cells a | b beside the face, their
+// temperatures and MC-limited transverse temperature slopes, their in-plane tangential
+// field (B_y on an x-face, B_x on a y-face) and B_z, the normal face field bn, J_z at the
+// face's two end nodes (lower first), the spacing along the normal.
+template <typename S>
+__device__ __forceinline__ void nonideal_face_terms(bool xface, S bn, S t_a, S t_b, S slope_a, S slope_b, S bt_a,
+                                                    S bt_b, S bz_a, S bz_b, S jz_0, S jz_1, S hn, S ihn, S eta,
+                                                    S kpar, S kperp, S (&F)[7]) {
+  using M = Math<S>;
+  if (kpar != S(0) || kperp != S(0)) {
+    const S transverse = limited_slope<2>(slope_a, slope_b);
+    const S bt = S(0.5) * (bt_a + bt_b);
+    const S bzf = S(0.5) * (bz_a + bz_b);
+    const S tiny = sizeof(S) == 4 ? S(1.17549435e-38f) : S(2.2250738585072014e-308);
+    const S magnitude = rmax(rsqrt_(bn * bn + bt * bt + bzf * bzf), tiny);
+    const S im = M::inv(magnitude);
+    const S b_n = M::div(bn, magnitude, im), b_t = M::div(bt, magnitude, im);
+    const S normal = M::div(t_b - t_a, hn, ihn);
+    F[4] -= kpar * b_n * (b_n * normal + b_t * transverse) + kperp * normal;
+  }
+  if (eta != S(0)) {
+    const S bz_f = S(0.5) * (bz_a + bz_b);
+    const S bt_f = S(0.5) * (bt_a + bt_b);
+    const S jz_f = S(0.5) * (jz_0 + jz_1);
+    if (xface) {
+      const S jy = -M::div(bz_b - bz_a, hn, ihn);  // J_y = -dB_z/dx
+      F[6] += eta * jy;
+      F[4] += eta * (jy * bz_f - jz_f * bt_f);
+    } else {
+      const S jx = M::div(bz_b - bz_a, hn, ihn);  // J_x = dB_z/dy
+      F[6] += -eta * jx;
+      F[4] += eta * (jz_f * bt_f - jx * bz_f);
+    }
+  }
+}
+
 // CT-contact upwind pick (ct_contact_pyccel.py:17-24).
 template <typename R>
 __device__ __forceinline__ R upwind(R mass, R positive, R negative) {

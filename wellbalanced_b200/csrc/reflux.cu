@@ -71,9 +71,49 @@ __device__ void cell_primitive(const S* src, const PatchDesc& P, int ndim, int i
 // The flux through the lower face along `axis` of haloed cell (i, j, k), in the frame of
 // that axis; conserved rows returned in physical order (2D: rho, mx, my, mz, E, Bz; 3D:
 // rho, mx, my, mz, E), computed in the state's precision like the stage kernels.
-template <typename S, int LIM>
+// The fields at the lower x- and y-faces of haloed 2D cell offset o (as the stage kernel forms them).
+template <typename S>
+__device__ __forceinline__ void lower_face_fields(const S* A, int64_t o, int64_t p0, S dx, S idx, S dy, S idy,
+                                                  const double* b0, S& bxl, S& byl) {
+  using M = Math<S>;
+  bxl = M::div(A[o + 1] - A[o], dy, idy) + S(b0[0]);
+  byl = -M::div(A[o + p0] - A[o], dx, idx) + S(b0[1]);
+}
+
+// J_z = dB_y/dx - dB_x/dy at haloed 2D node (i, j), the lower-left corner of cell (i, j),
+// from the four faces around it (carafe/kernels/mhd_resistive/mhd_resistive_pyccel.py:21-30).
+template <typename S>
+__device__ S node_current(const S* src, const PatchDesc& P, int i, int j, const double* b0) {
+  using M = Math<S>;
+  const S* A = src + 6 * P.fstride;
+  const int64_t p0 = P.pitch0, o = cell_offset(P, i, j, 0);
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+  const S idx = M::inv(dx), idy = M::inv(dy);
+  S bx, by, bx_below, by_left, unused;
+  lower_face_fields(A, o, p0, dx, idx, dy, idy, b0, bx, by);
+  lower_face_fields(A, o - p0, p0, dx, idx, dy, idy, b0, unused, by_left);
+  lower_face_fields(A, o - 1, p0, dx, idx, dy, idy, b0, bx_below, unused);
+  return M::div(by - by_left, dx, idx) - M::div(bx - bx_below, dy, idy);
+}
+
+// Temperature p / rho of haloed 2D cell (i, j).
+template <typename S>
+__device__ S cell_temperature(const S* src, const PatchDesc& P, int i, int j, const double* b0, double gamma) {
+  using M = Math<S>;
+  S q[8], unused;
+  cell_primitive<S>(src, P, 2, i, j, 0, 0, b0, gamma, q, unused);
+  return M::div(q[4], q[0], M::inv(q[0]));
+}
+
+// The non-ideal coefficients of the 2D face fluxes: resistivity and the parallel and
+// perpendicular conductivities.
+struct FacePhysics {
+  double eta, kappa_par, kappa_perp;
+};
+
+template <typename S, int LIM, bool PHYS>
 __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, int i, int j, int k,
-                          const double* b0, double gamma, double (&out)[6]) {
+                          const double* b0, double gamma, const FacePhysics& phys, double (&out)[6]) {
   int comp[7], rows[6];
   int ncons;
   if (ndim == 2) {
@@ -120,15 +160,44 @@ __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, 
   S L[7], Rt[7], F[7];
   reconstruct<LIM>(qs[0], qs[1], qs[2], qs[3], L, Rt);
   hlld_flux(L, Rt, bn, S(gamma), S(1.0 / (gamma - 1.0)), F);
+  if (PHYS && ndim == 2) {
+    // the resistive and conductive terms, with the stage kernel's arithmetic: cells a | b
+    // are qs[1] | qs[2] (haloed cells (i-1, j) | (i, j) on an x-face, (i, j-1) | (i, j) on a y-face)
+    using M = Math<S>;
+    const bool xface = axis == 0;
+    const S dx = S(P.dx[0]), dy = S(P.dx[1]);
+    const S idx = M::inv(dx), idy = M::inv(dy);
+    const S ht = xface ? dy : dx, iht = xface ? idy : idx;
+    S slope[2] = {S(0), S(0)};
+    if (phys.kappa_par != 0.0 || phys.kappa_perp != 0.0) {
+      for (int side = 0; side < 2; ++side) {
+        const int ci = xface ? i - 1 + side : i, cj = xface ? j : j - 1 + side;
+        const int ti = xface ? 0 : 1, tj = xface ? 1 : 0;  // step to the transverse neighbours
+        const S t0 = cell_temperature<S>(src, P, ci - ti, cj - tj, b0, gamma);
+        const S t2 = cell_temperature<S>(src, P, ci + ti, cj + tj, b0, gamma);
+        const S t1 = M::div(qs[1 + side][4], qs[1 + side][0], M::inv(qs[1 + side][0]));
+        slope[side] = limited_slope<2>(M::div(t2 - t1, ht, iht), M::div(t1 - t0, ht, iht));
+      }
+    }
+    S jz_0 = S(0), jz_1 = S(0);
+    if (phys.eta != 0.0) {
+      jz_0 = node_current<S>(src, P, i, j, b0);
+      jz_1 = xface ? node_current<S>(src, P, i, j + 1, b0) : node_current<S>(src, P, i + 1, j, b0);
+    }
+    const S t_a = M::div(qs[1][4], qs[1][0], M::inv(qs[1][0]));
+    const S t_b = M::div(qs[2][4], qs[2][0], M::inv(qs[2][0]));
+    nonideal_face_terms(xface, bn, t_a, t_b, slope[0], slope[1], qs[1][5], qs[2][5], qs[1][6], qs[2][6], jz_0, jz_1,
+                        xface ? dx : dy, xface ? idx : idy, S(phys.eta), S(phys.kappa_par), S(phys.kappa_perp), F);
+  }
   for (int t = 0; t < ncons; ++t) out[t] = double(F[rows[t]]);
 }
 
 // One thread per coarse face of an interface: reg[slot] += mean of the fine faces over
 // it - the coarse face (each op holds both sides, so no two threads share a slot).
-template <typename S, int LIM>
+template <typename S, int LIM, bool PHYS>
 __global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc* __restrict__ patches,
                                      const FaceFluxOp* __restrict__ ops, double b0x, double b0y, double b0z,
-                                     double gamma, double* __restrict__ reg) {
+                                     double gamma, FacePhysics phys, double* __restrict__ reg) {
   const FaceFluxOp op = ops[blockIdx.x];
   const PatchDesc C = patches[op.coarse];
   const PatchDesc F = patches[op.fine];
@@ -142,7 +211,7 @@ __global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc
     idx[op.t1] = op.coarse_t0[0] + s1;
     if (op.ndim == 3) idx[op.t2] = op.coarse_t0[1] + s2;
     double coarse[6];
-    face_flux<S, LIM>(pool + C.off, C, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, coarse);
+    face_flux<S, LIM, PHYS>(pool + C.off, C, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, phys, coarse);
     double fine[6] = {0, 0, 0, 0, 0, 0};
     for (int a = 0; a < fine_a; ++a)
       for (int b = 0; b < fine_b; ++b) {
@@ -151,7 +220,7 @@ __global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc
         f[op.t1] = op.fine_t0[0] + 2 * s1 + a;
         if (op.ndim == 3) f[op.t2] = op.fine_t0[1] + 2 * s2 + b;
         double g[6];
-        face_flux<S, LIM>(pool + F.off, F, op.ndim, op.axis, f[0], f[1], f[2], b0, gamma, g);
+        face_flux<S, LIM, PHYS>(pool + F.off, F, op.ndim, op.axis, f[0], f[1], f[2], b0, gamma, phys, g);
         for (int q = 0; q < ncons; ++q) fine[q] += g[q];
       }
     const double count = double(fine_a * fine_b);
@@ -184,16 +253,29 @@ __global__ void reflux_apply_kernel(S* __restrict__ pool, const PatchDesc* __res
   }
 }
 
+template <typename S, bool PHYS>
+void launch_face_flux_kernel(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops,
+                             const double* b0, double gamma, int limiter, const FacePhysics& phys, double* reg,
+                             cudaStream_t stream) {
+  switch (limiter) {
+    case 0: face_flux_ops_kernel<S, 0, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 1: face_flux_ops_kernel<S, 1, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 2: face_flux_ops_kernel<S, 2, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    default: face_flux_ops_kernel<S, 3, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+  }
+}
+
+// physics: null for ideal MHD, else {eta, kappa_par, kappa_perp} (2D interfaces only)
 template <typename S>
 int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
-                         double gamma, int limiter, double* reg, cudaStream_t stream) {
+                         double gamma, int limiter, const double* physics, double* reg, cudaStream_t stream) {
   if (nops <= 0) return kOk;
-  switch (limiter) {
-    case 0: face_flux_ops_kernel<S, 0><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
-    case 1: face_flux_ops_kernel<S, 1><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
-    case 2: face_flux_ops_kernel<S, 2><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
-    default: face_flux_ops_kernel<S, 3><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, reg); break;
-  }
+  if (physics && (physics[0] != 0.0 || physics[1] != 0.0 || physics[2] != 0.0))
+    launch_face_flux_kernel<S, true>(pool, patches, ops, nops, b0, gamma, limiter,
+                                     FacePhysics{physics[0], physics[1], physics[2]}, reg, stream);
+  else
+    launch_face_flux_kernel<S, false>(pool, patches, ops, nops, b0, gamma, limiter, FacePhysics{0.0, 0.0, 0.0}, reg,
+                                      stream);
   return check_launch("face flux ops");
 }
 
@@ -205,9 +287,9 @@ int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, 
 }
 
 template int launch_face_flux_ops<float>(const float*, const PatchDesc*, const FaceFluxOp*, int, const double*, double,
-                                         int, double*, cudaStream_t);
+                                         int, const double*, double*, cudaStream_t);
 template int launch_face_flux_ops<double>(const double*, const PatchDesc*, const FaceFluxOp*, int, const double*,
-                                          double, int, double*, cudaStream_t);
+                                          double, int, const double*, double*, cudaStream_t);
 template int launch_reflux_apply<float>(float*, const PatchDesc*, const RefluxOp*, int, double*, const double*,
                                         cudaStream_t);
 template int launch_reflux_apply<double>(double*, const PatchDesc*, const RefluxOp*, int, double*, const double*,

@@ -167,52 +167,28 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
     if (PHYS) {
       // the cells beside the face (local indices) and the step to their transverse neighbours
       const int ca = base + step, cb = base + 2 * step, across = xface ? 1 : CY;
-      const S hn = xface ? dx : dy, ihn = xface ? idx : idy;   // spacing along the normal
-      const S ht = xface ? dy : dx, iht = xface ? idy : idx;   // and across it
-      const S kpar = S(a.kappa_par), kperp = S(a.kappa_perp), eta = S(a.eta);
-      if (kpar != S(0) || kperp != S(0)) {
-        // heat flux (carafe/kernels/mhd_conductive/mhd_conductive_pyccel.py:38-100):
-        // q = kpar b_n (b_n dT/dn + b_t dT/dt) + kperp dT/dn, dT/dt the MC mean of the two
-        // cells' MC-limited transverse slopes
-        S slope[2];
+      const S ht = xface ? dy : dx, iht = xface ? idy : idx;  // spacing across the face's normal
+      S slope_a = S(0), slope_b = S(0);
+      if (a.kappa_par != 0.0 || a.kappa_perp != 0.0) {
+        // MC-limited transverse temperature slopes of the two cells
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
           const int c = side == 0 ? ca : cb;
           const S t0 = temperature<S, NC>(sP, c - across), t1 = temperature<S, NC>(sP, c),
                   t2 = temperature<S, NC>(sP, c + across);
-          slope[side] = limited_slope<2>(M::div(t2 - t1, ht, iht), M::div(t1 - t0, ht, iht));
-        }
-        const S transverse = limited_slope<2>(slope[0], slope[1]);
-        const int bt_row = xface ? 6 : 5;  // the in-plane tangential field
-        const S bt = S(0.5) * (sP[bt_row * NC + ca] + sP[bt_row * NC + cb]);
-        const S bzf = S(0.5) * (sP[7 * NC + ca] + sP[7 * NC + cb]);
-        const S tiny = sizeof(S) == 4 ? S(1.17549435e-38f) : S(2.2250738585072014e-308);
-        const S magnitude = rmax(rsqrt_(bn * bn + bt * bt + bzf * bzf), tiny);
-        const S im = M::inv(magnitude);
-        const S b_n = M::div(bn, magnitude, im), b_t = M::div(bt, magnitude, im);
-        const S normal = M::div(temperature<S, NC>(sP, cb) - temperature<S, NC>(sP, ca), hn, ihn);
-        F[4] -= kpar * b_n * (b_n * normal + b_t * transverse) + kperp * normal;
-      }
-      if (eta != S(0)) {
-        const S bza = sP[7 * NC + ca], bzb = sP[7 * NC + cb];
-        const S bz_f = S(0.5) * (bza + bzb);
-        if (xface) {
-          // J_y = -dB_z/dx; J_z from the nodes at the face's two ends
-          const S jy = -M::div(bzb - bza, dx, idx);
-          const S by_f = S(0.5) * (sP[6 * NC + ca] + sP[6 * NC + cb]);
-          const S jz_f = S(0.5) * (node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy) +
-                                   node_current<S, CY>(sBx, sBy, fi, fj + 1, dx, idx, dy, idy));
-          F[6] += eta * jy;
-          F[4] += eta * (jy * bz_f - jz_f * by_f);
-        } else {
-          const S jx = M::div(bzb - bza, dy, idy);
-          const S bx_f = S(0.5) * (sP[5 * NC + ca] + sP[5 * NC + cb]);
-          const S jz_f = S(0.5) * (node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy) +
-                                   node_current<S, CY>(sBx, sBy, fi + 1, fj, dx, idx, dy, idy));
-          F[6] += -eta * jx;
-          F[4] += eta * (jz_f * bx_f - jx * bz_f);
+          (side == 0 ? slope_a : slope_b) = limited_slope<2>(M::div(t2 - t1, ht, iht), M::div(t1 - t0, ht, iht));
         }
       }
+      S jz_0 = S(0), jz_1 = S(0);
+      if (a.eta != 0.0) {
+        jz_0 = node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy);
+        jz_1 = xface ? node_current<S, CY>(sBx, sBy, fi, fj + 1, dx, idx, dy, idy)
+                     : node_current<S, CY>(sBx, sBy, fi + 1, fj, dx, idx, dy, idy);
+      }
+      const int bt_row = xface ? 6 : 5;  // the in-plane tangential field
+      nonideal_face_terms(xface, bn, temperature<S, NC>(sP, ca), temperature<S, NC>(sP, cb), slope_a, slope_b,
+                          sP[bt_row * NC + ca], sP[bt_row * NC + cb], sP[7 * NC + ca], sP[7 * NC + cb], jz_0, jz_1,
+                          xface ? dx : dy, xface ? idx : idy, S(a.eta), S(a.kappa_par), S(a.kappa_perp), F);
     }
     // walls: nothing but the pressure crosses (carafe/mhd.py:874-886)
     bool wall;

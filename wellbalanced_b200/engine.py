@@ -207,9 +207,15 @@ class Engine:
         """Register += fine-mean minus coarse fluxes of every coarse-fine interface face."""
         if self.nface:
             b = self.mean_field
-            _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
-                      self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
-                      self.register.data_ptr(), self._s())
+            if self.ndim == 2 and self.physics is not None and any(self.physics[:3]):
+                eta, kappa_par, kappa_perp = self.physics[:3]
+                _lib.call("wb_face_flux_ops_physics", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], self.gamma, self.limiter, eta,
+                          kappa_par, kappa_perp, self.register.data_ptr(), self._s())
+            else:
+                _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
+                          self.register.data_ptr(), self._s())
             self.launches += 1
 
     def reflux(self, pool):

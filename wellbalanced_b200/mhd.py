@@ -127,11 +127,6 @@ class MHD2D:
         self._groups_potential = groups[1:]
         physics = (self.resistivity, self.conduction[0], self.conduction[1], self.gravity[0], self.gravity[1])
         if any(physics):
-            if self._fused and self.hierarchy.max_level > 0:
-                raise NotImplementedError(
-                    "resistivity, conduction and gravity run on one level: the flux register does not "
-                    "carry their face terms yet"
-                )
             self.engine.physics = tuple(float(v) for v in physics)
 
     # construction of common cases (carafe/mhd.py:486-671) -----------------------------------------

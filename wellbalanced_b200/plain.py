@@ -8,8 +8,8 @@ after the reference's transposes in 3D —, ``ct_contact`` — all planes of a 3
 one launch —, ``mhd_conductive``, ``mhd_resistive``), every intermediate (primitive
 variables, face fields, fluxes, edge fields) lives in HBM, and the flux-register update,
 gravity sources, potential update and Heun combine are device array operations. It is
-the float64 baseline the fused kernels are measured against, and it carries the terms
-the fused kernels leave out (resistivity, Braginskii conduction, gravity).
+the float64 baseline the fused kernels are measured against, and in 3D it carries the
+terms the fused 3D kernel leaves out (resistivity, gravity).
 """
 
 from __future__ import annotations
