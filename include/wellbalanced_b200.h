@@ -112,6 +112,16 @@ int wb_stage2d_physics(int precision, const void* src, const void* base, void* d
                        int limiter, double eta, double kappa_par, double kappa_perp, double gx, double gy,
                        unsigned long long* bad, void* stream);
 
+/* wb_stage3d with the reference's resistivity and gravity in the same pass
+ * (carafe/mhd3d.py:561-600, 639-671): E += eta J on every edge and eta (J x B) on every
+ * face's energy flux, J = curl B on the edges from the face fields and B the mean of the
+ * four faces around each face; rho g and m . g on the cells. All zero gives the ideal
+ * kernel. */
+int wb_stage3d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
+                       const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+                       double b0z, int limiter, int lx, double eta, double gx, double gy, double gz,
+                       unsigned long long* bad, void* stream);
+
 /* Tile shape of the stage kernels: 2D (TX, TY); 3D (TY, TZ). */
 int wb_tile_shape(int ndim, int precision, int* a, int* b);
 
@@ -144,13 +154,14 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
  * fine patches takes its corrections from separate calls (one per axis and side). */
 int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
                      double b0y, double b0z, double gamma, int limiter, double* reg, void* stream);
-/* The same register update for a 2D hierarchy with the non-ideal face terms of
- * wb_stage2d_physics: each recomputed face flux carries the resistive eta J terms and the
- * Braginskii heat flux, as the reference's fluxes do when its register records them
- * (carafe/mhd.py:866-872, 906-919). Every op must be a 2D interface. */
+/* The same register update with the non-ideal face terms of wb_stage2d_physics /
+ * wb_stage3d_physics: each recomputed face flux carries the resistive terms (and, in 2D,
+ * the Braginskii heat flux), as the reference's fluxes do when its register records them
+ * (carafe/mhd.py:866-872, 906-919; carafe/mhd3d.py:630-632). 3D interfaces take eta only
+ * (the reference's MHD3D has no conduction). */
 int wb_face_flux_ops_physics(int precision, const void* pool, const void* patches, const void* ops, int nops,
-                             double b0x, double b0y, double gamma, int limiter, double eta, double kappa_par,
-                             double kappa_perp, double* reg, void* stream);
+                             double b0x, double b0y, double b0z, double gamma, int limiter, double eta,
+                             double kappa_par, double kappa_perp, double* reg, void* stream);
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
                     const double* dt, void* stream);
 

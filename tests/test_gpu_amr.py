@@ -123,7 +123,7 @@ def test_refined_2d_float32_drift_is_at_float32_round_off():
     assert model.composite_divergence() < 1e-6
 
 
-def _alfven_pair(precision=64):
+def _alfven_pair(precision=64, **options):
     from oracle.mesh import Hierarchy
     from oracle.mhd3d import MHD3D as OracleMHD3D
     from wellbalanced_b200.mesh import AMRHierarchy
@@ -148,7 +148,8 @@ def _alfven_pair(precision=64):
     oh.add_patch(1, ((8, 20), (4, 12), (2, 10)))
     dh = AMRHierarchy((16, 8, 8), bounds, periodic=(True,) * 3)
     dh.add_patch(1, ((8, 20), (4, 12), (2, 10)))
-    models = (OracleMHD3D(oh, mean_field=tuple(n)), MHD3D(dh, mean_field=tuple(n), precision=precision))
+    models = (OracleMHD3D(oh, mean_field=tuple(n), **options),
+              MHD3D(dh, mean_field=tuple(n), precision=precision, **options))
     for m in models:
         m.set_state(1.0, lambda x, y, z: [-b for b in perpendicular(x, y, z)], 0.1,
                     vector_potential=(potential(0), potential(1), potential(2)))
@@ -169,6 +170,29 @@ def test_refined_3d_matches_the_oracle_and_conserves():
     after = device.totals()
     for name in before:
         assert abs(after[name] - before[name]) < 1e-14 * max(1.0, abs(before[name])) * 100
+    assert device.divergence() < 1e-14
+
+
+def test_refined_3d_with_resistivity_and_gravity_matches_the_oracle():
+    """The fused 3D kernel's resistive and gravity terms on a refined hierarchy: the flux
+    register carries eta (J x B) on the recomputed coarse and fine faces (the reference
+    records the energy fluxes after adding it, carafe/mhd3d.py:630-632, 651-657)."""
+    oracle, device = _alfven_pair(resistivity=0.01, gravity=(0.02, -0.05, 0.03))
+    for _ in range(6):
+        dt = oracle.step()
+        device.step(dt)
+    for op, dp in zip(oracle.hierarchy.patches, device.hierarchy.patches, strict=True):
+        names = [*oracle.names.values(), *oracle.potential]
+        for f, name in enumerate(names):
+            np.testing.assert_allclose(device.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                       err_msg=f"level {op.level} {name}")
+    _, device = _alfven_pair(resistivity=0.01)
+    before = device.totals()
+    for _ in range(6):
+        device.step()
+    after = device.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-12 * max(1.0, abs(before[name])), name
     assert device.divergence() < 1e-14
 
 

@@ -413,3 +413,48 @@ def test_plain_3d_resistivity_and_gravity_match_the_reference(runs3d):
     got = device.state()
     for key in want:
         np.testing.assert_allclose(got[key], want[key], rtol=1e-12, atol=1e-12, err_msg=key)
+
+
+def test_fused_3d_resistivity_and_gravity_match_the_reference(runs3d):
+    """The fused 3D stage kernel with resistivity (the reference's own resistive run) and
+    with resistivity, gravity and a mean field (against the oracle's 3D step), in float64
+    to 1e-12 and in float32 to float32 round-off."""
+    from oracle.mesh import Hierarchy
+    from oracle.mhd3d import MHD3D as OracleMHD3D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    k = 2.0 * np.pi
+    model = MHD3D(AMRHierarchy((4, 4, 16), ((0.0, 1.0),) * 3, periodic=(True,) * 3), resistivity=0.01,
+                  precision=64)
+    model.set_state(1.0, (0.0, 0.0, 0.0), 1.0,
+                    vector_potential=(lambda x, y, z: np.cos(k * z) / k, lambda x, y, z: np.sin(k * z) / k, 0.0))
+    for _ in range(5):
+        model.step()
+    close(model.state(), runs3d, "resistive3d", 1e-12)
+
+    def state(m):
+        m.set_state(lambda x, y, z: 1.0 + 0.3 * (z > 0.5), (0.0, 0.0, lambda x, y, z: 0.05 * np.sin(k * x)),
+                    lambda x, y, z: 2.0 - 0.2 * z,
+                    vector_potential=(lambda x, y, z: 0.03 * np.sin(k * y) / k,
+                                      lambda x, y, z: 0.05 * np.cos(k * x) / k, 0.0))
+        return m
+
+    options = dict(gravity=(0.05, 0.0, -0.2), resistivity=0.005, limiter="minmod", mean_field=(0.0, 0.05, 0.1))
+    shape = (20, 18, 24)  # several tiles along y and z, tiles of 16 planes along x
+    oracle = state(OracleMHD3D(Hierarchy(shape, ((0.0, 1.0),) * 3, (True,) * 3), **options))
+    fused64 = state(MHD3D(AMRHierarchy(shape, ((0.0, 1.0),) * 3, periodic=(True,) * 3), precision=64, lx=16,
+                          **options))
+    fused32 = state(MHD3D(AMRHierarchy(shape, ((0.0, 1.0),) * 3, periodic=(True,) * 3), precision=32, lx=16,
+                          **options))
+    for _ in range(4):
+        dt = oracle.step()
+        fused64.step(dt)
+        fused32.step(dt)
+    want = oracle.state()
+    got64, got32 = fused64.state(), fused32.state()
+    for key in want:
+        np.testing.assert_allclose(got64[key], want[key], rtol=1e-12, atol=1e-12, err_msg=key)
+        scale = float(np.max(np.abs(want[key])))
+        assert float(np.max(np.abs(got32[key] - want[key]))) < 2e-5 * max(scale, 1.0), key
+    assert fused64.divergence() < 1e-13

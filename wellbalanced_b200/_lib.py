@@ -36,6 +36,8 @@ SIGNATURES = {
                    c_int, c_int, c_dp, c_dp, c_dp],
     "wb_stage2d_physics": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_int,
                            c_double, c_double, c_double, c_double, c_double, c_dp, c_dp],
+    "wb_stage3d_physics": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double,
+                           c_double, c_int, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp],
     "wb_tile_shape": [c_int, c_int, c_dp, c_dp],
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],
@@ -52,8 +54,8 @@ SIGNATURES = {
     "wb_interp_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_face_flux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp, c_dp],
-    "wb_face_flux_ops_physics": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_int, c_double,
-                                 c_double, c_double, c_dp, c_dp],
+    "wb_face_flux_ops_physics": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int,
+                                 c_double, c_double, c_double, c_dp, c_dp],
     "wb_reflux_apply": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],
     "wb_struct_sizes": [c_dp, c_int],
 }

@@ -235,6 +235,32 @@ int wb_stage3d(int precision, const void* src, const void* base, void* dst, cons
   return launch_stage3d<double>(a, ntiles, limiter, as_stream(stream));
 }
 
+int wb_stage3d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
+                       const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z,
+                       int limiter, int lx, double eta, double gx, double gy, double gz, unsigned long long* bad,
+                       void* stream) {
+  set_error("");
+  if (!precision_ok(precision, "stage3d_physics") ||
+      !ptrs_ok({src, dst, patches, tiles, dt, bad}, "stage3d_physics"))
+    return kBadArgument;
+  if (ntiles < 0 || !(gamma > 1.0) || lx <= 0 || !(eta >= 0.0)) {
+    set_error("stage3d_physics: ntiles must be >= 0, gamma > 1, lx > 0 and eta >= 0");
+    return kBadArgument;
+  }
+  if (precision == 32) {
+    StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
+                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
+                       1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, nullptr, lx};
+    a.eta = eta, a.gravity[0] = gx, a.gravity[1] = gy, a.gravity[2] = gz;
+    return launch_stage3d<float>(a, ntiles, limiter, as_stream(stream));
+  }
+  StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
+                      static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
+                      1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, nullptr, lx};
+  a.eta = eta, a.gravity[0] = gx, a.gravity[1] = gy, a.gravity[2] = gz;
+  return launch_stage3d<double>(a, ntiles, limiter, as_stream(stream));
+}
+
 int wb_tile_shape(int ndim, int precision, int* a, int* b) {
   set_error("");
   if (!precision_ok(precision, "tile_shape") || !a || !b || (ndim != 2 && ndim != 3)) {
@@ -338,15 +364,15 @@ int wb_face_flux_ops(int precision, const void* pool, const void* patches, const
 }
 
 int wb_face_flux_ops_physics(int precision, const void* pool, const void* patches, const void* ops, int nops,
-                             double b0x, double b0y, double gamma, int limiter, double eta, double kappa_par,
-                             double kappa_perp, double* reg, void* stream) {
+                             double b0x, double b0y, double b0z, double gamma, int limiter, double eta,
+                             double kappa_par, double kappa_perp, double* reg, void* stream) {
   set_error("");
   if (!(eta >= 0.0) || !(kappa_par >= 0.0) || !(kappa_perp >= 0.0)) {
     set_error("face_flux_ops_physics: eta %g, kappa_par %g, kappa_perp %g must be non-negative", eta, kappa_par,
               kappa_perp);
     return kBadArgument;
   }
-  const double b0[3] = {b0x, b0y, 0.0};
+  const double b0[3] = {b0x, b0y, b0z};
   const double physics[3] = {eta, kappa_par, kappa_perp};
   return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, physics, reg, stream);
 }

@@ -105,8 +105,71 @@ __device__ S cell_temperature(const S* src, const PatchDesc& P, int i, int j, co
   return M::div(q[4], q[0], M::inv(q[0]));
 }
 
-// The non-ideal coefficients of the 2D face fluxes: resistivity and the parallel and
-// perpendicular conductivities.
+// The field at the lower `axis`-face of haloed 3D cell (i, j, k): the curl of the edge
+// potential plus the mean field, with the arithmetic of the 3D stage kernel.
+template <typename S>
+__device__ S face_field3(const S* src, const PatchDesc& P, int axis, int i, int j, int k, const double* b0) {
+  using M = Math<S>;
+  const int64_t fs = P.fstride, p0 = P.pitch0, p1 = P.pitch1;
+  const int64_t o = cell_offset(P, i, j, k);
+  const S* Ax = src + 5 * fs;
+  const S* Ay = src + 6 * fs;
+  const S* Az = src + 7 * fs;
+  const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
+  const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
+  if (axis == 0) return M::div(Az[o + p1] - Az[o], dy, idy) - M::div(Ay[o + 1] - Ay[o], dz, idz) + S(b0[0]);
+  if (axis == 1) return M::div(Ax[o + 1] - Ax[o], dz, idz) - M::div(Az[o + p0] - Az[o], dx, idx) + S(b0[1]);
+  return M::div(Ay[o + p0] - Ay[o], dx, idx) - M::div(Ax[o + p1] - Ax[o], dy, idy) + S(b0[2]);
+}
+
+// J_c = d_a B_b - d_b B_a ((c, a, b) cyclic) on the 3D c-edge whose lower corner is haloed
+// cell y (carafe/mhd3d.py:579-590).
+struct Cell3 {
+  int v[3];
+};
+
+// J_c = d_a B_b - d_b B_a ((c, a, b) cyclic) on the 3D c-edge whose lower corner is haloed
+// cell y (carafe/mhd3d.py:579-590).
+template <typename S>
+__device__ S edge_current3(const S* src, const PatchDesc& P, int c, Cell3 y, const double* b0) {
+  using M = Math<S>;
+  const int a = (c + 1) % 3, b = (c + 2) % 3;
+  Cell3 ya = y, yb = y;
+  --ya.v[a];
+  --yb.v[b];
+  const S da = S(P.dx[a]), db = S(P.dx[b]);
+  return M::div(face_field3<S>(src, P, b, y.v[0], y.v[1], y.v[2], b0) -
+                    face_field3<S>(src, P, b, ya.v[0], ya.v[1], ya.v[2], b0),
+                da, M::inv(da)) -
+         M::div(face_field3<S>(src, P, a, y.v[0], y.v[1], y.v[2], b0) -
+                    face_field3<S>(src, P, a, yb.v[0], yb.v[1], yb.v[2], b0),
+                db, M::inv(db));
+}
+
+// eta (J_b B_c - J_c B_b) on the lower s-face of haloed 3D cell x ((s, b, c) cyclic): J the
+// mean of the face's two b- and two c-edges, B the mean of the four faces around it
+// (carafe/mhd3d.py:590-600).
+template <typename S>
+__device__ S resistive_energy3(const S* src, const PatchDesc& P, int s, Cell3 x, const double* b0, S eta) {
+  const int b = (s + 1) % 3, c = (s + 2) % 3;
+  auto shifted = [&](int axis1, int d1, int axis2, int d2) {
+    Cell3 y = x;
+    y.v[axis1] += d1;
+    y.v[axis2] += d2;
+    return y;
+  };
+  auto field = [&](int axis, Cell3 y) { return face_field3<S>(src, P, axis, y.v[0], y.v[1], y.v[2], b0); };
+  const S jb = S(0.5) * (edge_current3<S>(src, P, b, x, b0) + edge_current3<S>(src, P, b, shifted(c, 1, c, 0), b0));
+  const S jc = S(0.5) * (edge_current3<S>(src, P, c, x, b0) + edge_current3<S>(src, P, c, shifted(b, 1, b, 0), b0));
+  const S bc = S(0.5) * (S(0.5) * (field(c, shifted(s, -1, s, 0)) + field(c, x)) +
+                         S(0.5) * (field(c, shifted(s, -1, c, 1)) + field(c, shifted(c, 1, c, 0))));
+  const S bb = S(0.5) * (S(0.5) * (field(b, shifted(s, -1, s, 0)) + field(b, x)) +
+                         S(0.5) * (field(b, shifted(s, -1, b, 1)) + field(b, shifted(b, 1, b, 0))));
+  return eta * (jb * bc - jc * bb);
+}
+
+// The non-ideal coefficients of the face fluxes: resistivity and the parallel and
+// perpendicular conductivities (2D only).
 struct FacePhysics {
   double eta, kappa_par, kappa_perp;
 };
@@ -189,6 +252,9 @@ __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, 
     nonideal_face_terms(xface, bn, t_a, t_b, slope[0], slope[1], qs[1][5], qs[2][5], qs[1][6], qs[2][6], jz_0, jz_1,
                         xface ? dx : dy, xface ? idx : idy, S(phys.eta), S(phys.kappa_par), S(phys.kappa_perp), F);
   }
+  if (PHYS && ndim == 3 && phys.eta != 0.0) {
+    F[4] += resistive_energy3<S>(src, P, axis, Cell3{{i, j, k}}, b0, S(phys.eta));
+  }
   for (int t = 0; t < ncons; ++t) out[t] = double(F[rows[t]]);
 }
 
@@ -265,7 +331,7 @@ void launch_face_flux_kernel(const S* pool, const PatchDesc* patches, const Face
   }
 }
 
-// physics: null for ideal MHD, else {eta, kappa_par, kappa_perp} (2D interfaces only)
+// physics: null for ideal MHD, else {eta, kappa_par, kappa_perp} (3D interfaces take eta only)
 template <typename S>
 int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
                          double gamma, int limiter, const double* physics, double* reg, cudaStream_t stream) {

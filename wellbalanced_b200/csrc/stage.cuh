@@ -25,10 +25,10 @@ struct StageArgs {
   unsigned long long* bad;      // count of non-positive / non-finite cells
   double* bflux;                // boundary-face fluxes of each patch (nullable)
   int lx;                       // 3D: cell planes per tile along x
-  // 2D non-ideal terms (zero: ideal MHD): resistivity, Braginskii conduction along and
-  // across the field, gravity
+  // non-ideal terms (zero: ideal MHD): resistivity, Braginskii conduction along and
+  // across the field (2D only), gravity
   double eta = 0.0, kappa_par = 0.0, kappa_perp = 0.0;
-  double gravity[2] = {0.0, 0.0};
+  double gravity[3] = {0.0, 0.0, 0.0};
 };
 
 template <typename S>

@@ -21,6 +21,11 @@
 //      stage 2 (carafe/mhd3d.py:635-671, 726-754).
 // Primitive variables, fluxes and edge fields stay on chip; each stage reads the state
 // once (plus halo overlap between tiles) and writes it once.
+// PHYS adds the reference's resistivity and gravity (carafe/mhd3d.py:561-600, 639-671):
+// the face fields are kept for three planes (p-1, p, p+1), so that B2 forms J = curl B
+// on the edges around its faces, adds eta (J x B) to the energy flux of its x-, y- and
+// z-faces and hands eta J of its column's three edges to C (E += eta J); C adds rho g and
+// m . g to the cells.
 #include "layout.cuh"
 #include "numerics.cuh"
 #include "stage.cuh"
@@ -51,17 +56,29 @@ struct Occupancy3D {
   static constexpr int kBlocks = sizeof(S) == 4 ? 2 : 1;
 };
 
-template <typename S, int LIM>
+// Planes of face fields kept in shared memory: two, or three with the resistive terms.
+template <bool PHYS>
+__host__ __device__ constexpr int face_slots() {
+  return PHYS ? 3 : 2;
+}
+
+template <bool PHYS>
+__device__ __forceinline__ int face_slot(int plane) {
+  return PHYS ? (plane + 6) % 3 : (plane + 4) & 1;  // plane >= -3
+}
+
+template <typename S, int LIM, bool PHYS>
 __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
   constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int RZ = TZ + 4, NR = (TY + 4) * (TZ + 4);  // plane region j, k in [-2, T+2)
   constexpr int GZ = TZ + 1, G = (TY + 1) * (TZ + 1);    // face / column grids
   constexpr int NCORE = TY * TZ;
+  constexpr int NB = face_slots<PHYS>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   S* sP = reinterpret_cast<S*>(smem_raw);  // [2 slots][8][NR] primitive variables
-  S* sBn = sP + 2 * 8 * NR;                 // [2 slots][3][NR] field at each cell's lower faces
-  S* sEc = sBn + 2 * 3 * NR;                // [4 slots][3][G] cell E_x, E_y, E_z
+  S* sBn = sP + 2 * 8 * NR;                 // [NB slots][3][NR] field at each cell's lower faces
+  S* sEc = sBn + NB * 3 * NR;               // [4 slots][3][G] cell E_x, E_y, E_z
   S* sYZ = sEc + 4 * 3 * G;                 // [3 slots][2 dirs][7][G] y- and z-face fluxes
   S* sX = sYZ + 3 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
 
@@ -113,6 +130,25 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   for (int c = 0; c < 7; ++c) slope[c] = S(0);
   S fprev[5] = {S(0), S(0), S(0), S(0), S(0)};
   S fnow[5] = {S(0), S(0), S(0), S(0), S(0)};
+  S ejx = S(0), ejy = S(0), ejz = S(0);  // eta J on the column's edges (PHYS)
+  // PHYS: the field at the lower `axis`-face of cell (plane, j, k) of the tile, and the
+  // current J_c = d_a B_b - d_b B_a ((c, a, b) cyclic) on the c-edge whose lower corner
+  // is that cell (carafe/mhd3d.py:579-590); planes p-1 .. p+1 are held during B2
+  auto face = [&](int plane, int axis, int j, int k) -> S {
+    return sBn[(face_slot<PHYS>(plane) * 3 + axis) * NR + (j + 2) * RZ + (k + 2)];
+  };
+  auto jx_at = [&](int plane, int j, int k) -> S {
+    return M::div(face(plane, 2, j, k) - face(plane, 2, j - 1, k), dy, idy) -
+           M::div(face(plane, 1, j, k) - face(plane, 1, j, k - 1), dz, idz);
+  };
+  auto jy_at = [&](int plane, int j, int k) -> S {
+    return M::div(face(plane, 0, j, k) - face(plane, 0, j, k - 1), dz, idz) -
+           M::div(face(plane, 2, j, k) - face(plane - 1, 2, j, k), dx, idx);
+  };
+  auto jz_at = [&](int plane, int j, int k) -> S {
+    return M::div(face(plane, 1, j, k) - face(plane - 1, 1, j, k), dx, idx) -
+           M::div(face(plane, 0, j, k) - face(plane, 0, j - 1, k), dy, idy);
+  };
   const S dt = S(a.dt[P.instance]);
   const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
   S* __restrict__ dst = a.dst + P.off;
@@ -136,7 +172,7 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       const int slot = (c + 4) & 1;
       const int slot4 = (c + 8) & 3;
       S* P8 = sP + slot * 8 * NR;
-      S* B3 = sBn + slot * 3 * NR;
+      S* B3 = sBn + (PHYS ? face_slot<PHYS>(c) : slot) * 3 * NR;
       S* E3 = sEc + slot4 * 3 * G;
       const int I = c + kHalo;
       for (int r = tid; r < NR; r += blockDim.x) {
@@ -197,7 +233,7 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
     {
       const int slot = (p + 4) & 1, slot3 = (p + 6) % 3;
       const S* Pp = sP + slot * 8 * NR;
-      const S* Bp = sBn + slot * 3 * NR;
+      const S* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : slot) * 3 * NR;
       const bool need_yz = p >= x0 - 1 && (p < xe || xn > xe);
       if (need_yz) {
         S* Y7 = sYZ + (slot3 * 2 + 0) * 7 * G;
@@ -261,11 +297,23 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       S now[7];
 #pragma unroll
       for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q[1][cc] - q[0][cc], q[2][cc] - q[1][cc]);
-      const S* Bp = sBn + ((p + 4) & 1) * 3 * NR;
+      const S* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : ((p + 4) & 1)) * 3 * NR;
       if (p >= x0) {
         S L[7], Rt[7], F[7];
         reconstruct_sloped(q[0], q[1], slope, now, L, Rt);
         hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
+        if (PHYS && a.eta != 0.0 && tid < NCORE) {
+          // eta (J_y B_z - J_z B_y) on the x-face: J of its two y- and two z-edges, B of
+          // the four y- and z-faces around it (carafe/mhd3d.py:590-600)
+          const S eta = S(a.eta);
+          const S jb = S(0.5) * (jy_at(p, cj, ck) + jy_at(p, cj, ck + 1));
+          const S jc = S(0.5) * (jz_at(p, cj, ck) + jz_at(p, cj + 1, ck));
+          const S bc = S(0.5) * (S(0.5) * (face(p - 1, 2, cj, ck) + face(p, 2, cj, ck)) +
+                                 S(0.5) * (face(p - 1, 2, cj, ck + 1) + face(p, 2, cj, ck + 1)));
+          const S bb = S(0.5) * (S(0.5) * (face(p - 1, 1, cj, ck) + face(p, 1, cj, ck)) +
+                                 S(0.5) * (face(p - 1, 1, cj + 1, ck) + face(p, 1, cj + 1, ck)));
+          F[4] += eta * (jb * bc - jc * bb);
+        }
         // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
         sX[col_g] = F[0];
         sX[G + col_g] = F[5];
@@ -275,6 +323,39 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       }
 #pragma unroll
       for (int cc = 0; cc < 7; ++cc) slope[cc] = now[cc];
+      if (PHYS && a.eta != 0.0 && p >= x0) {
+        const S eta = S(a.eta);
+        if (p < xe) {
+          // eta (J_z B_x - J_x B_z) on the y-face (cell p, node yj, cell yk) and
+          // eta (J_x B_y - J_y B_x) on the z-face (cell p, cell zj, node zk), added to the
+          // energy fluxes this thread formed in B1 (read by C one plane later)
+          const int sl3 = (p + 6) % 3;
+          if (yk >= 0) {
+            const S jb = S(0.5) * (jz_at(p, yj, yk) + jz_at(p + 1, yj, yk));
+            const S jc = S(0.5) * (jx_at(p, yj, yk) + jx_at(p, yj, yk + 1));
+            const S bc = S(0.5) * (S(0.5) * (face(p, 0, yj - 1, yk) + face(p, 0, yj, yk)) +
+                                   S(0.5) * (face(p + 1, 0, yj - 1, yk) + face(p + 1, 0, yj, yk)));
+            const S bb = S(0.5) * (S(0.5) * (face(p, 2, yj - 1, yk) + face(p, 2, yj, yk)) +
+                                   S(0.5) * (face(p, 2, yj - 1, yk + 1) + face(p, 2, yj, yk + 1)));
+            sYZ[(sl3 * 2 + 0) * 7 * G + 4 * G + y_g] += eta * (jb * bc - jc * bb);
+          }
+          if (zj >= 0) {
+            const S jb = S(0.5) * (jx_at(p, zj, zk) + jx_at(p, zj + 1, zk));
+            const S jc = S(0.5) * (jy_at(p, zj, zk) + jy_at(p + 1, zj, zk));
+            const S bc = S(0.5) * (S(0.5) * (face(p, 1, zj, zk - 1) + face(p, 1, zj, zk)) +
+                                   S(0.5) * (face(p, 1, zj + 1, zk - 1) + face(p, 1, zj + 1, zk)));
+            const S bb = S(0.5) * (S(0.5) * (face(p, 0, zj, zk - 1) + face(p, 0, zj, zk)) +
+                                   S(0.5) * (face(p + 1, 0, zj, zk - 1) + face(p + 1, 0, zj, zk)));
+            sYZ[(sl3 * 2 + 1) * 7 * G + 4 * G + z_g] += eta * (jb * bc - jc * bb);
+          }
+        }
+        if (tid < NCORE) {
+          // eta J on the column's x-edge (cell plane p) and y- and z-edges (node plane p)
+          ejx = eta * jx_at(p, cj, ck);
+          ejy = eta * jy_at(p, cj, ck);
+          ejz = eta * jz_at(p, cj, ck);
+        }
+      }
     }
     __syncthreads();
 
@@ -304,15 +385,22 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
                         M::div(Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)], dy, idy) +
                         M::div(Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)], dz, idz);
           S value = src[qf * fs + o] - dt * div;
+          if (PHYS) {
+            // gravity: rho g on the momentum, m . g on the energy, from the stage's input
+            const S g0 = S(a.gravity[0]), g1 = S(a.gravity[1]), g2 = S(a.gravity[2]);
+            if (qf >= 1 && qf <= 3) value += dt * (S(a.gravity[qf - 1]) * src[o]);
+            if (qf == 4) value += dt * (src[fs + o] * g0 + src[2 * fs + o] * g1 + src[3 * fs + o] * g2);
+          }
           if (base_state) value = (value + base_state[qf * fs + o]) * S(0.5);
           dst[qf * fs + o] = value;
         }
       }
       // E_x on the x-edges of cell plane p: (a, b) = (y, z)
       if (p < xe && gj < own_ny && gk < own_nz) {
-        const S ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
+        S ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
                              Zc[6 * G + zi(j - 1, k)], Zc[6 * G + zi(j, k)], Zc[zi(j - 1, k)], Zc[zi(j, k)],
                              Ec[gi(j - 1, k - 1)], Ec[gi(j, k - 1)], Ec[gi(j - 1, k)], Ec[gi(j, k)]);
+        if (PHYS) ex += ejx;
         const int64_t o = 5 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
         S value = src[o] - dt * ex;
         if (base_state) value = (value + base_state[o]) * S(0.5);
@@ -321,9 +409,10 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
       if (p < xn) {
         // E_y on the y-edges of node plane p: (a, b) = (z, x)
         if (gj < ny && gk < own_nz) {
-          const S ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
+          S ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
                                sX[2 * G + gi(j, k - 1)], sX[2 * G + gi(j, k)], sX[gi(j, k - 1)], sX[gi(j, k)],
                                Ep[G + gi(j, k - 1)], Ep[G + gi(j, k)], Ec[G + gi(j, k - 1)], Ec[G + gi(j, k)]);
+          if (PHYS) ey += ejy;
           const int64_t o = 6 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
           S value = src[o] - dt * ey;
           if (base_state) value = (value + base_state[o]) * S(0.5);
@@ -331,10 +420,11 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
         }
         // E_z on the z-edges of node plane p: (a, b) = (x, y)
         if (gj < own_ny && gk < nz) {
-          const S ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
+          S ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
                                Yp[6 * G + yi(j, k)], Yc[6 * G + yi(j, k)], Yp[yi(j, k)], Yc[yi(j, k)],
                                Ep[2 * G + gi(j - 1, k)], Ec[2 * G + gi(j - 1, k)], Ep[2 * G + gi(j, k)],
                                Ec[2 * G + gi(j, k)]);
+          if (PHYS) ez += ejz;
           const int64_t o = 7 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
           S value = src[o] - dt * ez;
           if (base_state) value = (value + base_state[o]) * S(0.5);
@@ -356,17 +446,24 @@ template <typename S>
 int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
   constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int NR = (TY + 4) * (TZ + 4), G = (TY + 1) * (TZ + 1);
-  const size_t smem = sizeof(S) * (2 * 8 * NR + 2 * 3 * NR + 4 * 3 * G + 3 * 2 * 7 * G + 3 * G);
   if (ntiles <= 0) return kOk;
   if (args.lx <= 0) {
     set_error("stage3d: lx must be positive");
     return kBadArgument;
   }
+  const bool phys = args.eta != 0.0 || args.gravity[0] != 0.0 || args.gravity[1] != 0.0 || args.gravity[2] != 0.0;
+  const size_t smem =
+      sizeof(S) * (2 * 8 * NR + (phys ? 3 : 2) * 3 * NR + 4 * 3 * G + 3 * 2 * 7 * G + 3 * G);
   switch (limiter) {
-#define WB_CASE(L)                                                                                   \
-  case L:                                                                                            \
-    cudaFuncSetAttribute(stage3d_kernel<S, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-    stage3d_kernel<S, L><<<ntiles, 288, smem, stream>>>(args);                                       \
+#define WB_CASE(L)                                                                                              \
+  case L:                                                                                                       \
+    if (phys) {                                                                                                 \
+      cudaFuncSetAttribute(stage3d_kernel<S, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+      stage3d_kernel<S, L, true><<<ntiles, 288, smem, stream>>>(args);                                        \
+    } else {                                                                                                    \
+      cudaFuncSetAttribute(stage3d_kernel<S, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
+      stage3d_kernel<S, L, false><<<ntiles, 288, smem, stream>>>(args);                                       \
+    }                                                                                                           \
     break;
     WB_CASE(0)
     WB_CASE(1)

@@ -110,7 +110,8 @@ class Engine:
         self.launches = 0
         #: optional list collecting (start, end) CUDA events around each stage kernel
         self.stage_events = None
-        #: 2D non-ideal terms (eta, kappa_par, kappa_perp, gx, gy), None for ideal MHD
+        #: non-ideal terms, None for ideal MHD: 2D (eta, kappa_par, kappa_perp, gx, gy),
+        #: 3D (eta, gx, gy, gz)
         self.physics = None
 
     # low-level launches ----------------------------------------------------------------------
@@ -170,6 +171,11 @@ class Engine:
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
                       self.gamma, b[0], b[1], self.limiter, self.bad.data_ptr(),
                       None if bflux is None else bflux.data_ptr(), s)
+        elif self.physics is not None:
+            _lib.call("wb_stage3d_physics", self.precision, src.data_ptr(),
+                      None if base is None else base.data_ptr(), dst.data_ptr(), self.patches.data_ptr(),
+                      self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(), self.gamma, b[0], b[1], b[2],
+                      self.limiter, self.layout.lx, *self.physics, self.bad.data_ptr(), s)
         else:
             _lib.call("wb_stage3d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
@@ -207,10 +213,11 @@ class Engine:
         """Register += fine-mean minus coarse fluxes of every coarse-fine interface face."""
         if self.nface:
             b = self.mean_field
-            if self.ndim == 2 and self.physics is not None and any(self.physics[:3]):
-                eta, kappa_par, kappa_perp = self.physics[:3]
+            if self.physics is not None:
+                eta, kappa_par, kappa_perp = self.physics[:3] if self.ndim == 2 else (self.physics[0], 0.0, 0.0)
+            if self.physics is not None and (eta or kappa_par or kappa_perp):
                 _lib.call("wb_face_flux_ops_physics", self.precision, pool.data_ptr(), self.patches.data_ptr(),
-                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], self.gamma, self.limiter, eta,
+                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter, eta,
                           kappa_par, kappa_perp, self.register.data_ptr(), self._s())
             else:
                 _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),

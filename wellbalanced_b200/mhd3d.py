@@ -62,8 +62,6 @@ class MHD3D:
             raise ValueError("resistivity must be non-negative")
         if len(mean_field) != 3 or len(gravity) != 3:
             raise ValueError("mean_field and gravity have three components")
-        if self._fused and (resistivity or any(gravity)):
-            raise NotImplementedError("the fused 3D device step covers ideal MHD (no resistivity or gravity)")
         self.hierarchy = hierarchy
         self.gamma = float(gamma)
         self.mean_field = tuple(float(b) for b in mean_field)
@@ -103,6 +101,9 @@ class MHD3D:
         groups = self.engine.layout.groups
         self._groups_all = groups
         self._groups_potential = groups[1:]
+        physics = (self.resistivity, *self.gravity)
+        if any(physics):
+            self.engine.physics = tuple(float(v) for v in physics)
 
     # test problems (carafe/mhd3d.py:236-346) -----------------------------------------------------
     @classmethod
