@@ -12,9 +12,18 @@ import itertools
 import numpy as np
 
 
+PROXY = 1 << 30  # a dense block standing for a box of another rank's patch
+
+
 def offset_of(row, i, j, k):
-    """Element offset of haloed index (i, j, k); asserts it lies inside the padded field."""
+    """Element offset of haloed index (i, j, k); asserts it lies inside the padded field
+    (for a proxy block, whose pitches are its box's, only the patch's haloed extents)."""
     n = [int(v) + 5 for v in row["n"]]
+    if int(row["flags"]) & PROXY:
+        assert 0 <= i < n[0] and 0 <= j < n[1] and (not row["pitch1"] or 0 <= k < n[2]), (i, j, k, n)
+        if row["pitch1"]:
+            return int(i) * int(row["pitch0"]) + int(j) * int(row["pitch1"]) + int(k)
+        return int(i) * int(row["pitch0"]) + int(j)
     if row["pitch1"]:
         assert 0 <= i < n[0] and 0 <= j < n[1] and 0 <= k < n[2], (i, j, k, n)
         assert int(k) < int(row["pitch1"])

@@ -87,6 +87,43 @@ def test_refined_2d_with_resistivity_conduction_and_gravity_matches_the_oracle()
     assert model.divergence() < 1e-14
 
 
+def _oracle_leaf_values(oracle):
+    """The reference's leaf_values (carafe/mhd.py:1059-1111) restated on the oracle, with
+    the device's cell order (patch by patch, row-major)."""
+    from wellbalanced_b200.mhd import covered_cells
+
+    h = oracle.hierarchy
+    oracle.fill_halos()
+    parts = {}
+    for patch in h.patches:
+        nx, ny = patch.shape
+        prim, bxf, byf, _, _ = oracle.primitive(patch)
+        jz = oracle.current(bxf, byf, patch.level)
+        corner = 0.25 * sum(jz[1 + a : 1 + a + nx, 1 + b : 1 + b + ny] for a in (0, 1) for b in (0, 1))
+        values = np.stack([*(q[2 : 2 + nx, 2 : 2 + ny] for q in prim), corner])
+        leaf = ~covered_cells(h, patch)
+        for i, value in enumerate(values):
+            parts.setdefault(i, []).append(value[leaf])
+    return [np.concatenate(parts[i]) for i in range(9)]
+
+
+def test_leaf_values_and_sheet_diagnostics_match_the_oracle():
+    from wellbalanced_b200.mhd import MHD2D, sheet_diagnostics
+
+    oracle, device = _pair()
+    for _ in range(5):
+        device.step(oracle.step())
+    leaf = device.leaf_values()
+    want = _oracle_leaf_values(oracle)
+    for name, expected in zip(MHD2D.LEAF_VARIABLES, want, strict=True):
+        np.testing.assert_allclose(leaf[name], expected, rtol=1e-11, atol=1e-12, err_msg=name)
+    assert leaf["level"].max() == 1 and leaf["x"].size == leaf["density"].size
+    mine = sheet_diagnostics(device, leaf)
+    theirs = sheet_diagnostics(device, {**leaf, **dict(zip(MHD2D.LEAF_VARIABLES, want, strict=True))})
+    assert mine["o_points"] == theirs["o_points"] and mine["x_points"] == theirs["x_points"]
+    assert abs(mine["psi"] - theirs["psi"]) < 1e-12 and abs(mine["max_current"] - theirs["max_current"]) < 1e-10
+
+
 def test_refined_2d_conserves_and_keeps_div_b_zero():
     from wellbalanced_b200.mesh import AMRHierarchy
     from wellbalanced_b200.mhd import MHD2D

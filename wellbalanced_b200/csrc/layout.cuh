@@ -26,6 +26,9 @@ constexpr int kWallHi2 = 1 << 5;
 constexpr int kOwnLast0 = 1 << 8;  // the patch computes its last node plane along axis 0
 constexpr int kOwnLast1 = 1 << 9;
 constexpr int kOwnLast2 = 1 << 10;
+// a dense block standing for a box of another rank's patch (mailboxes, proxies): the
+// copy, interpolation, restriction and face-flux kernels address it like the patch
+constexpr int kProxy = 1 << 30;
 
 struct PatchDesc {
   int64_t off;       // element offset of field 0 in the pool

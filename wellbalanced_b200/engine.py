@@ -122,35 +122,39 @@ class Engine:
 
     def fill(self, pool, levels=None):
         """Halos of every patch of `pool`, level by level (coarse first)."""
-        L = self.layout
+        for level in range(len(self.copy_phases)):
+            if levels is None or level in levels:
+                self._fill_level(pool, level)
+
+    def _fill_level(self, pool, level):
+        """Interpolation from the level below, same-level copies, boundary faces."""
         prec = self.precision
         s = self._s()
-        for level, (same, nsame, boundary) in enumerate(self.copy_phases):
-            if levels is not None and level not in levels:
-                continue
-            interp, ninterp = self.interp_levels[level]
-            if ninterp:
-                _lib.call("wb_interp_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp, s)
+        same, nsame, boundary = self.copy_phases[level]
+        interp, ninterp = self.interp_levels[level]
+        if ninterp:
+            _lib.call("wb_interp_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp, s)
+            self.launches += 1
+        if nsame:
+            _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), same.data_ptr(), nsame, s)
+            self.launches += 1
+        for ops, nops in boundary:
+            if nops:
+                _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), ops.data_ptr(), nops, s)
                 self.launches += 1
-            if nsame:
-                _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), same.data_ptr(), nsame, s)
-                self.launches += 1
-            for ops, nops in boundary:
-                if nops:
-                    _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), ops.data_ptr(), nops, s)
-                    self.launches += 1
-        del L
 
     def restrict(self, pool, groups):
         """Coarse values under finer patches from the fine ones (finest level first)."""
-        s = self._s()
         for level in range(self.layout.max_level, 0, -1):
             for g in groups:
-                ops, nops = self.restrict_levels[level][g]
-                if nops:
-                    _lib.call("wb_restrict_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
-                              ops.data_ptr(), nops, s)
-                    self.launches += 1
+                self._restrict_level(pool, level, g)
+
+    def _restrict_level(self, pool, level, g):
+        ops, nops = self.restrict_levels[level][g]
+        if nops:
+            _lib.call("wb_restrict_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(), ops.data_ptr(),
+                      nops, self._s())
+            self.launches += 1
 
     def stage(self, src, base, dst, bflux=None):
         b = self.mean_field

@@ -476,18 +476,7 @@ class MHD2D:
         return worst / scale if scale else 0.0
 
     def _covered(self, patch):
-        mask = np.zeros(patch.shape, dtype=bool)
-        for fine in self.hierarchy.patches_at_level(patch.level + 1):
-            idx = []
-            for a in range(2):
-                (flo, fhi), (lo, hi) = fine.box[a], patch.box[a]
-                s, e = max(flo // 2, lo), min(fhi // 2, hi)
-                if s >= e:
-                    break
-                idx.append(slice(s - lo, e - lo))
-            else:
-                mask[tuple(idx)] = True
-        return mask
+        return covered_cells(self.hierarchy, patch)
 
     def totals(self) -> dict[str, float]:
         """Integrals of the conserved fields over the domain from the leaf cells (float64)."""
@@ -516,6 +505,58 @@ class MHD2D:
                 out[name][i0:i1, j0:j1] = self.gather(patch, f)
             out["az"][i0 : i1 + 1, j0 : j1 + 1] = self.gather(patch, 6, node=True)
         return out
+
+    #: the variables of `leaf_values` besides the coordinates and the level
+    LEAF_VARIABLES = ("density", "velocity_x", "velocity_y", "velocity_z", "pressure", "magnetic_field_x",
+                      "magnetic_field_y", "magnetic_field_z", "current_z")
+
+    def _leaf_block(self, patch) -> torch.Tensor:
+        """(9, nx, ny) float64 on the device: the primitive variables of the patch's cells
+        (mhd_primitive_pyccel.py:23-87) and J_z at the cell as the mean of its four corner
+        nodes (carafe/mhd.py:1089-1096), from the haloed state."""
+        state = self.engine.state
+        nx, ny = patch.shape
+        dx, dy = self.hierarchy.spacing(patch.level)
+        view = [self.engine.view(state, patch, f).to(torch.float64) for f in range(7)]
+        az = view[6]                                      # haloed nodes (nx + 5, ny + 5)
+        bxf = (az[:, 1:] - az[:, :-1]) / dy + self.mean_field[0]   # [I, J]: node I of cell J
+        byf = -(az[1:, :] - az[:-1, :]) / dx + self.mean_field[1]  # [I, J]: cell I, node J
+        cells = (slice(HALO, HALO + nx), slice(HALO, HALO + ny))
+        rho, mx, my, mz, energy, bz = (v[cells] for v in view[:6])
+        bx = 0.5 * (bxf[HALO : HALO + nx, HALO : HALO + ny] + bxf[HALO + 1 : HALO + nx + 1, HALO : HALO + ny])
+        by = 0.5 * (byf[HALO : HALO + nx, HALO : HALO + ny] + byf[HALO : HALO + nx, HALO + 1 : HALO + ny + 1])
+        u, v, w = mx / rho, my / rho, mz / rho
+        p = (self.gamma - 1.0) * (energy - 0.5 * rho * (u * u + v * v + w * w) - 0.5 * (bx * bx + by * by + bz * bz))
+        # J_z at haloed nodes I, J in [1, n + 4): dB_y/dx - dB_x/dy
+        jz = (byf[1:, 1:-1] - byf[:-1, 1:-1]) / dx - (bxf[1:-1, 1:] - bxf[1:-1, :-1]) / dy
+        corner = torch.zeros_like(rho)
+        for a in (0, 1):
+            for b in (0, 1):
+                corner = corner + jz[HALO - 1 + a : HALO - 1 + a + nx, HALO - 1 + b : HALO - 1 + b + ny]
+        return torch.stack([rho, u, v, w, p, bx, by, bz, 0.25 * corner])
+
+    def leaf_values(self) -> dict[str, np.ndarray]:
+        """The primitive variables on the leaf cells of the hierarchy (carafe/mhd.py:1059-1111).
+
+        One value per leaf cell (a cell no finer patch covers): ``x``, ``y`` (the centres),
+        ``level``, the variables of `dataset` and ``current_z`` (the mean of the corners).
+        The cells come patch by patch in the hierarchy's order, each patch's in row-major
+        (x, y) order.
+        """
+        self._check_ready()
+        h = self.hierarchy
+        self.engine.fill(self.engine.state)
+        parts: dict[str, list[np.ndarray]] = {name: [] for name in ("x", "y", "level", *self.LEAF_VARIABLES)}
+        for patch in h.patches:
+            leaf = ~self._covered(patch)
+            block = self._leaf_block(patch)[:, torch.from_numpy(leaf).to(self.engine.device)].cpu().numpy()
+            x, y = self._coordinates(patch, node=False)
+            parts["x"].append(x[leaf])
+            parts["y"].append(y[leaf])
+            parts["level"].append(np.full(int(leaf.sum()), patch.level))
+            for name, values in zip(self.LEAF_VARIABLES, block, strict=True):
+                parts[name].append(values)
+        return {name: np.concatenate(values) for name, values in parts.items()}
 
     def dataset(self, level: int = 0) -> Dataset:
         """The primitive variables of ``level`` over its cell centres (``mhd.py:1177-1226``)."""
@@ -553,6 +594,79 @@ class MHD2D:
         }
         coords = {"x": Variable("x", x, r"$x$"), "y": Variable("y", y, r"$y$")}
         return Dataset(data, coords=coords, attrs={"time": self.time, "level": level, "gamma": self.gamma})
+
+
+def covered_cells(hierarchy, patch) -> np.ndarray:
+    """The cells of a 2D patch that a patch of the next level covers (bool, patch shape)."""
+    mask = np.zeros(patch.shape, dtype=bool)
+    for fine in hierarchy.patches_at_level(patch.level + 1):
+        idx = []
+        for a in range(2):
+            (flo, fhi), (lo, hi) = fine.box[a], patch.box[a]
+            s, e = max(flo // 2, lo), min(fhi // 2, hi)
+            if s >= e:
+                break
+            idx.append(slice(s - lo, e - lo))
+        else:
+            mask[tuple(idx)] = True
+    return mask
+
+
+def _locate(hierarchy, leaf, points):
+    """The index in `leaf` of the leaf cell holding each point ((2, n) array): the finest
+    level whose leaf cells contain it."""
+    lower = np.asarray(hierarchy.lower_bound, dtype=float)
+    owner = {}
+    for level in range(hierarchy.max_level + 1):
+        spacing = np.asarray(hierarchy.spacing(level))
+        mine = leaf["level"] == level
+        table = np.full(hierarchy.level_shape(level), -1, dtype=np.int64)
+        i = np.floor((leaf["x"][mine] - lower[0]) / spacing[0]).astype(np.int64)
+        j = np.floor((leaf["y"][mine] - lower[1]) / spacing[1]).astype(np.int64)
+        table[i, j] = np.flatnonzero(mine)
+        owner[level] = (table, spacing)
+    found = np.full(points.shape[1], -1, dtype=np.int64)
+    for level in range(hierarchy.max_level, -1, -1):
+        table, spacing = owner[level]
+        i = np.floor((points[0] - lower[0]) / spacing[0]).astype(np.int64)
+        j = np.floor((points[1] - lower[1]) / spacing[1]).astype(np.int64)
+        i = np.clip(i, 0, table.shape[0] - 1)
+        j = np.clip(j, 0, table.shape[1] - 1)
+        hit = table[i, j]
+        found = np.where(found < 0, hit, found)
+    if np.any(found < 0):
+        raise ValueError("a point lies outside the leaf cells")
+    return found
+
+
+def sheet_diagnostics(model, leaf=None) -> dict:
+    """The reconnected flux and the plasmoids of the lower sheet of `harris_sheets`
+    (carafe/mhd.py:1291-1329).
+
+    Along the line ``y = Ly / 4``: ``psi = (1/2) int |B_y| dx`` at the finest spacing,
+    the O-points (B_y turning from positive to negative along x) and X-points, and the
+    largest ``|J_z|``. ``leaf``: the `MHD2D.leaf_values` already computed.
+    """
+    mesh = model.hierarchy
+    leaf = model.leaf_values() if leaf is None else leaf
+    (x0, x1), (y0, y1) = mesh.bounds
+    line = y0 + 0.25 * (y1 - y0)
+    finest = mesh.spacing(mesh.max_level)[0]
+    x = x0 + (np.arange(round((x1 - x0) / finest)) + 0.5) * finest
+    below = _locate(mesh, leaf, np.array([x, np.full_like(x, line - 1e-9)]))
+    above = _locate(mesh, leaf, np.array([x, np.full_like(x, line + 1e-9)]))
+    by = 0.5 * (leaf["magnetic_field_y"][below] + leaf["magnetic_field_y"][above])
+    psi = 0.5 * float(np.sum(np.abs(by)) * finest)
+    sign = np.sign(by)
+    turns = sign * np.roll(sign, -1) < 0
+    return {
+        "time": model.time,
+        "psi": psi,
+        "o_points": int(np.sum(turns & (sign > 0))),
+        "x_points": int(np.sum(turns & (sign < 0))),
+        "max_current": float(np.max(np.abs(leaf["current_z"]))),
+        "leaf_cells": int(leaf["density"].size),
+    }
 
 
 def harris_sheets(hierarchy, *, width, beta=0.2, perturbation=1e-3, noise=0.0, seed=0):
