@@ -141,7 +141,7 @@ def describe(timings):
 
 
 class Turbulence:
-    kernel = "wb::stage3d_kernel<float, 2>"
+    kernel = "wb::stage3d_kernel<float, 2, false>"
     bytes_per_zone_update = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
 
     def __init__(self, args, rank):
@@ -199,16 +199,24 @@ class Turbulence:
         return out
 
 
+def _kernel2d(engine):
+    tx, ty = engine.layout.tile_shape
+    return f"wb::stage2d_kernel<float, 2, false, {tx}, {ty}>"
+
+
 class BatchWorkload:
-    kernel = "wb::stage2d_kernel<float, 2>"
     bytes_per_zone_update = 5 * 7 * 4  # 5 state passes x 7 values (6 cell + 1 node) x float32
+
+    @property
+    def kernel(self):
+        return _kernel2d(self.engine)
 
     def __init__(self, args, rank):
         from wellbalanced_b200.batch import Batch
 
         self.count = args.count
         self.rank = rank
-        self.batch = Batch.orszag_tang(self.count, seed=rank, precision=32)
+        self.batch = Batch.orszag_tang(self.count, seed=rank, precision=32, tile="auto")
         self.engine = self.batch.engine
         self.cells = self.batch.cells
 
@@ -234,6 +242,7 @@ class BatchWorkload:
             "instances": self.count,
             "mean_side": float(sum(sides) / len(sides)),
             "tile": {"x": self.engine.layout.tile_shape[0], "y": self.engine.layout.tile_shape[1]},
+            "autotune_tile_ms_per_launch": self.batch.tile_timings,
         }
 
     def plain(self, count=8, steps=2):
@@ -289,14 +298,17 @@ class BatchWorkload:
 
 
 class Harris:
-    kernel = "wb::stage2d_kernel<float, 2>"
     bytes_per_zone_update = 5 * 7 * 4
+
+    @property
+    def kernel(self):
+        return _kernel2d(self.engine)
 
     def __init__(self, args, rank):
         from wellbalanced_b200.mhd import MHD2D
 
         self.rank = rank
-        self.model = _harris_model(MHD2D, 32, rank)
+        self.model = _harris_model(MHD2D, 32, rank, tile="auto")
         self.engine = self.model.engine
         self.cells = int(sum(p.shape[0] * p.shape[1] for p in self.model.hierarchy.patches))
 
@@ -323,6 +335,7 @@ class Harris:
             "patches_per_level": {str(lv): len(h.patches_at_level(lv)) for lv in range(h.max_level + 1)},
             "refined_patch_sides": [min(min(s) for s in refined), max(max(s) for s in refined)] if refined else None,
             "tile": {"x": self.engine.layout.tile_shape[0], "y": self.engine.layout.tile_shape[1]},
+            "autotune_tile_ms_per_launch": self.model.tile_timings,
         }
 
     def plain(self, steps=2):

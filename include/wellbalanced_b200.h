@@ -122,8 +122,19 @@ int wb_stage3d_physics(int precision, const void* src, const void* base, void* d
                        double b0z, int limiter, int lx, double eta, double gx, double gy, double gz,
                        unsigned long long* bad, void* stream);
 
+/* wb_stage2d on a work list cut into tx x ty tiles, one of the shapes wb_tile_shapes lists
+ * (no counterpart in the reference: the tile shape is this implementation's schedule,
+ * picked by the autotuner). Ideal MHD; the non-ideal kernel runs on the default shape. */
+int wb_stage2d_tiled(int precision, const void* src, const void* base, void* dst, const void* patches,
+                     const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+                     int limiter, int tx, int ty, unsigned long long* bad, double* bflux, void* stream);
+
 /* Tile shape of the stage kernels: 2D (TX, TY); 3D (TY, TZ). */
 int wb_tile_shape(int ndim, int precision, int* a, int* b);
+
+/* The 2D tile shapes the stage kernel is built for: up to `max` (tx, ty) pairs into
+ * shapes[2 * i], shapes[2 * i + 1], the default first; returns how many there are. */
+int wb_tile_shapes(int ndim, int precision, int* shapes, int max);
 
 /* Per-instance max fast-wave rate and min density (carafe/mhd.py:930-963,
  * carafe/mhd3d.py:674-724) as order-preserving keys: keys[2i], keys[2i+1]. Work list:

@@ -458,3 +458,32 @@ def test_fused_3d_resistivity_and_gravity_match_the_reference(runs3d):
         scale = float(np.max(np.abs(want[key])))
         assert float(np.max(np.abs(got32[key] - want[key]))) < 2e-5 * max(scale, 1.0), key
     assert fused64.divergence() < 1e-13
+
+
+def test_every_2d_tile_shape_gives_the_same_steps():
+    """The 2D stage kernel on each tile shape it is built for: a face's flux and a cell's
+    update use the same arithmetic whichever tile holds them, so the steps are bitwise
+    those of the default shape (patch sizes that are not multiples of the tiles)."""
+    from wellbalanced_b200 import _lib
+    from wellbalanced_b200.autotune import tune_tile2d
+    from wellbalanced_b200.mhd import MHD2D
+
+    for precision in (32, 64):
+        reference = MHD2D.orszag_tang(40, precision=precision, limiter="mc")
+        for _ in range(3):
+            reference.step()
+        want = reference.engine.state.clone()
+        for tile in _lib.tile_shapes_2d(precision):
+            model = MHD2D.orszag_tang(40, precision=precision, limiter="mc", tile=tile)
+            assert model.engine.layout.tile_shape == tile
+            for _ in range(3):
+                model.step()
+            assert torch.equal(model.engine.state, want), (precision, tile)
+        tuned = MHD2D.orszag_tang(40, precision=precision, limiter="mc", tile="auto")
+        assert tuned.tile in _lib.tile_shapes_2d(precision)
+        for _ in range(3):
+            tuned.step()
+        assert torch.equal(tuned.engine.state, want)
+        best, timings = tune_tile2d(tuned.engine, use_cache=False)
+        assert set(timings) == {f"{tx}x{ty}" for tx, ty in _lib.tile_shapes_2d(precision)}
+        assert all(v > 0 for v in timings.values())

@@ -38,7 +38,10 @@ SIGNATURES = {
                            c_double, c_double, c_double, c_double, c_double, c_dp, c_dp],
     "wb_stage3d_physics": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double,
                            c_double, c_int, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp],
+    "wb_stage2d_tiled": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_int,
+                         c_int, c_int, c_dp, c_dp, c_dp],
     "wb_tile_shape": [c_int, c_int, c_dp, c_dp],
+    "wb_tile_shapes": [c_int, c_int, c_dp, c_int],
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],
     "wb_finalize_dt": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
@@ -103,6 +106,16 @@ def call(name, *args):
     if status != 0:
         raise WBError(f"{name}: status {status}: {lib.wb_last_error().decode()}")
     return status
+
+
+def tile_shapes_2d(precision) -> list[tuple[int, int]]:
+    """The (tx, ty) tile shapes the 2D stage kernel is built for, the default first."""
+    lib = load()
+    buf = (ctypes.c_int * 32)()
+    count = lib.wb_tile_shapes(2, int(precision), buf, 16)
+    if count < 0:
+        raise WBError(f"wb_tile_shapes: status {count}: {lib.wb_last_error().decode()}")
+    return [(buf[2 * i], buf[2 * i + 1]) for i in range(min(count, 16))]
 
 
 def version() -> str:

@@ -1,12 +1,14 @@
-"""Autotuner of the stage kernels' schedule.
+"""Autotuner of the stage kernels' schedule and tile shapes.
 
 The 3D stage kernel marches each 16 x 16 (y, z) column over ``lx`` x-planes per tile: a
 longer march reads fewer halo planes per cell (two extra planes per tile) but gives fewer
-tiles to spread over the 148 SMs, so the best ``lx`` depends on the patch sizes. `tune_lx`
-times the stage kernel (its stage-1 form, which writes only the scratch pool) on an
-engine's own layout and state for each candidate and keeps the fastest; results are
-remembered per (precision, patch shapes) for the process. ``MHD3D(..., lx="auto")`` tunes
-when its state is first set.
+tiles to spread over the 148 SMs, so the best ``lx`` depends on the patch sizes. The 2D
+stage kernel is built for a few tile shapes (``wb_tile_shapes``): small tiles waste less
+of small patches and give more blocks, large ones re-read fewer halo cells. `tune_lx` and
+`tune_tile2d` time the stage kernel (its stage-1 form, which writes only the scratch pool)
+on an engine's own layout and state for each candidate and keep the fastest; results are
+remembered per (precision, limiter, patch shapes) for the process. ``MHD3D(...,
+lx="auto")`` and ``MHD2D(..., tile="auto")`` tune when their state is first set.
 """
 
 from __future__ import annotations
@@ -16,7 +18,7 @@ import torch
 from wellbalanced_b200 import _lib
 
 CANDIDATES = (8, 16, 32, 64, 128)
-_CACHE: dict[tuple, int] = {}
+_CACHE: dict[tuple, object] = {}
 
 
 def _key(engine):
@@ -65,6 +67,46 @@ def tune_lx(engine, candidates=CANDIDATES, repeats=5, use_cache=True):
     _set_lx(engine, best)
     _CACHE[key] = best
     return best, timings
+
+
+def _set_tile(engine, tile):
+    from wellbalanced_b200.engine import _device_bytes
+
+    engine.layout.set_tile(tile)
+    engine.tiles = _device_bytes(engine.layout.tiles, engine.device, _lib.TILE)
+    engine.ntiles = int(engine.layout.tiles.size)
+
+
+def tune_tile2d(engine, repeats=5, use_cache=True):
+    """The fastest tile shape of the 2D stage kernel for `engine`; the engine is left set
+    to it. Returns ``((tx, ty), {"TXxTY": mean ms per stage launch})`` (an empty dict when
+    cached). Ideal MHD only: the non-ideal kernel runs on the default tiles."""
+    if engine.ndim != 2:
+        raise ValueError("the tile shapes apply to the 2D stage kernel")
+    if engine.physics is not None:
+        raise ValueError("the non-ideal 2D kernel runs on the default tile shape")
+    key = ("tile2d", *_key(engine))
+    if use_cache and key in _CACHE:
+        _set_tile(engine, _CACHE[key])
+        return _CACHE[key], {}
+    timings = {}
+    bad = engine.bad.clone()
+    for tile in _lib.tile_shapes_2d(engine.precision):
+        _set_tile(engine, tile)
+        engine.stage(engine.state, None, engine.stage_pool)  # warm-up
+        torch.cuda.synchronize(engine.device)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(repeats):
+            engine.stage(engine.state, None, engine.stage_pool)
+        end.record()
+        torch.cuda.synchronize(engine.device)
+        timings[tile] = start.elapsed_time(end) / repeats
+    engine.bad.copy_(bad)
+    best = min(timings, key=timings.get)
+    _set_tile(engine, best)
+    _CACHE[key] = best
+    return best, {f"{tx}x{ty}": ms for (tx, ty), ms in timings.items()}
 
 
 def describe(timings):

@@ -26,7 +26,7 @@ class Batch:
     """N independent periodic 2D MHD problems on the device (ideal MHD, fused stages)."""
 
     def __init__(self, sides, *, gamma=5.0 / 3.0, limiter="mc", cfl=0.4, precision=32, device="cuda",
-                 bounds=((0.0, 1.0), (0.0, 1.0))):
+                 bounds=((0.0, 1.0), (0.0, 1.0)), tile=None):
         if limiter not in LIMITER_CODES:
             raise ValueError(f"limiter is one of {sorted(LIMITER_CODES)}")
         if not 0.0 < cfl <= 1.0:
@@ -53,6 +53,15 @@ class Batch:
         self._patch_starts = np.cumsum([0] + [1] * self.count)
         self.steps = 0
         self._graph = None
+        # tile shape of the stage kernel: None (default), (tx, ty), or "auto" (tuned in
+        # finish_state, on the batch's own patch sizes)
+        self._auto_tile = tile == "auto"
+        self.tile = None if tile is None or self._auto_tile else tuple(tile)
+        self.tile_timings = None
+        if self.tile is not None:
+            from wellbalanced_b200.autotune import _set_tile
+
+            _set_tile(self.engine, self.tile)
 
     @classmethod
     def orszag_tang(cls, count, *, seed=0, precision=32, **options):
@@ -94,6 +103,12 @@ class Batch:
 
     def finish_state(self):
         self.engine.fill(self.engine.state)
+        if self._auto_tile:
+            from wellbalanced_b200.autotune import tune_tile2d
+
+            self.tile, timings = tune_tile2d(self.engine)
+            self.tile_timings = timings or self.tile_timings
+            self._graph = None
         self.engine.time.zero_()
         self.steps = 0
 

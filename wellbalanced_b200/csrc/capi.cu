@@ -165,10 +165,9 @@ int wb_mhd_conductive(const double* prim, const double* bxf, const double* byf, 
                                 as_stream(stream));
 }
 
-int wb_stage2d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
-               int ntiles, const double* dt, double gamma, double b0x, double b0y, int limiter,
-               unsigned long long* bad, double* bflux, void* stream) {
-  set_error("");
+static int stage2d(int precision, const void* src, const void* base, void* dst, const void* patches,
+                   const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, int limiter,
+                   int tx, int ty, unsigned long long* bad, double* bflux, void* stream) {
   if (!precision_ok(precision, "stage2d") || !ptrs_ok({src, dst, patches, tiles, dt, bad}, "stage2d"))
     return kBadArgument;
   if (ntiles < 0 || !(gamma > 1.0)) {
@@ -179,12 +178,40 @@ int wb_stage2d(int precision, const void* src, const void* base, void* dst, cons
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                        1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, bflux, 0};
-    return launch_stage2d<float>(a, ntiles, limiter, as_stream(stream));
+    return launch_stage2d<float>(a, ntiles, limiter, tx, ty, as_stream(stream));
   }
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, bflux, 0};
-  return launch_stage2d<double>(a, ntiles, limiter, as_stream(stream));
+  return launch_stage2d<double>(a, ntiles, limiter, tx, ty, as_stream(stream));
+}
+
+int wb_stage2d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
+               int ntiles, const double* dt, double gamma, double b0x, double b0y, int limiter,
+               unsigned long long* bad, double* bflux, void* stream) {
+  set_error("");
+  int tx, ty;
+  tile_shape_2d(precision == 64, &tx, &ty);
+  return stage2d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, limiter, tx, ty, bad, bflux,
+                 stream);
+}
+
+int wb_stage2d_tiled(int precision, const void* src, const void* base, void* dst, const void* patches,
+                     const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, int limiter,
+                     int tx, int ty, unsigned long long* bad, double* bflux, void* stream) {
+  set_error("");
+  return stage2d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, limiter, tx, ty, bad, bflux,
+                 stream);
+}
+
+int wb_tile_shapes(int ndim, int precision, int* shapes, int max) {
+  set_error("");
+  if (!precision_ok(precision, "tile_shapes") || (max > 0 && !shapes)) return kBadArgument;
+  if (ndim != 2) {
+    set_error("tile_shapes: the 3D kernel has one tile shape (wb_tile_shape) and a tunable x-march");
+    return kBadArgument;
+  }
+  return tile_shapes_2d(precision == 64, shapes, max);
 }
 
 int wb_stage2d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
@@ -199,18 +226,20 @@ int wb_stage2d_physics(int precision, const void* src, const void* base, void* d
     set_error("stage2d_physics: ntiles must be >= 0, gamma > 1, and eta and the conductivities >= 0");
     return kBadArgument;
   }
+  int tx, ty;  // the non-ideal kernel runs on the default tiles
+  tile_shape_2d(precision == 64, &tx, &ty);
   if (precision == 32) {
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                        1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, nullptr, 0};
     a.eta = eta, a.kappa_par = kappa_par, a.kappa_perp = kappa_perp, a.gravity[0] = gx, a.gravity[1] = gy;
-    return launch_stage2d<float>(a, ntiles, limiter, as_stream(stream));
+    return launch_stage2d<float>(a, ntiles, limiter, tx, ty, as_stream(stream));
   }
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, nullptr, 0};
   a.eta = eta, a.kappa_par = kappa_par, a.kappa_perp = kappa_perp, a.gravity[0] = gx, a.gravity[1] = gy;
-  return launch_stage2d<double>(a, ntiles, limiter, as_stream(stream));
+  return launch_stage2d<double>(a, ntiles, limiter, tx, ty, as_stream(stream));
 }
 
 int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,

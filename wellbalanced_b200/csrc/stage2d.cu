@@ -17,16 +17,23 @@
 
 namespace wb {
 
+// Tile shapes (TX x TY cells) the 2D stage kernel is built for; the first of each precision
+// is the default and the only one with the non-ideal terms. The others are candidates of
+// the autotuner (more tiles for small patches, less halo overhead for large ones).
 template <typename S>
 struct Tile2D;
 
 template <>
 struct Tile2D<float> {
   static constexpr int TX = 16, TY = 32;
+  static constexpr int kShapes = 4;
+  static constexpr int kShape[kShapes][2] = {{16, 32}, {8, 32}, {16, 16}, {32, 16}};
 };
 template <>
 struct Tile2D<double> {
   static constexpr int TX = 8, TY = 32;
+  static constexpr int kShapes = 3;
+  static constexpr int kShape[kShapes][2] = {{8, 32}, {8, 16}, {16, 16}};
 };
 
 template <typename S>
@@ -55,10 +62,9 @@ __device__ __forceinline__ S temperature(const S* sP, int t) {
 
 // PHYS: the resistive and Braginskii-conductive face terms and gravity sources of the
 // reference (carafe/mhd.py:844-927) in the same kernel; false for ideal MHD.
-template <typename S, int LIM, bool PHYS>
+template <typename S, int LIM, bool PHYS, int TX, int TY>
 __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
-  constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
   constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
   constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -273,39 +279,76 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
   }
 }
 
-template <typename S>
-int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
-  constexpr int TX = Tile2D<S>::TX, TY = Tile2D<S>::TY;
+template <typename S, int LIM, bool PHYS, int TX, int TY>
+void launch_shape(const StageArgs<S>& args, int ntiles, cudaStream_t stream) {
   constexpr int NC = (TX + 4) * (TY + 4), NF = (TX + 1) * (TY + 1);
   const size_t smem = sizeof(S) * (11 * NC + 14 * NF);
+  cudaFuncSetAttribute(stage2d_kernel<S, LIM, PHYS, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  stage2d_kernel<S, LIM, PHYS, TX, TY><<<ntiles, 256, smem, stream>>>(args);
+}
+
+// One limiter: the default shape (ideal or non-ideal) or one of the other shapes (ideal).
+template <typename S, int LIM>
+int launch_limiter(const StageArgs<S>& args, int ntiles, bool phys, int shape, cudaStream_t stream) {
+  using T = Tile2D<S>;
+  if (shape == 0) {
+    if (phys)
+      launch_shape<S, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+    else
+      launch_shape<S, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+    return kOk;
+  }
+  if (phys) {
+    set_error("stage2d: the non-ideal terms run on the default %dx%d tiles", T::TX, T::TY);
+    return kBadArgument;
+  }
+  switch (shape) {
+    case 1: launch_shape<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream); break;
+    case 2: launch_shape<S, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream); break;
+    default:
+      if constexpr (T::kShapes > 3) launch_shape<S, LIM, false, T::kShape[3][0], T::kShape[3][1]>(args, ntiles, stream);
+      break;
+  }
+  return kOk;
+}
+
+template <typename S>
+int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, int tx, int ty, cudaStream_t stream) {
   if (ntiles <= 0) return kOk;
+  int shape = -1;
+  for (int i = 0; i < Tile2D<S>::kShapes; ++i)
+    if (Tile2D<S>::kShape[i][0] == tx && Tile2D<S>::kShape[i][1] == ty) shape = i;
+  if (shape < 0) {
+    set_error("stage2d: no %dx%d tile shape for this precision", tx, ty);
+    return kBadArgument;
+  }
   const bool phys = args.eta != 0.0 || args.kappa_par != 0.0 || args.kappa_perp != 0.0 || args.gravity[0] != 0.0 ||
                     args.gravity[1] != 0.0;
+  int status;
   switch (limiter) {
-#define WB_CASE(L)                                                                                           \
-  case L:                                                                                                    \
-    if (phys) {                                                                                              \
-      cudaFuncSetAttribute(stage2d_kernel<S, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-      stage2d_kernel<S, L, true><<<ntiles, 256, smem, stream>>>(args);                                       \
-    } else {                                                                                                 \
-      cudaFuncSetAttribute(stage2d_kernel<S, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-      stage2d_kernel<S, L, false><<<ntiles, 256, smem, stream>>>(args);                                      \
-    }                                                                                                        \
-    break;
-    WB_CASE(0)
-    WB_CASE(1)
-    WB_CASE(2)
-    WB_CASE(3)
-#undef WB_CASE
+    case 0: status = launch_limiter<S, 0>(args, ntiles, phys, shape, stream); break;
+    case 1: status = launch_limiter<S, 1>(args, ntiles, phys, shape, stream); break;
+    case 2: status = launch_limiter<S, 2>(args, ntiles, phys, shape, stream); break;
+    case 3: status = launch_limiter<S, 3>(args, ntiles, phys, shape, stream); break;
     default:
       set_error("limiter code %d is not one of 0..3", limiter);
       return kBadArgument;
   }
+  if (status != kOk) return status;
   return check_launch("stage2d");
 }
 
-template int launch_stage2d<float>(const StageArgs<float>&, int, int, cudaStream_t);
-template int launch_stage2d<double>(const StageArgs<double>&, int, int, cudaStream_t);
+template int launch_stage2d<float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
+template int launch_stage2d<double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+
+int tile_shapes_2d(int fp64, int* shapes, int max) {
+  const int count = fp64 ? Tile2D<double>::kShapes : Tile2D<float>::kShapes;
+  for (int i = 0; i < count && i < max; ++i) {
+    shapes[2 * i] = fp64 ? Tile2D<double>::kShape[i][0] : Tile2D<float>::kShape[i][0];
+    shapes[2 * i + 1] = fp64 ? Tile2D<double>::kShape[i][1] : Tile2D<float>::kShape[i][1];
+  }
+  return count;
+}
 
 void tile_shape_2d(int fp64, int* tx, int* ty) {
   *tx = fp64 ? Tile2D<double>::TX : Tile2D<float>::TX;

@@ -209,6 +209,7 @@ class RankLayout:
         self.precision = layout.precision
         self.lx = layout.lx
         self.tile_shape = layout.tile_shape
+        self.default_tile = getattr(layout, "default_tile", layout.tile_shape)
         self.walls = layout.walls
         self.max_level = layout.max_level
         self.h = None

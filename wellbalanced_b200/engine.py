@@ -167,13 +167,16 @@ class Engine:
             start.record(torch.cuda.current_stream(self.device) if self.stream is None else self.stream)
         self.launches += 1
         if self.ndim == 2 and self.physics is not None:
+            if tuple(self.layout.tile_shape) != tuple(self.layout.default_tile):
+                raise ValueError("the non-ideal 2D stage kernel runs on the default tile shape")
             _lib.call("wb_stage2d_physics", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
                       self.gamma, b[0], b[1], self.limiter, *self.physics, self.bad.data_ptr(), s)
         elif self.ndim == 2:
-            _lib.call("wb_stage2d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
+            tx, ty = self.layout.tile_shape
+            _lib.call("wb_stage2d_tiled", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
-                      self.gamma, b[0], b[1], self.limiter, self.bad.data_ptr(),
+                      self.gamma, b[0], b[1], self.limiter, tx, ty, self.bad.data_ptr(),
                       None if bflux is None else bflux.data_ptr(), s)
         elif self.physics is not None:
             _lib.call("wb_stage3d_physics", self.precision, src.data_ptr(),

@@ -179,7 +179,7 @@ class Layout:
     """Pool layout, work lists and op lists of a hierarchy for the MHD state."""
 
     def __init__(self, hierarchy: AMRHierarchy, *, walls=None, precision=32, lx=32, instances=None,
-                 align=8):
+                 align=8, tile=None):
         self.h = hierarchy
         self.ndim = hierarchy.ndim
         if self.ndim not in (2, 3):
@@ -188,6 +188,8 @@ class Layout:
         self.groups = field_groups(self.ndim)
         self.precision = precision
         self.lx = lx
+        #: 2D: the (tx, ty) tile shape of the stage kernel's work list (None: the default)
+        self.tile = None if tile is None else tuple(int(v) for v in tile)
         self.walls = walls or ((False, False),) * self.ndim
         patches = hierarchy.patches
         self.npatches = len(patches)
@@ -311,21 +313,40 @@ class Layout:
         a, b = ctypes.c_int(), ctypes.c_int()
         _lib.call("wb_tile_shape", self.ndim, self.precision, ctypes.addressof(a), ctypes.addressof(b))
         self.tile_shape = (a.value, b.value)
+        self.default_tile = self.tile_shape
+        if self.ndim == 2 and getattr(self, "tile", None) is not None:
+            if self.tile not in _lib.tile_shapes_2d(self.precision):
+                raise ValueError(f"no {self.tile} tile shape; built: {_lib.tile_shapes_2d(self.precision)}")
+            self.tile_shape = self.tile
         del lib
+        self._cut_tiles()
+
+    def set_tile(self, tile):
+        """Cut the 2D stage kernel's work list into `tile` = (tx, ty) tiles (one of the
+        shapes `_lib.tile_shapes_2d` lists)."""
+        tile = tuple(int(v) for v in tile)
+        if self.ndim != 2 or tile not in _lib.tile_shapes_2d(self.precision):
+            raise ValueError(f"no 2D tile shape {tile} for float{self.precision}")
+        self.tile = self.tile_shape = tile
+        self._cut_tiles()
+
+    def _cut_tiles(self):
+        """The stage kernel's work list: every patch's computed cells and nodes in tiles."""
         tiles = []
-        for p in self.h.patches:
-            own = [p.shape[a] + (1 if self.own[p.index][a] else 0) for a in range(self.ndim)]
+        for index in range(self.npatches):
+            n = [int(v) for v in self.rows[index]["n"]]
+            own = [n[a] + (1 if self.own[index][a] else 0) for a in range(self.ndim)]
             if self.ndim == 2:
                 tx, ty = self.tile_shape
                 for x0 in range(0, own[0], tx):
                     for y0 in range(0, own[1], ty):
-                        tiles.append((p.index, x0, y0, 0))
+                        tiles.append((index, x0, y0, 0))
             else:
                 ty, tz = self.tile_shape
                 for x0 in range(0, own[0], self.lx):
                     for y0 in range(0, own[1], ty):
                         for z0 in range(0, own[2], tz):
-                            tiles.append((p.index, x0, y0, z0))
+                            tiles.append((index, x0, y0, z0))
         self.tiles = np.array(tiles, dtype=np.int32).view(_lib.TILE).reshape(-1) if tiles else np.zeros(0, _lib.TILE)
 
     def _chunks(self, per=2048):
@@ -602,6 +623,8 @@ class Layout:
         out.precision = first.precision
         out.lx = first.lx
         out.tile_shape = first.tile_shape
+        out.tile = getattr(first, "tile", None)
+        out.default_tile = getattr(first, "default_tile", first.tile_shape)
         out.walls = first.walls
         rows, tiles, chunk_patch, chunk_start, inv = [], [], [], [], []
         same_levels, boundary_levels, interp_levels = {}, {}, {}

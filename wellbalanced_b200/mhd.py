@@ -60,6 +60,7 @@ class MHD2D:
         prefix: str = "mhd_",
         precision: int = 64,
         device: str = "cuda",
+        tile: tuple[int, int] | str | None = None,
     ) -> None:
         if hierarchy.ndim != 2:
             raise ValueError("MHD2D needs a 2D hierarchy")
@@ -101,6 +102,11 @@ class MHD2D:
         self.periodic = tuple(hierarchy.periodic)
         self.precision = int(precision)
         self.device = device
+        # tile shape of the stage kernel: None (the default), (tx, ty), or "auto" (tuned
+        # when the state is first set; ideal MHD only)
+        self._auto_tile = tile == "auto"
+        self.tile = None if tile is None or self._auto_tile else tuple(tile)
+        self.tile_timings = None
         self._build_engine()
         self.time = 0.0
         self.steps = 0
@@ -128,6 +134,12 @@ class MHD2D:
         physics = (self.resistivity, self.conduction[0], self.conduction[1], self.gravity[0], self.gravity[1])
         if any(physics):
             self.engine.physics = tuple(float(v) for v in physics)
+        if self.tile is not None and self._fused:
+            if self.engine.physics is not None and self.tile != self.engine.layout.default_tile:
+                raise ValueError("resistivity, conduction and gravity run on the default tile shape")
+            from wellbalanced_b200.autotune import _set_tile
+
+            _set_tile(self.engine, self.tile)
 
     # construction of common cases (carafe/mhd.py:486-671) -----------------------------------------
     @classmethod
@@ -298,6 +310,11 @@ class MHD2D:
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
+        if self._auto_tile and self._fused and eng.physics is None:
+            from wellbalanced_b200.autotune import tune_tile2d
+
+            self.tile, timings = tune_tile2d(eng)
+            self.tile_timings = timings or self.tile_timings
         self.time = 0.0
         self.steps = 0
         eng.time.zero_()
