@@ -88,6 +88,18 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
   const int own_nx = nx + ((P.flags & kOwnLast0) ? 1 : 0);
   const int own_ny = ny + ((P.flags & kOwnLast1) ? 1 : 0);
 
+  // stage 2: fetch the Heun base state of the tile's cells and nodes into L2 now (each row
+  // of the tile spans at most two 128-byte lines), so that phase 3 reads it from there
+  if (a.base) {
+    const S* bs = a.base + P.off;
+    const int rows = min(TX, own_nx - x0);
+    for (int t = threadIdx.x; t < 7 * rows * 2; t += blockDim.x) {
+      const int f = t / (rows * 2), row = (t / 2) % rows, half = t & 1;
+      const int col = min(y0 + 2 + half * (TY - 1), ny + 4);
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(bs + f * fs + int64_t(x0 + row + 2) * pitch + col));
+    }
+  }
+
   // 1. cells and nodes -> primitive variables -------------------------------------
   unsigned bad = 0;
   for (int t = threadIdx.x; t < NC; t += blockDim.x) {
