@@ -149,6 +149,7 @@ class Turbulence:
 
         self.n = args.cells
         self.rank = rank
+        self.args = args
         lx = args.lx if args.lx == "auto" else int(args.lx)
         self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=lx)
         self.engine = self.model.engine
@@ -158,11 +159,15 @@ class Turbulence:
     def advance(self, steps):
         self.model.advance(steps, check=False)
 
+    @staticmethod
+    def describe(args):
+        return (f"3D decaying turbulence, periodic {args.cells}^3, MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, "
+                "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1")
+
     def config(self):
         eng = self.engine
         return {
-            "workload": (f"3D decaying turbulence, periodic {self.n}^3, MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, "
-                         "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1"),
+            "workload": self.describe(self.args),
             "cells_per_gpu": self.cells,
             "tile": {"y": eng.layout.tile_shape[0], "z": eng.layout.tile_shape[1], "x_planes": self.lx},
             "autotune_ms_per_launch": describe(self.model.lx_timings),
@@ -216,6 +221,7 @@ class BatchWorkload:
 
         self.count = args.count
         self.rank = rank
+        self.args = args
         self.batch = Batch.orszag_tang(self.count, seed=rank, precision=32, tile="auto")
         self.engine = self.batch.engine
         self.cells = self.batch.cells
@@ -232,12 +238,16 @@ class BatchWorkload:
         self.batch._graph = None
         return 1e3 * seconds / steps
 
+    @staticmethod
+    def describe(args):
+        return (f"{args.count} independent periodic 2D Orszag-Tang problems, sides from {{32, 48, ..., 256}} "
+                "(seeded per rank), amplitudes x U[0.5, 1.5], MC-PLM + HLLD + CT, SSP-RK2, per-instance "
+                "CFL 0.4 dt, float32 state, one launch per kernel for all instances")
+
     def config(self):
         sides = [s for s, _ in self.batch.sides]
         return {
-            "workload": (f"{self.count} independent periodic 2D Orszag-Tang problems, sides from {{32, 48, ..., 256}} "
-                         f"(seed {self.rank}), amplitudes x U[0.5, 1.5], MC-PLM + HLLD + CT, SSP-RK2, per-instance "
-                         "CFL 0.4 dt, float32 state, one launch per kernel for all instances"),
+            "workload": self.describe(self.args),
             "cells_per_gpu": self.cells,
             "instances": self.count,
             "mean_side": float(sum(sides) / len(sides)),
@@ -322,14 +332,18 @@ class Harris:
         self.model._graph = None
         return 1e3 * seconds / steps
 
+    @staticmethod
+    def describe(args):
+        return (f"2D Harris sheet on [-1,1]x[-2,2], base {HARRIS_BASE[0]}x{HARRIS_BASE[1]}, periodic x, "
+                f"outflow y, {HARRIS_LEVELS} refined levels on |J| dx > {HARRIS_THRESHOLD} (patches <= "
+                f"{2 * HARRIS_PATCH} cells a side), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.4 at the finest dx, "
+                "float32 state with float64 refluxing, all patches in one launch per kernel")
+
     def config(self):
         h = self.model.hierarchy
         refined = [p.shape for p in h.patches if p.level]
         return {
-            "workload": (f"2D Harris sheet on [-1,1]x[-2,2], base {HARRIS_BASE[0]}x{HARRIS_BASE[1]}, periodic x, "
-                         f"outflow y, {h.max_level} refined levels on |J| dx > {HARRIS_THRESHOLD} (patches <= "
-                         f"{2 * HARRIS_PATCH} cells a side), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.4 at the finest dx, "
-                         "float32 state with float64 refluxing, all patches in one launch per kernel"),
+            "workload": self.describe(None),
             "cells_per_gpu": self.cells,
             "patches": len(h.patches),
             "patches_per_level": {str(lv): len(h.patches_at_level(lv)) for lv in range(h.max_level + 1)},
@@ -461,7 +475,7 @@ def reference_arm(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"{args.workload}; CPU sample per process: {sample}"},
+        "config": {"workload": WORKLOADS[args.workload].describe(args), "cpu_sample": sample},
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
