@@ -160,11 +160,13 @@ def test_refined_2d_float32_drift_is_at_float32_round_off():
     assert model.composite_divergence() < 1e-6
 
 
-def _alfven_pair(precision=64, **options):
+def _alfven_pair(precision=64, device_cls=None, **options):
     from oracle.mesh import Hierarchy
     from oracle.mhd3d import MHD3D as OracleMHD3D
     from wellbalanced_b200.mesh import AMRHierarchy
     from wellbalanced_b200.mhd3d import MHD3D
+
+    MHD3D = device_cls or MHD3D  # noqa: N806
 
     wavevector = 2 * np.pi * np.array([0.5, 1.0, 1.0])
     k = np.linalg.norm(wavevector)
@@ -246,3 +248,41 @@ def test_graph_replay_equals_direct_steps_on_a_refined_hierarchy():
     assert a.steps == b.steps == 5
     assert a.time == b.time
     np.testing.assert_array_equal(a.engine.state.cpu().numpy(), b.engine.state.cpu().numpy())
+
+
+def test_plain_float64_paths_reflux_like_the_oracle():
+    """The per-kernel float64 paths on refined hierarchies: the flux register from the
+    sweeps' own fluxes and the reflux after the step (patchwork's FluxRegister as the
+    reference calls it), patch by patch against the oracle, in 2D (with resistivity and
+    conduction) and 3D."""
+    from oracle.mesh import Hierarchy
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.plain import PlainMHD2D, PlainMHD3D
+
+    cells = 16
+    box = ((cells - cells // 2, cells + cells // 2), (cells // 2, 3 * cells // 2))
+    for options in ({}, {"resistivity": 2e-3, "conduction": (2e-2, 1e-3)}):
+        oh = Hierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), (True, True))
+        oh.add_patch(1, box)
+        dh = AMRHierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True))
+        dh.add_patch(1, box)
+        oracle = OracleMHD2D(oh, limiter="minmod", **options)
+        plain = PlainMHD2D(dh, limiter="minmod", **options)
+        s = _refined_state()
+        for m in (oracle, plain):
+            m.set_state(s["density"], s["velocity"], s["pressure"], vector_potential=s["vector_potential"], bz=s["bz"])
+        for _ in range(6):
+            plain.step(oracle.step())
+        for op, dp in zip(oracle.hierarchy.patches, plain.hierarchy.patches, strict=True):
+            for f, name in enumerate(oracle.names.values()):
+                np.testing.assert_allclose(plain.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                           err_msg=f"level {op.level} {name} {options}")
+    oracle, plain = _alfven_pair(device_cls=PlainMHD3D, resistivity=0.01)
+    for _ in range(4):
+        plain.step(oracle.step())
+    for op, dp in zip(oracle.hierarchy.patches, plain.hierarchy.patches, strict=True):
+        names = [*oracle.names.values(), *oracle.potential]
+        for f, name in enumerate(names):
+            np.testing.assert_allclose(plain.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
+                                       err_msg=f"3D level {op.level} {name}")

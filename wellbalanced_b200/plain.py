@@ -6,7 +6,8 @@ and stage, the haloed block is gathered into contiguous arrays, the reference's 
 kernels run one by one through the C ABI (``mhd_primitive``, ``mhd_sweep`` per axis —
 after the reference's transposes in 3D —, ``ct_contact`` — all planes of a 3D block in
 one launch —, ``mhd_conductive``, ``mhd_resistive``), every intermediate (primitive
-variables, face fields, fluxes, edge fields) lives in HBM, and the flux-register update,
+variables, face fields, fluxes, edge fields) lives in HBM, and the flux-register update
+(the fine-minus-coarse fluxes of every coarse-fine interface, from the sweeps' own fluxes),
 gravity sources, potential update and Heun combine are device array operations. It is
 the float64 baseline the fused kernels are measured against, and in 3D it carries the
 terms the fused 3D kernel leaves out (resistivity, gravity).
@@ -24,6 +25,51 @@ from wellbalanced_b200.mhd3d import CONSERVED_3D, MHD3D
 
 _FLUX_ROWS = ((0, 1, 2, 3, 4, 6), (0, 2, 1, 3, 4, 6))
 _WALL_ROWS = [0, 2, 3, 4, 6]
+
+
+def _face_ops(engine):
+    import numpy as np
+
+    ops = engine.layout.face_flux_ops
+    return [] if ops is None or ops.size == 0 else list(np.atleast_1d(ops))
+
+
+def _register_update(engine, blocks):
+    """reg += (mean of the fine faces - the coarse face) at every coarse-fine interface
+    face, from the per-patch flux blocks of a stage (patchwork's FluxRegister.update as
+    carafe/mhd.py:906-919 calls it; the slots of the device register, which `Engine.reflux`
+    applies with 0.5 dt after the step).
+
+    ``blocks(patch_index, axis)``: a tensor (fields, ...) of that patch's fluxes through
+    its faces normal to ``axis``, indexed [field, face along axis, transverse haloed or
+    interior indices] as `_plane` reads them.
+    """
+    reg = engine.register
+    for op in _face_ops(engine):
+        axis, length, width = int(op["axis"]), int(op["len"]), int(op["width"])
+        coarse = _plane(blocks(int(op["coarse"]), axis), op, "coarse", length // width, width, 1)
+        fine = _plane(blocks(int(op["fine"]), axis), op, "fine", length // width, width, 2)
+        if int(op["ndim"]) == 2:
+            total = fine[:, :, 0] + fine[:, :, 1]
+            count = 2.0
+        else:
+            total = fine[:, :, 0, :, 0] + fine[:, :, 0, :, 1] + fine[:, :, 1, :, 0] + fine[:, :, 1, :, 1]
+            count = 4.0
+        values = total.reshape(total.shape[0], -1) / count - coarse.reshape(coarse.shape[0], -1)
+        off = int(op["reg_off"])
+        reg[off : off + values.numel()] += values.reshape(-1)
+
+
+def _plane(flux, op, side, n1, n2, step):
+    """The faces of one side of an op from a flux block: 2D (fields, n1[, 2]); 3D (fields,
+    n1[, 2], n2[, 2]). ``flux`` is indexed [field, normal face, t1, t2] after `_oriented`."""
+    plane = int(op[f"{side}_plane"]) - HALO
+    t0 = [int(v) for v in op[f"{side}_t0"]]
+    if int(op["ndim"]) == 2:
+        rows = flux[:, plane, t0[0] : t0[0] + step * n1]
+        return rows.reshape(rows.shape[0], n1, step) if step == 2 else rows
+    rows = flux[:, plane, t0[0] : t0[0] + step * n1, t0[1] : t0[1] + step * n2]
+    return rows.reshape(rows.shape[0], n1, step, n2, step) if step == 2 else rows
 
 
 def _stream():
@@ -96,6 +142,13 @@ class PlainMHD2D(MHD2D):
         eng = self.engine
         eng.fill(eng.state)
         fluxes = {p.index: self._patch_fluxes(p) for p in self.hierarchy.patches}
+        if self.hierarchy.max_level > 0:
+            # x-faces: [row, face, haloed y]; y-faces [row, haloed x, face] -> [row, face, haloed x]
+            def blocks(index, axis):
+                rows = list(_FLUX_ROWS[axis])
+                return fluxes[index][0][rows] if axis == 0 else fluxes[index][1][rows].transpose(1, 2)
+
+            _register_update(eng, blocks)
         gx, gy = self.gravity
         sources = {}
         if gx or gy:
@@ -154,6 +207,8 @@ class PlainMHD2D(MHD2D):
         eng.state.add_(start)
         eng.state.mul_(0.5)
         if self.hierarchy.max_level > 0:
+            eng.dt.fill_(float(dt))
+            eng.reflux(eng.state)
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
         self._raise_if_bad()
@@ -311,6 +366,16 @@ class PlainMHD3D(MHD3D):
         eng = self.engine
         eng.fill(eng.state)
         results = {p.index: self._patch_fluxes(p) for p in self.hierarchy.patches}
+        if self.hierarchy.max_level > 0:
+            # interior blocks [face along axis, ...] -> [field, face, t1, t2] with haloed
+            # transverse indices (two zero-padded halo layers in front)
+            def blocks(index, axis):
+                t1, t2 = (b for b in range(3) if b != axis)  # the ops' transverse axes, in order
+                stacked = torch.stack([results[index][0][name][axis] for name in CONSERVED_3D])
+                oriented = stacked.permute(0, 1 + axis, 1 + t1, 1 + t2)
+                return torch.nn.functional.pad(oriented, (HALO, 0, HALO, 0))
+
+            _register_update(eng, blocks)
         g = self.gravity
         sources = {}
         if any(g):
@@ -358,6 +423,8 @@ class PlainMHD3D(MHD3D):
         eng.state.add_(start)
         eng.state.mul_(0.5)
         if self.hierarchy.max_level > 0:
+            eng.dt.fill_(float(dt))
+            eng.reflux(eng.state)
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
         self._raise_if_bad()
