@@ -141,8 +141,12 @@ def describe(timings):
 
 
 class Turbulence:
-    kernel = "wb::stage3d_kernel<float, 2, false>"
     bytes_per_zone_update = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
+
+    @property
+    def kernel(self):
+        ty, tz = self.engine.layout.tile_shape
+        return f"wb::stage3d_kernel<float, 2, false, {ty}, {tz}>"
 
     def __init__(self, args, rank):
         from wellbalanced_b200.mhd3d import MHD3D

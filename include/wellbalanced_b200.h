@@ -129,11 +129,20 @@ int wb_stage2d_tiled(int precision, const void* src, const void* base, void* dst
                      const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
                      int limiter, int tx, int ty, unsigned long long* bad, double* bflux, void* stream);
 
+/* wb_stage3d on a work list cut into ty x tz columns, one of the shapes wb_tile_shapes
+ * lists (no counterpart in the reference: the autotuner's schedule). Ideal MHD; the
+ * non-ideal kernel runs on the default shape. */
+int wb_stage3d_tiled(int precision, const void* src, const void* base, void* dst, const void* patches,
+                     const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y,
+                     double b0z, int limiter, int lx, int ty, int tz, unsigned long long* bad, double* bflux,
+                     void* stream);
+
 /* Tile shape of the stage kernels: 2D (TX, TY); 3D (TY, TZ). */
 int wb_tile_shape(int ndim, int precision, int* a, int* b);
 
-/* The 2D tile shapes the stage kernel is built for: up to `max` (tx, ty) pairs into
- * shapes[2 * i], shapes[2 * i + 1], the default first; returns how many there are. */
+/* The tile shapes the 2D / 3D stage kernel is built for: up to `max` pairs ((tx, ty) in
+ * 2D, (ty, tz) in 3D) into shapes[2 * i], shapes[2 * i + 1], the default first; returns
+ * how many there are. */
 int wb_tile_shapes(int ndim, int precision, int* shapes, int max);
 
 /* Per-instance max fast-wave rate and min density (carafe/mhd.py:930-963,

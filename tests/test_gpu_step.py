@@ -366,8 +366,10 @@ def test_plain_3d_step_matches_the_reference(runs3d):
 
 
 def test_autotuned_x_march_gives_the_same_steps():
-    """`lx="auto"` times the stage kernel for each x-march length and keeps the fastest;
-    the tiling changes no arithmetic, so every choice gives bitwise the same steps."""
+    """`lx="auto"` times the stage kernel for each tile shape and x-march length and keeps
+    the fastest. The x-march changes no arithmetic (bitwise the same steps); another tile
+    shape is another instantiation of the kernel, whose compiled multiply-adds may round
+    differently, so the steps agree to float32 rounding."""
     import torch
 
     from wellbalanced_b200.autotune import CANDIDATES
@@ -375,11 +377,29 @@ def test_autotuned_x_march_gives_the_same_steps():
 
     tuned = MHD3D.turbulence(24, seed=2, precision=32, lx="auto")
     fixed = MHD3D.turbulence(24, seed=2, precision=32, lx=8)
-    assert tuned.lx in CANDIDATES and tuned.lx_timings and tuned.lx == min(tuned.lx_timings, key=tuned.lx_timings.get)
+    ty, tz = tuned.engine.layout.tile_shape
+    assert tuned.lx in CANDIDATES and tuned.lx_timings
+    assert f"{ty}x{tz}/{tuned.lx}" == min(tuned.lx_timings, key=tuned.lx_timings.get)
     for _ in range(3):
         fixed.step(tuned.step())
     torch.cuda.synchronize()
-    assert torch.equal(tuned.engine.state, fixed.engine.state)
+    if tuned.engine.layout.tile_shape == fixed.engine.layout.tile_shape:
+        assert torch.equal(tuned.engine.state, fixed.engine.state)
+    else:
+        assert torch.allclose(tuned.engine.state, fixed.engine.state, rtol=1e-5, atol=1e-6)
+    # same shape, another x-march: bitwise
+    other = MHD3D.turbulence(24, seed=2, precision=32, lx=16)
+    other.engine.layout.set_tile(tuned.engine.layout.tile_shape)
+    from wellbalanced_b200.autotune import _set_lx
+
+    _set_lx(other.engine, 16)
+    again = MHD3D.turbulence(24, seed=2, precision=32, lx=8)
+    again.engine.layout.set_tile(tuned.engine.layout.tile_shape)
+    _set_lx(again.engine, 8)
+    for _ in range(3):
+        again.step(other.step())
+    torch.cuda.synchronize()
+    assert torch.equal(other.engine.state, again.engine.state)
 
 
 def test_plain_3d_resistivity_and_gravity_match_the_reference(runs3d):
@@ -487,3 +507,44 @@ def test_every_2d_tile_shape_gives_the_same_steps():
         best, timings = tune_tile2d(tuned.engine, use_cache=False)
         assert set(timings) == {f"{tx}x{ty}" for tx, ty in _lib.tile_shapes_2d(precision)}
         assert all(v > 0 for v in timings.values())
+
+
+def test_every_3d_tile_shape_gives_the_same_steps():
+    """The 3D stage kernel on each tile shape it is built for (with the rim threads of the
+    smaller tile) gives the steps of the default shape, float32 and float64, on a box whose
+    sides are not multiples of the tiles: to rounding, since each shape is a separate
+    instantiation whose compiled multiply-adds may round differently (a wrong index would
+    show at O(1))."""
+    from wellbalanced_b200 import _lib
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    k = 2.0 * np.pi
+
+    def model(precision, tile=None, lx=8):
+        m = MHD3D(AMRHierarchy((20, 18, 26), ((0.0, 1.0),) * 3, periodic=(True, True, False)), precision=precision,
+                  limiter="mc", cfl=0.3, lx=lx)
+        if tile is not None:
+            from wellbalanced_b200.autotune import _set_lx
+
+            m.engine.layout.set_tile(tile)
+            _set_lx(m.engine, lx)
+        m.set_state(lambda x, y, z: 1.0 + 0.2 * np.sin(k * (x + y)),
+                    (lambda x, y, z: 0.5 * np.sin(k * y), lambda x, y, z: 0.5 * np.sin(k * z),
+                     lambda x, y, z: 0.5 * np.sin(k * x)),
+                    1.0,
+                    vector_potential=(lambda x, y, z: 0.1 * np.cos(k * z), lambda x, y, z: 0.1 * np.cos(k * x),
+                                      lambda x, y, z: 0.1 * np.cos(k * y)))
+        return m
+
+    for precision in (32, 64):
+        reference = model(precision)
+        for _ in range(3):
+            reference.step()
+        for tile in _lib.tile_shapes(3, precision):
+            m = model(precision, tile)
+            assert m.engine.layout.tile_shape == tile
+            for _ in range(3):
+                m.step()
+            tol = 1e-5 if precision == 32 else 1e-12
+            assert torch.allclose(m.engine.state, reference.engine.state, rtol=tol, atol=tol * 0.1), (precision, tile)

@@ -40,6 +40,8 @@ SIGNATURES = {
                            c_double, c_int, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp],
     "wb_stage2d_tiled": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_int,
                          c_int, c_int, c_dp, c_dp, c_dp],
+    "wb_stage3d_tiled": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_double,
+                         c_int, c_int, c_int, c_int, c_dp, c_dp, c_dp],
     "wb_tile_shape": [c_int, c_int, c_dp, c_dp],
     "wb_tile_shapes": [c_int, c_int, c_dp, c_int],
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
@@ -110,9 +112,15 @@ def call(name, *args):
 
 def tile_shapes_2d(precision) -> list[tuple[int, int]]:
     """The (tx, ty) tile shapes the 2D stage kernel is built for, the default first."""
+    return tile_shapes(2, precision)
+
+
+def tile_shapes(ndim, precision) -> list[tuple[int, int]]:
+    """The tile shapes the stage kernel of `ndim` is built for ((tx, ty) in 2D, (ty, tz) in
+    3D), the default first."""
     lib = load()
     buf = (ctypes.c_int * 32)()
-    count = lib.wb_tile_shapes(2, int(precision), buf, 16)
+    count = lib.wb_tile_shapes(int(ndim), int(precision), buf, 16)
     if count < 0:
         raise WBError(f"wb_tile_shapes: status {count}: {lib.wb_last_error().decode()}")
     return [(buf[2 * i], buf[2 * i + 1]) for i in range(min(count, 16))]

@@ -207,11 +207,11 @@ int wb_stage2d_tiled(int precision, const void* src, const void* base, void* dst
 int wb_tile_shapes(int ndim, int precision, int* shapes, int max) {
   set_error("");
   if (!precision_ok(precision, "tile_shapes") || (max > 0 && !shapes)) return kBadArgument;
-  if (ndim != 2) {
-    set_error("tile_shapes: the 3D kernel has one tile shape (wb_tile_shape) and a tunable x-march");
+  if (ndim != 2 && ndim != 3) {
+    set_error("tile_shapes: ndim must be 2 or 3");
     return kBadArgument;
   }
-  return tile_shapes_2d(precision == 64, shapes, max);
+  return ndim == 2 ? tile_shapes_2d(precision == 64, shapes, max) : tile_shapes_3d(precision == 64, shapes, max);
 }
 
 int wb_stage2d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
@@ -242,10 +242,9 @@ int wb_stage2d_physics(int precision, const void* src, const void* base, void* d
   return launch_stage2d<double>(a, ntiles, limiter, tx, ty, as_stream(stream));
 }
 
-int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
-               int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z, int limiter, int lx,
-               unsigned long long* bad, double* bflux, void* stream) {
-  set_error("");
+static int stage3d(int precision, const void* src, const void* base, void* dst, const void* patches,
+                   const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z,
+                   int limiter, int lx, int ty, int tz, unsigned long long* bad, double* bflux, void* stream) {
   if (!precision_ok(precision, "stage3d") || !ptrs_ok({src, dst, patches, tiles, dt, bad}, "stage3d"))
     return kBadArgument;
   if (ntiles < 0 || !(gamma > 1.0) || lx <= 0) {
@@ -256,12 +255,30 @@ int wb_stage3d(int precision, const void* src, const void* base, void* dst, cons
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                        1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, bflux, lx};
-    return launch_stage3d<float>(a, ntiles, limiter, as_stream(stream));
+    return launch_stage3d<float>(a, ntiles, limiter, ty, tz, as_stream(stream));
   }
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, bflux, lx};
-  return launch_stage3d<double>(a, ntiles, limiter, as_stream(stream));
+  return launch_stage3d<double>(a, ntiles, limiter, ty, tz, as_stream(stream));
+}
+
+int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
+               int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z, int limiter, int lx,
+               unsigned long long* bad, double* bflux, void* stream) {
+  set_error("");
+  int ty, tz;
+  tile_shape_3d(precision == 64, &ty, &tz);
+  return stage3d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, b0z, limiter, lx, ty, tz,
+                 bad, bflux, stream);
+}
+
+int wb_stage3d_tiled(int precision, const void* src, const void* base, void* dst, const void* patches,
+                     const void* tiles, int ntiles, const double* dt, double gamma, double b0x, double b0y, double b0z,
+                     int limiter, int lx, int ty, int tz, unsigned long long* bad, double* bflux, void* stream) {
+  set_error("");
+  return stage3d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, b0z, limiter, lx, ty, tz,
+                 bad, bflux, stream);
 }
 
 int wb_stage3d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
@@ -276,18 +293,20 @@ int wb_stage3d_physics(int precision, const void* src, const void* base, void* d
     set_error("stage3d_physics: ntiles must be >= 0, gamma > 1, lx > 0 and eta >= 0");
     return kBadArgument;
   }
+  int ty, tz;  // the non-ideal kernel runs on the default tiles
+  tile_shape_3d(precision == 64, &ty, &tz);
   if (precision == 32) {
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                        1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, nullptr, lx};
     a.eta = eta, a.gravity[0] = gx, a.gravity[1] = gy, a.gravity[2] = gz;
-    return launch_stage3d<float>(a, ntiles, limiter, as_stream(stream));
+    return launch_stage3d<float>(a, ntiles, limiter, ty, tz, as_stream(stream));
   }
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, nullptr, lx};
   a.eta = eta, a.gravity[0] = gx, a.gravity[1] = gy, a.gravity[2] = gz;
-  return launch_stage3d<double>(a, ntiles, limiter, as_stream(stream));
+  return launch_stage3d<double>(a, ntiles, limiter, ty, tz, as_stream(stream));
 }
 
 int wb_tile_shape(int ndim, int precision, int* a, int* b) {

@@ -34,12 +34,15 @@ struct StageArgs {
 // tx x ty: the tile shape the work list was cut with (one of tile_shapes_2d)
 template <typename S>
 int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, int tx, int ty, cudaStream_t stream);
+// ty x tz: the tile shape the work list was cut with (one of tile_shapes_3d)
 template <typename S>
-int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream);
+int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, int ty, int tz, cudaStream_t stream);
 
 void tile_shape_2d(int fp64, int* tx, int* ty);
 // The 2D tile shapes built, (tx, ty) pairs, the default first; returns their count.
 int tile_shapes_2d(int fp64, int* shapes, int max);
+// The 3D tile shapes built, (ty, tz) pairs, the default first; returns their count.
+int tile_shapes_3d(int fp64, int* shapes, int max);
 void tile_shape_3d(int fp64, int* ty, int* tz);
 
 // Fast-wave rate max and density min of every patch's cells, per instance, as

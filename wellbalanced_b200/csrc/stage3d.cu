@@ -1,7 +1,8 @@
 // Fused 3D stage kernel: one RK stage of the 3D step over a work list of tiles.
 //
 // A tile is TY x TZ columns (y, z) of a patch, marched along x over `lx` cell planes.
-// 288 threads, each with fixed roles per plane (two barriers per plane):
+// TY TZ + TY + TZ threads (288 for the default 16 x 16 tile), each with fixed roles per
+// plane (two barriers per plane):
 //   * one x-face column (j, k) of the L-shaped set the tile needs — its thread keeps
 //     the four cell planes of the x-stencil of that column in registers;
 //   * one y-face and one z-face of the current plane;
@@ -33,10 +34,28 @@
 
 namespace wb {
 
+// Tile shapes (TY x TZ columns) the kernel is built for, the default first (the only one
+// with the non-ideal terms); the others are candidates of the autotuner: a 8 x 16 tile
+// needs half the shared memory, so twice the CTAs share an SM, at more halo work per cell.
 template <typename S>
 struct Tile3D {
   static constexpr int TY = 16, TZ = 16;
+  static constexpr int kShapes = 2;
+  static constexpr int kShape[kShapes][2] = {{16, 16}, {8, 16}};
 };
+
+template <int TY, int TZ>
+__host__ __device__ constexpr int threads3d() {
+  return TY * TZ + TY + TZ;
+}
+
+// Shared memory of a tile shape: primitive variables (2 planes), face fields (2 or 3),
+// cell E (4 planes), y/z face fluxes (3 planes), x-face fluxes.
+template <typename S, bool PHYS, int TY, int TZ>
+__host__ __device__ constexpr size_t smem3d() {
+  return sizeof(S) * (2 * 8 * (TY + 4) * (TZ + 4) + (PHYS ? 3 : 2) * 3 * (TY + 4) * (TZ + 4) +
+                      4 * 3 * (TY + 1) * (TZ + 1) + 3 * 2 * 7 * (TY + 1) * (TZ + 1) + 3 * (TY + 1) * (TZ + 1));
+}
 
 // Hint that a global value will be read soon: fetch its line into L2.
 __device__ __forceinline__ void prefetch_l2(const void* ptr) {
@@ -50,10 +69,12 @@ __device__ __forceinline__ bool bad3(S r, S u, S v, S w, S p, S bx, S by, S bz) 
            isfinite(by) && isfinite(bz));
 }
 
-// float32: two CTAs per SM (<= 113 registers a thread); float64: one (its shared memory).
-template <typename S>
+// CTAs per SM the shared memory allows (228 KB per SM, 1 KB reserved per CTA), at most 4:
+// the register cap of the launch bounds follows from it.
+template <typename S, bool PHYS, int TY, int TZ>
 struct Occupancy3D {
-  static constexpr int kBlocks = sizeof(S) == 4 ? 2 : 1;
+  static constexpr int kFit = int(233472 / (smem3d<S, PHYS, TY, TZ>() + 1024));
+  static constexpr int kBlocks = kFit < 1 ? 1 : (kFit > 4 ? 4 : kFit);
 };
 
 // Planes of face fields kept in shared memory: two, or three with the resistive terms.
@@ -67,10 +88,10 @@ __device__ __forceinline__ int face_slot(int plane) {
   return PHYS ? (plane + 6) % 3 : (plane + 4) & 1;  // plane >= -3
 }
 
-template <typename S, int LIM, bool PHYS>
-__global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(const StageArgs<S> a) {
+template <typename S, int LIM, bool PHYS, int TY, int TZ>
+__global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY, TZ>::kBlocks))
+    stage3d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
-  constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
   constexpr int RZ = TZ + 4, NR = (TY + 4) * (TZ + 4);  // plane region j, k in [-2, T+2)
   constexpr int GZ = TZ + 1, G = (TY + 1) * (TZ + 1);    // face / column grids
   constexpr int NCORE = TY * TZ;
@@ -106,14 +127,22 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   if (tid < NCORE) {
     cj = yj = zj = tid / TZ;
     ck = yk = zk = tid % TZ;
-  } else if (tid < NCORE + TZ) {
-    cj = -1, ck = tid - NCORE;
-    yj = TY, yk = tid - NCORE;
-    zj = tid - NCORE, zk = TZ;  // TY == TZ
   } else {
-    cj = tid - NCORE - TZ, ck = -1;
-    yj = tid - NCORE - TZ, yk = -1;
-    zj = -1, zk = tid - NCORE - TZ;
+    // the rim: x-columns (-1, k) and (j, -1), y-faces (TY, k) and (j, -1), z-faces
+    // (j, TZ) and (-1, k)
+    const int u = tid - NCORE;
+    if (u < TZ) {
+      cj = -1, ck = u;
+      yj = TY, yk = u;
+    } else {
+      cj = u - TZ, ck = -1;
+      yj = u - TZ, yk = -1;
+    }
+    if (u < TY) {
+      zj = u, zk = TZ;
+    } else {
+      zj = -1, zk = u - TY;
+    }
   }
   const int col_r = (cj + 2) * RZ + (ck + 2);  // column's position in the plane region
   const int col_g = (cj + 1) * GZ + (ck + 1);  // column's index in the face grid
@@ -442,43 +471,71 @@ __global__ void __launch_bounds__(288, Occupancy3D<S>::kBlocks) stage3d_kernel(c
   if (bad) atomicAdd(a.bad, (unsigned long long)bad);
 }
 
+template <typename S, int LIM, bool PHYS, int TY, int TZ>
+void launch_shape3d(const StageArgs<S>& args, int ntiles, cudaStream_t stream) {
+  constexpr size_t smem = smem3d<S, PHYS, TY, TZ>();
+  cudaFuncSetAttribute(stage3d_kernel<S, LIM, PHYS, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  stage3d_kernel<S, LIM, PHYS, TY, TZ><<<ntiles, threads3d<TY, TZ>(), smem, stream>>>(args);
+}
+
+template <typename S, int LIM>
+int launch_limiter3d(const StageArgs<S>& args, int ntiles, bool phys, int shape, cudaStream_t stream) {
+  using T = Tile3D<S>;
+  if (shape == 0) {
+    if (phys)
+      launch_shape3d<S, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+    else
+      launch_shape3d<S, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+    return kOk;
+  }
+  if (phys) {
+    set_error("stage3d: the non-ideal terms run on the default %dx%d tiles", T::TY, T::TZ);
+    return kBadArgument;
+  }
+  launch_shape3d<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream);
+  return kOk;
+}
+
 template <typename S>
-int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, cudaStream_t stream) {
-  constexpr int TY = Tile3D<S>::TY, TZ = Tile3D<S>::TZ;
-  constexpr int NR = (TY + 4) * (TZ + 4), G = (TY + 1) * (TZ + 1);
+int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, int ty, int tz, cudaStream_t stream) {
   if (ntiles <= 0) return kOk;
   if (args.lx <= 0) {
     set_error("stage3d: lx must be positive");
     return kBadArgument;
   }
+  int shape = -1;
+  for (int i = 0; i < Tile3D<S>::kShapes; ++i)
+    if (Tile3D<S>::kShape[i][0] == ty && Tile3D<S>::kShape[i][1] == tz) shape = i;
+  if (shape < 0) {
+    set_error("stage3d: no %dx%d tile shape", ty, tz);
+    return kBadArgument;
+  }
   const bool phys = args.eta != 0.0 || args.gravity[0] != 0.0 || args.gravity[1] != 0.0 || args.gravity[2] != 0.0;
-  const size_t smem =
-      sizeof(S) * (2 * 8 * NR + (phys ? 3 : 2) * 3 * NR + 4 * 3 * G + 3 * 2 * 7 * G + 3 * G);
+  int status;
   switch (limiter) {
-#define WB_CASE(L)                                                                                              \
-  case L:                                                                                                       \
-    if (phys) {                                                                                                 \
-      cudaFuncSetAttribute(stage3d_kernel<S, L, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-      stage3d_kernel<S, L, true><<<ntiles, 288, smem, stream>>>(args);                                        \
-    } else {                                                                                                    \
-      cudaFuncSetAttribute(stage3d_kernel<S, L, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)); \
-      stage3d_kernel<S, L, false><<<ntiles, 288, smem, stream>>>(args);                                       \
-    }                                                                                                           \
-    break;
-    WB_CASE(0)
-    WB_CASE(1)
-    WB_CASE(2)
-    WB_CASE(3)
-#undef WB_CASE
+    case 0: status = launch_limiter3d<S, 0>(args, ntiles, phys, shape, stream); break;
+    case 1: status = launch_limiter3d<S, 1>(args, ntiles, phys, shape, stream); break;
+    case 2: status = launch_limiter3d<S, 2>(args, ntiles, phys, shape, stream); break;
+    case 3: status = launch_limiter3d<S, 3>(args, ntiles, phys, shape, stream); break;
     default:
       set_error("limiter code %d is not one of 0..3", limiter);
       return kBadArgument;
   }
+  if (status != kOk) return status;
   return check_launch("stage3d");
 }
 
-template int launch_stage3d<float>(const StageArgs<float>&, int, int, cudaStream_t);
-template int launch_stage3d<double>(const StageArgs<double>&, int, int, cudaStream_t);
+template int launch_stage3d<float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
+template int launch_stage3d<double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+
+int tile_shapes_3d(int fp64, int* shapes, int max) {
+  const int count = fp64 ? Tile3D<double>::kShapes : Tile3D<float>::kShapes;
+  for (int i = 0; i < count && i < max; ++i) {
+    shapes[2 * i] = fp64 ? Tile3D<double>::kShape[i][0] : Tile3D<float>::kShape[i][0];
+    shapes[2 * i + 1] = fp64 ? Tile3D<double>::kShape[i][1] : Tile3D<float>::kShape[i][1];
+  }
+  return count;
+}
 
 void tile_shape_3d(int fp64, int* ty, int* tz) {
   *ty = fp64 ? Tile3D<double>::TY : Tile3D<float>::TY;

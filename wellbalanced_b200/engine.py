@@ -179,14 +179,17 @@ class Engine:
                       self.gamma, b[0], b[1], self.limiter, tx, ty, self.bad.data_ptr(),
                       None if bflux is None else bflux.data_ptr(), s)
         elif self.physics is not None:
+            if tuple(self.layout.tile_shape) != tuple(self.layout.default_tile):
+                raise ValueError("the non-ideal 3D stage kernel runs on the default tile shape")
             _lib.call("wb_stage3d_physics", self.precision, src.data_ptr(),
                       None if base is None else base.data_ptr(), dst.data_ptr(), self.patches.data_ptr(),
                       self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(), self.gamma, b[0], b[1], b[2],
                       self.limiter, self.layout.lx, *self.physics, self.bad.data_ptr(), s)
         else:
-            _lib.call("wb_stage3d", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
+            ty, tz = self.layout.tile_shape
+            _lib.call("wb_stage3d_tiled", self.precision, src.data_ptr(), None if base is None else base.data_ptr(),
                       dst.data_ptr(), self.patches.data_ptr(), self.tiles.data_ptr(), self.ntiles, self.dt.data_ptr(),
-                      self.gamma, b[0], b[1], b[2], self.limiter, self.layout.lx, self.bad.data_ptr(),
+                      self.gamma, b[0], b[1], b[2], self.limiter, self.layout.lx, ty, tz, self.bad.data_ptr(),
                       None if bflux is None else bflux.data_ptr(), s)
         if timing:
             end.record(torch.cuda.current_stream(self.device) if self.stream is None else self.stream)

@@ -314,19 +314,19 @@ class Layout:
         _lib.call("wb_tile_shape", self.ndim, self.precision, ctypes.addressof(a), ctypes.addressof(b))
         self.tile_shape = (a.value, b.value)
         self.default_tile = self.tile_shape
-        if self.ndim == 2 and getattr(self, "tile", None) is not None:
-            if self.tile not in _lib.tile_shapes_2d(self.precision):
-                raise ValueError(f"no {self.tile} tile shape; built: {_lib.tile_shapes_2d(self.precision)}")
+        if getattr(self, "tile", None) is not None:
+            if self.tile not in _lib.tile_shapes(self.ndim, self.precision):
+                raise ValueError(f"no {self.tile} tile shape; built: {_lib.tile_shapes(self.ndim, self.precision)}")
             self.tile_shape = self.tile
         del lib
         self._cut_tiles()
 
     def set_tile(self, tile):
-        """Cut the 2D stage kernel's work list into `tile` = (tx, ty) tiles (one of the
-        shapes `_lib.tile_shapes_2d` lists)."""
+        """Cut the stage kernel's work list into `tile` tiles: (tx, ty) in 2D, (ty, tz)
+        columns in 3D (one of the shapes `_lib.tile_shapes` lists)."""
         tile = tuple(int(v) for v in tile)
-        if self.ndim != 2 or tile not in _lib.tile_shapes_2d(self.precision):
-            raise ValueError(f"no 2D tile shape {tile} for float{self.precision}")
+        if tile not in _lib.tile_shapes(self.ndim, self.precision):
+            raise ValueError(f"no {self.ndim}D tile shape {tile} for float{self.precision}")
         self.tile = self.tile_shape = tile
         self._cut_tiles()
 
