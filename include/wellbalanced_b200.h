@@ -160,7 +160,8 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
                    int advance, void* stream);
 
 /* Halo and restriction op lists (struct CopyOp / InterpOp / RestrictOp), replacing
- * patchwork's exchange_halos and restrict (carafe/mhd.py:744-777, 981, 991). */
+ * patchwork's exchange_halos and restrict (carafe/mhd.py:744-777, 981, 991). An op covers
+ * fewer than 2^31 points of fields 0..7, and never writes a point it reads. */
 int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_interp_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);

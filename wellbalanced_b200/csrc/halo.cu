@@ -30,20 +30,31 @@ __global__ void __launch_bounds__(256) copy_ops_kernel(S* __restrict__ pool, con
   const PatchDesc D = patches[op.dst];
   const PatchDesc A = patches[op.src1];
   const PatchDesc B = patches[op.src2 >= 0 ? op.src2 : op.src1];
-  const int64_t count = int64_t(op.n[0]) * op.n[1] * op.n[2];
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int p2 = int(t % op.n[2]);
-    const int p1 = int((t / op.n[2]) % op.n[1]);
-    const int p0 = int(t / (int64_t(op.n[1]) * op.n[2]));
+  // 32-bit point index (the host keeps every op below 2^31 points)
+  const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
+  const unsigned count = unsigned(op.n[0]) * n1 * n2;
+  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
+    const unsigned line = t / n2;
+    const int p2 = int(t - line * n2);
+    const int p1 = int(line % n1);
+    const int p0 = int(line / n1);
     const int64_t od = offset_of(D, op.d[0] + p0, op.d[1] + p1, op.d[2] + p2);
     const int64_t o1 = offset_of(A, op.s1[0] + op.m1[0] * p0, op.s1[1] + op.m1[1] * p1, op.s1[2] + op.m1[2] * p2);
     const int64_t o2 = offset_of(B, op.s2[0] + op.m2[0] * p0, op.s2[1] + op.m2[1] * p1, op.s2[2] + op.m2[2] * p2);
-    for (int f = op.field_lo; f < op.field_hi; ++f) {
-      S v = S(op.w1) * pool[A.off + f * A.fstride + o1];
-      if (op.w2 != 0.0) v += S(op.w2) * pool[B.off + f * B.fstride + o2];
-      if (f == op.negate) v = -v;
-      pool[D.off + f * D.fstride + od] = v;
+    // every field's value first, then the stores: the loads of a point are in flight
+    // together (an op never writes a point it reads)
+    S v[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) {
+      if (f >= op.field_lo && f < op.field_hi) {
+        S x = S(op.w1) * pool[A.off + f * A.fstride + o1];
+        if (op.w2 != 0.0) x += S(op.w2) * pool[B.off + f * B.fstride + o2];
+        v[f] = f == op.negate ? -x : x;
+      }
     }
+#pragma unroll
+    for (int f = 0; f < 8; ++f)
+      if (f >= op.field_lo && f < op.field_hi) pool[D.off + f * D.fstride + od] = v[f];
   }
 }
 
@@ -86,11 +97,14 @@ __global__ void __launch_bounds__(256) interp_ops_kernel(S* __restrict__ pool, c
   const InterpOp op = ops[blockIdx.x];
   const PatchDesc F = patches[op.fine];
   const PatchDesc C = patches[op.coarse];
-  const int64_t count = int64_t(op.n[0]) * op.n[1] * op.n[2];
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int q2 = int(t % op.n[2]);
-    const int q1 = int((t / op.n[2]) % op.n[1]);
-    const int q0 = int(t / (int64_t(op.n[1]) * op.n[2]));
+  // 32-bit point index (the host keeps every op below 2^31 points)
+  const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
+  const unsigned count = unsigned(op.n[0]) * n1 * n2;
+  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
+    const unsigned line = t / n2;
+    const int q2 = int(t - line * n2);
+    const int q1 = int(line % n1);
+    const int q0 = int(line / n1);
     const int fi[3] = {op.d[0] + q0, op.d[1] + q1, op.d[2] + q2};  // fine haloed indices
     int c0[3], cnt[3];
     S w[3][4];
@@ -125,11 +139,14 @@ __global__ void __launch_bounds__(256) restrict_ops_kernel(S* __restrict__ pool,
   const RestrictOp op = ops[blockIdx.x];
   const PatchDesc F = patches[op.fine];
   const PatchDesc C = patches[op.coarse];
-  const int64_t count = int64_t(op.n[0]) * op.n[1] * op.n[2];
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int q2 = int(t % op.n[2]);
-    const int q1 = int((t / op.n[2]) % op.n[1]);
-    const int q0 = int(t / (int64_t(op.n[1]) * op.n[2]));
+  // 32-bit point index (the host keeps every op below 2^31 points)
+  const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
+  const unsigned count = unsigned(op.n[0]) * n1 * n2;
+  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
+    const unsigned line = t / n2;
+    const int q2 = int(t - line * n2);
+    const int q1 = int(line % n1);
+    const int q0 = int(line / n1);
     const int ci[3] = {op.c[0] + q0, op.c[1] + q1, op.c[2] + q2};  // coarse haloed
     const int fi[3] = {op.f[0] + 2 * q0, op.f[1] + 2 * q1, op.f[2] + 2 * q2};  // fine haloed start
     int cnt[3];

@@ -10,6 +10,7 @@ namespace wb {
 
 // dst[d + p] = w1 * src1[s1 + m1 * p] + w2 * src2[s2 + m2 * p], p over the box n,
 // fields [field_lo, field_hi), field `negate` negated. Indices are haloed patch indices.
+// (every op: fewer than 2^31 points, fields within 0..7, no point both read and written)
 struct CopyOp {
   int32_t dst, src1, src2;
   int32_t field_lo, field_hi, negate;

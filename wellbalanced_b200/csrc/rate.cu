@@ -37,13 +37,14 @@ __global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool,
   const S dx = S(P.dx[0]), dy = S(P.dx[1]);
   const S idx = M::inv(dx), idy = M::inv(dy);
   const S g = S(gamma), bx0 = S(b0x), by0 = S(b0y);
-  double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+  S largest = S(0), smallest = S(INFINITY);  // converted once, exactly (as in 3D)
   // work-list indices are 32-bit (chunk_start is int): 32-bit index arithmetic
   const unsigned total = unsigned(nx) * unsigned(ny);
   const unsigned start = unsigned(chunk_start[blockIdx.x]);
+#pragma unroll 2
   for (int s = 0; s < 8; ++s) {
     const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
-    if (t >= total) break;
+    if (t >= total) continue;
     const unsigned row = t / unsigned(ny);
     const int i = int(row) + kHalo, j = int(t - row * unsigned(ny)) + kHalo;
     const int64_t c = int64_t(i) * pitch + j;
@@ -57,10 +58,10 @@ __global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool,
     const S p = (g - S(1)) * (src[4 * fs + c] - S(0.5) * r * (u * u + v * v + w * w) - S(0.5) * (bx * bx + by * by + bz * bz));
     const S rate = M::div(rabs(u) + fast_speed(r, p, bx, by, bz, g), dx, idx) +
                    M::div(rabs(v) + fast_speed(r, p, by, bx, bz, g), dy, idy);
-    largest = fmax(largest, double(rate));
-    smallest = fmin(smallest, double(r));
+    largest = rmax(largest, rate);
+    smallest = rmin(smallest, r);
   }
-  block_reduce_keys(largest, smallest, keys + 2 * P.instance);
+  block_reduce_keys(double(largest), double(smallest), keys + 2 * P.instance);
 }
 
 template <typename S>
@@ -77,13 +78,16 @@ __global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool,
   const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
   const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
   const S g = S(gamma);
-  double largest = 0.0, smallest = __longlong_as_double(0x7ff0000000000000ll);
+  // the max / min in the state's type (exact: the max of the float rates converts to the
+  // max of their double images), converted once for the block reduction
+  S largest = S(0), smallest = S(INFINITY);
   // work-list indices are 32-bit (chunk_start is int): 32-bit index arithmetic
   const unsigned total = unsigned(nx) * unsigned(ny) * unsigned(nz);
   const unsigned start = unsigned(chunk_start[blockIdx.x]);
+#pragma unroll 2
   for (int s = 0; s < 8; ++s) {
     const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
-    if (t >= total) break;
+    if (t >= total) continue;
     const unsigned line = t / unsigned(nz);
     const unsigned plane = line / unsigned(ny);
     const int i = int(plane) + kHalo;
@@ -107,10 +111,10 @@ __global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool,
     const S rate = M::div(rabs(u) + fast_speed(r, p, bx, by, bz, g), dx, idx) +
                    M::div(rabs(v) + fast_speed(r, p, by, bz, bx, g), dy, idy) +
                    M::div(rabs(w) + fast_speed(r, p, bz, bx, by, g), dz, idz);
-    largest = fmax(largest, double(rate));
-    smallest = fmin(smallest, double(r));
+    largest = rmax(largest, rate);
+    smallest = rmin(smallest, r);
   }
-  block_reduce_keys(largest, smallest, keys + 2 * P.instance);
+  block_reduce_keys(double(largest), double(smallest), keys + 2 * P.instance);
 }
 
 // The work list of the rate kernels is derived from the patch table on the host and

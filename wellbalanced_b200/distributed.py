@@ -259,6 +259,8 @@ class RankLayout:
                         continue
                     lo, hi = plans[peer][key][src]
                     row, start, shift, n = dense_row(src, lo, hi)
+                    if n[0] * n[1] * n[2] >= 2**31:  # the copy kernel indexes an op's points in 32 bits
+                        raise ValueError(f"a mailbox box of {n} points")
                     row["off"] = start  # the pack op writes box index 0.. here
                     rows.append(row)
                     first = start if first is None else first

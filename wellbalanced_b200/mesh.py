@@ -800,6 +800,14 @@ class Layout:
         (one CUDA block runs one op, so large halo slabs need many)."""
         if not ops:
             return np.zeros(0, dtype)
+        for o in ops:
+            if dtype in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
+                rec = np.asarray(o).reshape(())
+                points = int(np.prod([int(v) for v in rec["n"]]))
+                if points >= 2**31:  # the op kernels index an op's points in 32 bits
+                    raise ValueError(f"an op of {points} points; the kernels take below 2**31")
+                if not 0 <= int(rec["field_lo"]) <= int(rec["field_hi"]) <= 8:  # the copy kernel holds 8 fields
+                    raise ValueError("op fields outside 0..7")
         if dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
             return np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
         out = []
