@@ -6,7 +6,7 @@
 //   * one x-face column (j, k) of the L-shaped set the tile needs — its thread keeps
 //     the four cell planes of the x-stencil of that column in registers;
 //   * one y-face and one z-face of the current plane;
-//   * (the first 256) one cell column and the three edges at its lower corner.
+//   * (the first TY TZ) one cell column and the three edges at its lower corner.
 // Per plane p the kernel
 //   A: loads cell plane p+1 (conserved cells; face fields as the curl of the edge
 //      potential, carafe/mhd3d.py:361-386), forms the primitive variables (pressure in
