@@ -104,19 +104,54 @@ def _copy_mesh(mesh):
     return out
 
 
+#: set by main() when the workload's state fits in L2: a buffer larger than L2 that is
+#: rewritten before every timed step, outside its CUDA events
+L2_FLUSH = None
+
+
+def _flush_buffer(engine, device_index):
+    """A device buffer of twice the L2 size when both state pools fit in L2, else None."""
+    import torch
+
+    l2 = getattr(torch.cuda.get_device_properties(device_index), "L2_cache_size", 126 * 2**20) or 126 * 2**20
+    pools = 2 * engine.state.numel() * engine.state.element_size()
+    if pools >= l2:
+        return None
+    return torch.empty(2 * l2 // 4, dtype=torch.float32, device=engine.state.device)
+
+
+def _device_seconds(step, steps, flush=None):
+    """Device seconds of `steps` calls of `step` (CUDA events); with `flush`, the L2 is
+    overwritten before every call, outside the events, and the per-call times summed."""
+    import torch
+
+    if flush is None:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        for _ in range(steps):
+            step()
+        end.record()
+        torch.cuda.synchronize()
+        return start.elapsed_time(end) / 1e3
+    pairs = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        step()
+        end.record()
+        pairs.append((start, end))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in pairs) / 1e3
+
+
 def _time_steps(step, steps):
     """Device seconds of `steps` calls of `step` after one warm-up call (CUDA events)."""
     import torch
 
     step()
     torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    for _ in range(steps):
-        step()
-    end.record()
-    torch.cuda.synchronize()
-    return start.elapsed_time(end) / 1e3
+    return _device_seconds(step, steps, L2_FLUSH)
 
 
 def _rel_l1(ref, low, patches, steps):
@@ -592,6 +627,8 @@ def main():
 
     work = WORKLOADS[args.workload](args, rank)
     eng = work.engine
+    global L2_FLUSH
+    L2_FLUSH = _flush_buffer(eng, local)
     work.advance(args.warmup)
     torch.cuda.synchronize()
 
@@ -603,15 +640,13 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.3)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record()
-    work.advance(args.steps)
-    end.record()
-    torch.cuda.synchronize()
+    if L2_FLUSH is None:
+        seconds = _device_seconds(lambda: work.advance(args.steps), 1)
+    else:
+        seconds = _device_seconds(lambda: work.advance(1), args.steps, L2_FLUSH)
     barrier()
     clock_info = clocks.stop()
     launches = eng.launches - launches0
-    seconds = start.elapsed_time(end) / 1e3
     stage_ms = [s.elapsed_time(e) for s, e in eng.stage_events]
     eng.stage_events = None
     if int(eng.bad.item()):
@@ -636,16 +671,15 @@ def main():
         e2e_steps = max(3, min(args.steps, 20))
         barrier()
         torch.cuda.synchronize()
-        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s2.record()
-        for _ in range(e2e_steps):
+
+        def round_trip():
             pool.copy_(host, non_blocking=True)
             work.advance(1)
             host.copy_(pool, non_blocking=True)
-        e2.record()
-        torch.cuda.synchronize()
+
+        e2e_seconds = _device_seconds(round_trip, e2e_steps, L2_FLUSH)
         barrier()
-        t2 = torch.tensor([s2.elapsed_time(e2) / 1e3], dtype=torch.float64, device="cuda")
+        t2 = torch.tensor([e2e_seconds], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(t2, op=dist.ReduceOp.MAX)
         nbytes = host.numel() * host.element_size()
@@ -667,8 +701,13 @@ def main():
         achieved = per_launch / launch_s / 1e9
         config = work.config()
         config["parallelism"] = f"replicas x{world}"
-        config["l2"] = "inputs larger than L2 (state pool {:.2f} GB per copy)".format(
-            eng.state.numel() * eng.state.element_size() / 1e9)
+        pool_gb = eng.state.numel() * eng.state.element_size() / 1e9
+        if L2_FLUSH is None:
+            config["l2"] = "inputs larger than L2 (state pool {:.2f} GB per copy)".format(pool_gb)
+        else:
+            config["l2"] = ("L2 flushed before every timed step, outside its CUDA events (a {:.0f} MB write; "
+                            "state pool {:.3f} GB per copy, smaller than L2)").format(
+                L2_FLUSH.numel() * 4 / 1e6, pool_gb)
         line = {
             "metric": METRIC,
             "value": value,
