@@ -548,3 +548,24 @@ def test_every_3d_tile_shape_gives_the_same_steps():
                 m.step()
             tol = 1e-5 if precision == 32 else 1e-12
             assert torch.allclose(m.engine.state, reference.engine.state, rtol=tol, atol=tol * 0.1), (precision, tile)
+
+
+def test_saved_state_resumes_bitwise():
+    """`save` / `load` of the device pool: steps after a reload repeat the steps after the
+    save, bit for bit (2D float32, 3D float64)."""
+    from wellbalanced_b200.mhd import MHD2D
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    for model in (MHD2D.orszag_tang(32, precision=32, limiter="mc"),
+                  MHD3D.orszag_tang(16, precision=64, limiter="mc")):
+        for _ in range(3):
+            model.step()
+        saved, time, steps = model.save(), model.time, model.steps
+        dts = [model.step() for _ in range(4)]
+        after = model.engine.state.clone()
+        model.load(saved)
+        model.time, model.steps = time, steps
+        model.engine.time.fill_(time)
+        again = [model.step() for _ in range(4)]
+        assert again == dts
+        assert torch.equal(model.engine.state, after)

@@ -358,11 +358,13 @@ class MHD3D:
 
     # raw device state (checkpoint / host buffers) ------------------------------------------------
     def save(self, host=None):
-        """Copy the device state pool into ``host`` (a pinned CPU tensor, allocated if None)."""
+        """Copy the device state pool into ``host`` (a pinned CPU tensor, allocated if None);
+        returns it once the copy has landed."""
         pool = self.engine.state
         if host is None:
             host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
         host.copy_(pool, non_blocking=True)
+        torch.cuda.current_stream(pool.device).synchronize()
         return host
 
     def load(self, host) -> None:
