@@ -569,3 +569,23 @@ def test_saved_state_resumes_bitwise():
         again = [model.step() for _ in range(4)]
         assert again == dts
         assert torch.equal(model.engine.state, after)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_alfven_wave_converges_at_second_order(precision):
+    """The reference's convergence tests (tests/unit/test_mhd.py:78-86,
+    tests/unit/test_mhd3d.py:13-21): the circularly polarised Alfven wave after one period
+    at 8 and 16 cells, unlimited slopes; the error of B_y falls by 2^1.85 (2D) / 2^1.8
+    (3D), div B stays at round-off. float32 runs the same bound."""
+    from wellbalanced_b200.mhd import MHD2D
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    for cls, order in ((MHD2D, 1.85), (MHD3D, 1.8)):
+        errors = []
+        for cells in (8, 16):
+            model, exact = cls.alfven_wave(cells, limiter="none", precision=precision)
+            model.run(model.period)
+            by = model.dataset()["magnetic_field_y"].values
+            errors.append(float(np.mean(np.abs(by - exact["magnetic_field_y"].values))))
+            assert model.divergence() < (1e-14 if precision == 64 else 1e-6), cls.__name__
+        assert np.log2(errors[0] / errors[1]) > order, (cls.__name__, errors)
