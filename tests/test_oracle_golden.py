@@ -162,3 +162,42 @@ def test_3d_turbulence_matches_the_reference(runs3d):
     dts = [model.step() for _ in range(4)]
     np.testing.assert_allclose(dts, runs3d["turb16_dts"], rtol=1e-13)
     _close3(model, runs3d, "turb16", 1e-12)
+
+
+def test_oracle_refined_non_ideal_runs_conserve():
+    """The oracle's flux register on refined hierarchies with the non-ideal terms (the
+    reference records its fluxes after adding them): resistive + conductive 2D and
+    resistive 3D runs keep their composite totals to round-off (the checker the device's
+    refined non-ideal tests compare with)."""
+    from oracle.mesh import Hierarchy
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+    from oracle.mhd3d import MHD3D as OracleMHD3D
+
+    h = Hierarchy((16, 8), ((-1.0, 1.0), (-0.5, 0.5)), (True, True))
+    h.add_patch(1, ((8, 24), (4, 12)))
+    model = OracleMHD2D(h, limiter="minmod", resistivity=2e-3, conduction=(2e-2, 1e-3), mean_field=(0.1, 0.05))
+    model.set_state(lambda x, y: 1.0 + 0.5 * np.exp(-((x + 0.3) ** 2 + y**2) / 0.02), (2.0, 1.0, 0.3),
+                    lambda x, y: 1.0 + 0.2 * np.cos(np.pi * x),
+                    vector_potential=lambda x, y: 0.1 * np.maximum(0.3 - np.hypot(x, y), 0.0),
+                    bz=lambda x, y: 0.1 * np.sin(np.pi * x))
+    before = model.totals()
+    for _ in range(5):
+        model.step()
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-13 * max(1.0, abs(before[name])), name
+
+    k = 2.0 * np.pi
+    h3 = Hierarchy((8, 8, 8), ((0.0, 1.0),) * 3, (True,) * 3)
+    h3.add_patch(1, ((4, 12), (4, 12), (2, 10)))
+    model = OracleMHD3D(h3, resistivity=0.01, limiter="minmod")
+    model.set_state(lambda x, y, z: 1.0 + 0.2 * np.sin(k * (x + y)),
+                    (lambda x, y, z: 0.3 * np.sin(k * y), 0.0, lambda x, y, z: 0.3 * np.sin(k * x)), 1.0,
+                    vector_potential=(lambda x, y, z: 0.1 * np.cos(k * z), lambda x, y, z: 0.1 * np.cos(k * x),
+                                      lambda x, y, z: 0.1 * np.cos(k * y)))
+    before = model.totals()
+    for _ in range(3):
+        model.step()
+    after = model.totals()
+    for name in before:
+        assert abs(after[name] - before[name]) < 1e-13 * max(1.0, abs(before[name])), name
