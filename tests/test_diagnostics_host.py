@@ -63,3 +63,20 @@ def test_sheet_diagnostics_through_a_refined_patch():
     out = _check(h, 4)
     uniform = _check(AMRHierarchy((64, 128), ((-1.0, 1.0), (-2.0, 2.0)), periodic=(True, False)), 4)
     assert out["leaf_cells"] == uniform["leaf_cells"] - 30 * 8 + 60 * 16
+
+
+def test_dataset_variables_combine_element_wise():
+    """`dataset()` variables combine like xarray's aligned variables (``ds.pressure /
+    ds.density`` is the temperature)."""
+    from wellbalanced_b200.dataset import Dataset, Variable
+
+    p = Variable(("x", "y"), np.array([[2.0, 4.0], [6.0, 8.0]]))
+    rho = Variable(("x", "y"), np.array([[1.0, 2.0], [3.0, 4.0]]))
+    ds = Dataset({"pressure": p, "density": rho})
+    t = ds.pressure / ds.density
+    assert isinstance(t, Variable) and t.dims == ("x", "y")
+    np.testing.assert_array_equal(t.values, 2.0)
+    np.testing.assert_array_equal((1.0 - t).values, -1.0)
+    np.testing.assert_array_equal((0.5 * p + rho).values, 2 * rho.values)
+    np.testing.assert_array_equal(abs(-rho).values, rho.values)
+    assert float((p - rho).max()) == 4.0

@@ -3,7 +3,8 @@
 The reference returns an ``xarray.Dataset`` (``carafe/datasets.py:25-30``); xarray is
 not a dependency here, so this mirrors the part of its interface the reference's tests
 and examples use: ``ds["name"].values``, ``ds.name``, ``ds.data_vars``, ``ds.attrs``,
-coordinates ``ds.x.values``, ``.min()`` / ``.max()`` and ``long_name`` attributes.
+coordinates ``ds.x.values``, ``.min()`` / ``.max()``, element-wise arithmetic of
+variables and ``long_name`` attributes.
 """
 
 from __future__ import annotations
@@ -31,8 +32,40 @@ class Variable:
     def __array__(self, dtype=None, copy=None):
         return np.asarray(self.values, dtype=dtype)
 
+    # element-wise arithmetic with numbers, arrays and variables of the same dims, as
+    # xarray does for aligned variables (``ds.pressure / ds.density``)
+    def _apply(self, other, op):
+        return Variable(self.dims, op(self.values, np.asarray(other)))
+
+    def __add__(self, other):
+        return self._apply(other, np.add)
+
+    def __radd__(self, other):
+        return self._apply(other, lambda a, b: b + a)
+
     def __sub__(self, other):
-        return Variable(self.dims, self.values - np.asarray(other))
+        return self._apply(other, np.subtract)
+
+    def __rsub__(self, other):
+        return self._apply(other, lambda a, b: b - a)
+
+    def __mul__(self, other):
+        return self._apply(other, np.multiply)
+
+    def __rmul__(self, other):
+        return self._apply(other, lambda a, b: b * a)
+
+    def __truediv__(self, other):
+        return self._apply(other, np.true_divide)
+
+    def __rtruediv__(self, other):
+        return self._apply(other, lambda a, b: b / a)
+
+    def __neg__(self):
+        return Variable(self.dims, -self.values)
+
+    def __abs__(self):
+        return Variable(self.dims, np.abs(self.values))
 
     def __repr__(self):
         return f"Variable(dims={self.dims}, shape={self.values.shape})"
