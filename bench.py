@@ -597,19 +597,48 @@ def peaks():
 PROFILES = {"turbulence": "stage3d_turbulence.md", "batch": "stage2d_batch.md", "harris": "stage2d_harris.md"}
 
 
-def profile_traffic(workload, cells):
-    """DRAM bytes per stage launch from the committed ncu summary of the workload (its
-    per-cell figure times this run's cells), or None."""
+def profile_figure(workload, key):
+    """A per-cell figure (`key: value` line) of the committed ncu summary of the workload,
+    or None."""
     path = ROOT / "profiles" / PROFILES[workload]
     if not path.exists():
         return None
     for line in path.read_text().splitlines():
-        if line.strip().startswith("traffic_bytes_per_cell_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
-                return float(line.split(":", 1)[1].split()[0]) * cells
+                return float(line.split(":", 1)[1].split()[0])
             except ValueError:
                 return None
     return None
+
+
+def profile_traffic(workload, cells):
+    """DRAM bytes per stage launch from the committed ncu summary of the workload (its
+    per-cell figure times this run's cells), or None."""
+    per_cell = profile_figure(workload, "traffic_bytes_per_cell_launch")
+    return None if per_cell is None else per_cell * cells
+
+
+def issue_roofline(workload, cells, launch_s, clock_info):
+    """The stage kernel against its instruction-issue ceiling: the warp instructions of one
+    launch (the ncu summary's per-cell count times this run's cells) over the live launch
+    time, against one warp instruction per cycle on each of the four schedulers of every SM
+    at the SM clock sampled during the timed region (else the maximum clock)."""
+    import torch
+
+    per_cell = profile_figure(workload, "warp_instructions_per_cell_launch")
+    if per_cell is None or not launch_s > 0:
+        return None
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = None
+    if clock_info:
+        mhz = clock_info.get("sm_mhz") or clock_info.get("sm_max_mhz")
+    if not mhz:
+        return None
+    achieved = per_cell * cells / launch_s
+    peak = 4.0 * sms * mhz * 1e6
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "warp_instructions_per_cell_launch": per_cell, "sm_mhz": mhz, "sms": sms}
 
 
 def main():
@@ -756,6 +785,7 @@ def main():
                 "algorithmic_bytes_per_launch": per_launch,
                 "mean_launch_ms": 1e3 * launch_s,
                 "peak_kind": peak_kind,
+                "issue": issue_roofline(args.workload, cells, launch_s, clock_info),
             },
             "gpu_launches": launches,
             "clocks": clock_info,

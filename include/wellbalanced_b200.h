@@ -161,7 +161,9 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
 
 /* Halo and restriction op lists (struct CopyOp / InterpOp / RestrictOp), replacing
  * patchwork's exchange_halos and restrict (carafe/mhd.py:744-777, 981, 991). An op covers
- * fewer than 2^31 points of fields 0..7, and never writes a point it reads. */
+ * fewer than 2^31 points of fields 0..7, and never writes a point it reads. One 64-thread
+ * block runs one op: lists of small ops (64 points or fewer) run in one wave, and large
+ * boxes are best cut into ops of up to ~1024 points (wellbalanced_b200.mesh.size_ops). */
 int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_interp_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);

@@ -11,6 +11,14 @@
 //   cell-centred axes, coincident-or-4-point-midpoint along node axes.
 // * Restriction ops set coarse values under fine patches: the mean of the fine values
 //   along cell-centred axes, the coincident fine value along node axes.
+//
+// One block of 64 threads runs one op, its threads over the op's points: 32 such blocks
+// are resident per SM, so a level's many small halo ops (tens of points each) run in one
+// wave. The host cuts boxes into ops sized for the list (rows along the contiguous axis
+// first): one point per thread where the list is small, up to 1024 points per op where
+// it fills the GPU many times over. A thread issues every load of its point (all fields,
+// all interpolation weights) before any store: the stores go through the same pool
+// pointer, so loads placed after a store would wait for it.
 #include "layout.cuh"
 #include "halo.cuh"
 #include "wb_internal.cuh"
@@ -23,9 +31,11 @@ __device__ __forceinline__ int64_t offset_of(const PatchDesc& P, int i, int j, i
   return int64_t(i) * P.pitch0 + j;
 }
 
+constexpr int kOpThreads = 64;  // threads of the block that runs one op
+
 template <typename S>
-__global__ void __launch_bounds__(256) copy_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                                      const CopyOp* __restrict__ ops) {
+__global__ void __launch_bounds__(kOpThreads) copy_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                                             const CopyOp* __restrict__ ops) {
   const CopyOp op = ops[blockIdx.x];
   const PatchDesc D = patches[op.dst];
   const PatchDesc A = patches[op.src1];
@@ -33,7 +43,7 @@ __global__ void __launch_bounds__(256) copy_ops_kernel(S* __restrict__ pool, con
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
+  for (unsigned t = threadIdx.x; t < count; t += kOpThreads) {
     const unsigned line = t / n2;
     const int p2 = int(t - line * n2);
     const int p1 = int(line % n1);
@@ -41,8 +51,7 @@ __global__ void __launch_bounds__(256) copy_ops_kernel(S* __restrict__ pool, con
     const int64_t od = offset_of(D, op.d[0] + p0, op.d[1] + p1, op.d[2] + p2);
     const int64_t o1 = offset_of(A, op.s1[0] + op.m1[0] * p0, op.s1[1] + op.m1[1] * p1, op.s1[2] + op.m1[2] * p2);
     const int64_t o2 = offset_of(B, op.s2[0] + op.m2[0] * p0, op.s2[1] + op.m2[1] * p1, op.s2[2] + op.m2[2] * p2);
-    // every field's value first, then the stores: the loads of a point are in flight
-    // together (an op never writes a point it reads)
+    // every field's value first, then the stores (an op never writes a point it reads)
     S v[8];
 #pragma unroll
     for (int f = 0; f < 8; ++f) {
@@ -91,93 +100,135 @@ __device__ __forceinline__ void axis_weights(int node_axis, int g, int& c0, int&
   }
 }
 
+// One fine point of an interpolation op: the weights of every axis, then the loads of
+// all fields over all weights (fields innermost; each field's terms in the order a0, a1,
+// a2), then the stores.
+template <typename S, int NDIM>
+__device__ __forceinline__ void interp_point(S* __restrict__ pool, const PatchDesc& F, const PatchDesc& C,
+                                             const InterpOp& op, unsigned t, unsigned n1, unsigned n2) {
+  const unsigned line = t / n2;
+  const int q2 = int(t - line * n2);
+  const int q1 = int(line % n1);
+  const int q0 = int(line / n1);
+  const int fi[3] = {op.d[0] + q0, op.d[1] + q1, op.d[2] + q2};  // fine haloed indices
+  int c0[3], cnt[3];
+  S w[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (a >= NDIM) {
+      c0[a] = 0;
+      cnt[a] = 1;
+      w[a][0] = S(1);
+      continue;
+    }
+    const int g = fi[a] - kHalo + op.fine_lo[a];  // fine level index
+    axis_weights<S>((op.node_mask >> a) & 1, g, c0[a], cnt[a], w[a]);
+    c0[a] = c0[a] - op.coarse_lo[a] + kHalo;  // coarse haloed index
+  }
+  const int lo = op.field_lo, hi = op.field_hi;
+  S acc[8];
+#pragma unroll
+  for (int f = 0; f < 8; ++f) acc[f] = S(0);
+  constexpr int K2 = NDIM == 3 ? 4 : 1;
+#pragma unroll
+  for (int a0 = 0; a0 < 4; ++a0)
+#pragma unroll
+    for (int a1 = 0; a1 < 4; ++a1)
+#pragma unroll
+      for (int a2 = 0; a2 < K2; ++a2) {
+        if (a0 < cnt[0] && a1 < cnt[1] && a2 < cnt[2]) {
+          const S wt = w[0][a0] * w[1][a1] * w[2][a2];
+          const S* cf = pool + C.off + offset_of(C, c0[0] + a0, c0[1] + a1, NDIM == 3 ? c0[2] + a2 : 0);
+#pragma unroll
+          for (int f = 0; f < 8; ++f)
+            if (f >= lo && f < hi) acc[f] += wt * cf[f * C.fstride];
+        }
+      }
+  S* out = pool + F.off + offset_of(F, fi[0], fi[1], NDIM == 3 ? fi[2] : 0);
+#pragma unroll
+  for (int f = 0; f < 8; ++f)
+    if (f >= lo && f < hi) out[f * F.fstride] = acc[f];
+}
+
 template <typename S>
-__global__ void __launch_bounds__(256) interp_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                                        const InterpOp* __restrict__ ops) {
+__global__ void __launch_bounds__(kOpThreads) interp_ops_kernel(S* __restrict__ pool,
+                                                               const PatchDesc* __restrict__ patches,
+                                                               const InterpOp* __restrict__ ops) {
   const InterpOp op = ops[blockIdx.x];
   const PatchDesc F = patches[op.fine];
   const PatchDesc C = patches[op.coarse];
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
-    const unsigned line = t / n2;
-    const int q2 = int(t - line * n2);
-    const int q1 = int(line % n1);
-    const int q0 = int(line / n1);
-    const int fi[3] = {op.d[0] + q0, op.d[1] + q1, op.d[2] + q2};  // fine haloed indices
-    int c0[3], cnt[3];
-    S w[3][4];
-    for (int a = 0; a < 3; ++a) {
-      if (a >= op.ndim) {
-        c0[a] = 0;
-        cnt[a] = 1;
-        w[a][0] = S(1);
-        continue;
-      }
-      const int g = fi[a] - kHalo + op.fine_lo[a];  // fine level index
-      axis_weights<S>((op.node_mask >> a) & 1, g, c0[a], cnt[a], w[a]);
-      c0[a] = c0[a] - op.coarse_lo[a] + kHalo;  // coarse haloed index
-    }
-    const int64_t od = offset_of(F, fi[0], fi[1], op.ndim == 3 ? fi[2] : 0);
-    for (int f = op.field_lo; f < op.field_hi; ++f) {
-      const S* cf = pool + C.off + f * C.fstride;
-      S acc = S(0);
-      for (int a0 = 0; a0 < cnt[0]; ++a0)
-        for (int a1 = 0; a1 < cnt[1]; ++a1)
-          for (int a2 = 0; a2 < cnt[2]; ++a2)
-            acc += w[0][a0] * w[1][a1] * w[2][a2] *
-                   cf[offset_of(C, c0[0] + a0, c0[1] + a1, op.ndim == 3 ? c0[2] + a2 : 0)];
-      pool[F.off + f * F.fstride + od] = acc;
-    }
+  for (unsigned t = threadIdx.x; t < count; t += kOpThreads) {
+    if (op.ndim == 3)
+      interp_point<S, 3>(pool, F, C, op, t, n1, n2);
+    else
+      interp_point<S, 2>(pool, F, C, op, t, n1, n2);
   }
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) restrict_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                                          const RestrictOp* __restrict__ ops) {
+__global__ void __launch_bounds__(kOpThreads) restrict_ops_kernel(S* __restrict__ pool,
+                                                                 const PatchDesc* __restrict__ patches,
+                                                                 const RestrictOp* __restrict__ ops) {
   const RestrictOp op = ops[blockIdx.x];
   const PatchDesc F = patches[op.fine];
   const PatchDesc C = patches[op.coarse];
+  int cnt[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) cnt[a] = (a < op.ndim && !((op.node_mask >> a) & 1)) ? 2 : 1;
+  const int total = cnt[0] * cnt[1] * cnt[2];
+  const S scale = S(1) / S(total);
+  const int lo = op.field_lo, hi = op.field_hi;
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += blockDim.x) {
+  for (unsigned t = threadIdx.x; t < count; t += kOpThreads) {
     const unsigned line = t / n2;
     const int q2 = int(t - line * n2);
     const int q1 = int(line % n1);
     const int q0 = int(line / n1);
     const int ci[3] = {op.c[0] + q0, op.c[1] + q1, op.c[2] + q2};  // coarse haloed
     const int fi[3] = {op.f[0] + 2 * q0, op.f[1] + 2 * q1, op.f[2] + 2 * q2};  // fine haloed start
-    int cnt[3];
-    for (int a = 0; a < 3; ++a) cnt[a] = (a < op.ndim && !((op.node_mask >> a) & 1)) ? 2 : 1;
-    const S scale = S(1) / S(cnt[0] * cnt[1] * cnt[2]);
-    const int64_t oc = offset_of(C, ci[0], ci[1], op.ndim == 3 ? ci[2] : 0);
-    for (int f = op.field_lo; f < op.field_hi; ++f) {
-      const S* ff = pool + F.off + f * F.fstride;
-      S acc = S(0);
-      for (int a0 = 0; a0 < cnt[0]; ++a0)
-        for (int a1 = 0; a1 < cnt[1]; ++a1)
-          for (int a2 = 0; a2 < cnt[2]; ++a2)
-            acc += ff[offset_of(F, fi[0] + a0, fi[1] + a1, op.ndim == 3 ? fi[2] + a2 : 0)];
-      pool[C.off + f * C.fstride + oc] = cnt[0] * cnt[1] * cnt[2] == 1 ? acc : acc * scale;
-    }
+    // every fine value of every field first (fields innermost; each field's terms in the
+    // order a0, a1, a2), then the stores
+    S acc[8];
+#pragma unroll
+    for (int f = 0; f < 8; ++f) acc[f] = S(0);
+#pragma unroll
+    for (int a0 = 0; a0 < 2; ++a0)
+#pragma unroll
+      for (int a1 = 0; a1 < 2; ++a1)
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+          if (a0 < cnt[0] && a1 < cnt[1] && a2 < cnt[2]) {
+            const S* ff = pool + F.off + offset_of(F, fi[0] + a0, fi[1] + a1, op.ndim == 3 ? fi[2] + a2 : 0);
+#pragma unroll
+            for (int f = 0; f < 8; ++f)
+              if (f >= lo && f < hi) acc[f] += ff[f * F.fstride];
+          }
+        }
+    S* out = pool + C.off + offset_of(C, ci[0], ci[1], op.ndim == 3 ? ci[2] : 0);
+#pragma unroll
+    for (int f = 0; f < 8; ++f)
+      if (f >= lo && f < hi) out[f * C.fstride] = total == 1 ? acc[f] : acc[f] * scale;
   }
 }
 
 template <typename S>
 int launch_copy_ops(S* pool, const PatchDesc* patches, const CopyOp* ops, int nops, cudaStream_t stream) {
-  if (nops > 0) copy_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops);
+  if (nops > 0) copy_ops_kernel<S><<<nops, kOpThreads, 0, stream>>>(pool, patches, ops);
   return check_launch("halo copy");
 }
 template <typename S>
 int launch_interp_ops(S* pool, const PatchDesc* patches, const InterpOp* ops, int nops, cudaStream_t stream) {
-  if (nops > 0) interp_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops);
+  if (nops > 0) interp_ops_kernel<S><<<nops, kOpThreads, 0, stream>>>(pool, patches, ops);
   return check_launch("halo interpolation");
 }
 template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream) {
-  if (nops > 0) restrict_ops_kernel<S><<<nops, 256, 0, stream>>>(pool, patches, ops);
+  if (nops > 0) restrict_ops_kernel<S><<<nops, kOpThreads, 0, stream>>>(pool, patches, ops);
   return check_launch("restrict");
 }
 template int launch_copy_ops<float>(float*, const PatchDesc*, const CopyOp*, int, cudaStream_t);

@@ -258,39 +258,61 @@ __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, 
   for (int t = 0; t < ncons; ++t) out[t] = double(F[rows[t]]);
 }
 
-// One thread per coarse face of an interface: reg[slot] += mean of the fine faces over
-// it - the coarse face (each op holds both sides, so no two threads share a slot).
+// One block per interface side: reg[slot] += mean of the fine faces over each coarse
+// face - the coarse face (each op holds both sides, so no two blocks share a slot). The
+// coarse face and its 2 (2D) or 4 (3D) fine faces are evaluated by separate threads
+// (kFluxThreads / K coarse faces per round), then one thread per coarse face combines
+// them from shared memory, the fine faces summed in the order (a, b).
+constexpr int kFluxThreads = 128;
+
 template <typename S, int LIM, bool PHYS>
-__global__ void face_flux_ops_kernel(const S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                     const FaceFluxOp* __restrict__ ops, double b0x, double b0y, double b0z,
-                                     double gamma, FacePhysics phys, double* __restrict__ reg) {
+__global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __restrict__ pool,
+                                                                     const PatchDesc* __restrict__ patches,
+                                                                     const FaceFluxOp* __restrict__ ops, double b0x,
+                                                                     double b0y, double b0z, double gamma,
+                                                                     FacePhysics phys, double* __restrict__ reg) {
+  __shared__ double g[kFluxThreads][6];
   const FaceFluxOp op = ops[blockIdx.x];
   const PatchDesc C = patches[op.coarse];
   const PatchDesc F = patches[op.fine];
   const double b0[3] = {b0x, b0y, b0z};
   const int ncons = op.ndim == 2 ? 6 : 5;
-  const int fine_a = 2, fine_b = op.ndim == 3 ? 2 : 1;
-  for (int s = threadIdx.x; s < op.len; s += blockDim.x) {
-    const int s1 = s / op.width, s2 = s % op.width;
-    int idx[3] = {0, 0, 0};
-    idx[op.axis] = op.coarse_plane;
-    idx[op.t1] = op.coarse_t0[0] + s1;
-    if (op.ndim == 3) idx[op.t2] = op.coarse_t0[1] + s2;
-    double coarse[6];
-    face_flux<S, LIM, PHYS>(pool + C.off, C, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, phys, coarse);
-    double fine[6] = {0, 0, 0, 0, 0, 0};
-    for (int a = 0; a < fine_a; ++a)
-      for (int b = 0; b < fine_b; ++b) {
-        int f[3] = {0, 0, 0};
-        f[op.axis] = op.fine_plane;
-        f[op.t1] = op.fine_t0[0] + 2 * s1 + a;
-        if (op.ndim == 3) f[op.t2] = op.fine_t0[1] + 2 * s2 + b;
-        double g[6];
-        face_flux<S, LIM, PHYS>(pool + F.off, F, op.ndim, op.axis, f[0], f[1], f[2], b0, gamma, phys, g);
-        for (int q = 0; q < ncons; ++q) fine[q] += g[q];
+  const int fine_b = op.ndim == 3 ? 2 : 1;
+  const int K = 1 + 2 * fine_b;        // evaluations per coarse face
+  const int per = kFluxThreads / K;    // coarse faces per round
+  const int t = threadIdx.x;
+  const int e = t % K;
+  for (int s0 = 0; s0 < op.len; s0 += per) {
+    const int s = s0 + t / K;
+    if (t < per * K && s < op.len) {
+      const int s1 = s / op.width, s2 = s % op.width;
+      int idx[3] = {0, 0, 0};
+      double out[6] = {0, 0, 0, 0, 0, 0};
+      if (e == 0) {
+        idx[op.axis] = op.coarse_plane;
+        idx[op.t1] = op.coarse_t0[0] + s1;
+        if (op.ndim == 3) idx[op.t2] = op.coarse_t0[1] + s2;
+        face_flux<S, LIM, PHYS>(pool + C.off, C, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, phys, out);
+      } else {
+        const int a = (e - 1) / fine_b, b = (e - 1) % fine_b;
+        idx[op.axis] = op.fine_plane;
+        idx[op.t1] = op.fine_t0[0] + 2 * s1 + a;
+        if (op.ndim == 3) idx[op.t2] = op.fine_t0[1] + 2 * s2 + b;
+        face_flux<S, LIM, PHYS>(pool + F.off, F, op.ndim, op.axis, idx[0], idx[1], idx[2], b0, gamma, phys, out);
       }
-    const double count = double(fine_a * fine_b);
-    for (int q = 0; q < ncons; ++q) reg[op.reg_off + int64_t(q) * op.len + s] += fine[q] / count - coarse[q];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) g[t][q] = out[q];
+    }
+    __syncthreads();
+    if (t < per && s0 + t < op.len) {
+      const int s = s0 + t;
+      double fine[6] = {0, 0, 0, 0, 0, 0};
+      for (int k = 1; k < K; ++k)
+        for (int q = 0; q < ncons; ++q) fine[q] += g[t * K + k][q];
+      const double count = double(K - 1);
+      for (int q = 0; q < ncons; ++q) reg[op.reg_off + int64_t(q) * op.len + s] += fine[q] / count - g[t * K][q];
+    }
+    __syncthreads();
   }
 }
 
@@ -324,10 +346,10 @@ void launch_face_flux_kernel(const S* pool, const PatchDesc* patches, const Face
                              const double* b0, double gamma, int limiter, const FacePhysics& phys, double* reg,
                              cudaStream_t stream) {
   switch (limiter) {
-    case 0: face_flux_ops_kernel<S, 0, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    case 1: face_flux_ops_kernel<S, 1, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    case 2: face_flux_ops_kernel<S, 2, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    default: face_flux_ops_kernel<S, 3, PHYS><<<nops, 128, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 0: face_flux_ops_kernel<S, 0, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 1: face_flux_ops_kernel<S, 1, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 2: face_flux_ops_kernel<S, 2, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    default: face_flux_ops_kernel<S, 3, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
   }
 }
 

@@ -36,7 +36,7 @@ import torch
 
 from wellbalanced_b200 import _lib
 from wellbalanced_b200.engine import Engine, _device_bytes
-from wellbalanced_b200.mesh import _concat
+from wellbalanced_b200.mesh import _concat, size_ops, split_box_ops
 
 #: patch-row flag of a dense block that stands for a box of a patch (kProxy in layout.cuh)
 PROXY = 1 << 30
@@ -287,7 +287,7 @@ class RankLayout:
                     first = start if first is None else first
                 if first is not None:
                     rd.recv[peer] = (first, offset - first)
-            rd.pack_ops = _concat(rd.pack_ops, _lib.COPY_OP)
+            rd.pack_ops = split_box_ops(_concat(rd.pack_ops, _lib.COPY_OP))
             self.rounds[key] = rd
 
         def index(key, g):
@@ -435,10 +435,10 @@ class DistributedEngine(Engine):
     def __init__(self, rank_layout, transport, **options):
         super().__init__(None, layout=rank_layout, **options)
         self.transport = transport
-        self.rounds = {
-            key: (_device_bytes(rd.pack_ops, self.device, _lib.COPY_OP), int(rd.pack_ops.size), rd.send, rd.recv)
-            for key, rd in rank_layout.rounds.items()
-        }
+        self.rounds = {}
+        for key, rd in rank_layout.rounds.items():
+            ops = size_ops(rd.pack_ops) if rd.pack_ops.size else rd.pack_ops
+            self.rounds[key] = (_device_bytes(ops, self.device, _lib.COPY_OP), int(ops.size), rd.send, rd.recv)
 
     def pack(self, pool, key):
         """Copy this rank's boxes of round `key` into their mailboxes."""

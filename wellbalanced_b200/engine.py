@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from wellbalanced_b200 import _lib
-from wellbalanced_b200.mesh import Layout
+from wellbalanced_b200.mesh import Layout, _concat, size_ops
 
 _DTYPES = {32: torch.float32, 64: torch.float64}
 
@@ -78,16 +78,26 @@ class Engine:
         self.chunk_start = torch.from_numpy(L.chunk_start).to(self.device)
         self.nchunks = int(L.chunk_patch.size)
         self.inv_dx2_sum = torch.from_numpy(L.inv_dx2_sum).to(self.device)
+        # op lists on the device, each cut for the op kernels by its size (`size_ops`)
+        def upload(ops, dtype):
+            ops = size_ops(ops) if np.asarray(ops).size else np.zeros(0, dtype)
+            return _device_bytes(ops, self.device, dtype), int(ops.size)
+
         self.copy_phases = [
-            (_device_bytes(same, self.device, _lib.COPY_OP), same.size,
-             [(_device_bytes(b, self.device, _lib.COPY_OP), b.size) for b in bnd])
-            for same, bnd in L.copy_phases
+            (*upload(same, _lib.COPY_OP), [upload(b, _lib.COPY_OP) for b in bnd]) for same, bnd in L.copy_phases
         ]
-        self.interp_levels = [(_device_bytes(ops, self.device, _lib.INTERP_OP), ops.size) for ops in L.interp_levels]
+        self.interp_levels = [upload(ops, _lib.INTERP_OP) for ops in L.interp_levels]
         self.restrict_levels = {
-            level: {g: (_device_bytes(ops, self.device, _lib.RESTRICT_OP), ops.size) for g, ops in groups.items()}
+            level: {g: upload(ops, _lib.RESTRICT_OP) for g, ops in groups.items()}
             for level, groups in L.restrict_levels.items()
         }
+        # the ops of every field group of a level in one list: the groups write different
+        # fields of the coarse level and read only the fine one, so one launch runs them all
+        self.restrict_merged = {}
+        for level, groups in L.restrict_levels.items():
+            if len(groups) > 1:
+                ops = _concat(list(groups.values()), _lib.RESTRICT_OP)
+                self.restrict_merged[level] = (frozenset(groups), *upload(ops, _lib.RESTRICT_OP))
         n = L.ninstances
         self.ninstances = n
         self.dt = torch.zeros(n, dtype=torch.float64, device=self.device)
@@ -146,6 +156,14 @@ class Engine:
     def restrict(self, pool, groups):
         """Coarse values under finer patches from the fine ones (finest level first)."""
         for level in range(self.layout.max_level, 0, -1):
+            merged = self.restrict_merged.get(level)
+            if merged is not None and merged[0] == frozenset(groups):
+                ops, nops = merged[1], merged[2]
+                if nops:
+                    _lib.call("wb_restrict_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                              ops.data_ptr(), nops, self._s())
+                    self.launches += 1
+                continue
             for g in groups:
                 self._restrict_level(pool, level, g)
 

@@ -166,6 +166,79 @@ def _boxes_intersect(a, b):
     return tuple(out)
 
 
+#: largest op the host builds (points); `size_ops` cuts a list further when it is small
+OP_MAX_POINTS = 1024
+#: op blocks resident on a B200 at once (148 SMs x 32 blocks of 64 threads)
+OP_WAVE = 148 * 32
+
+
+def op_points(total):
+    """Points per op for a list of `total` points: 64 (one per thread of the op's block)
+    while the list fits one wave of blocks, else enough for one wave, up to 1024."""
+    per = -(-int(total) // OP_WAVE)
+    return int(min(OP_MAX_POINTS, max(64, -(-per // 64) * 64)))
+
+
+def size_ops(ops):
+    """A copy, interpolation or restriction op list cut for the op kernels: small lists
+    (a level's halos) into ops of one point per thread, so they run in one wave of short
+    blocks; large lists (a big box's halos) into ops of up to 1024 points."""
+    ops = np.atleast_1d(np.asarray(ops))
+    if ops.size == 0:
+        return ops
+    total = int(np.prod(ops["n"].astype(np.int64), axis=1).sum())
+    return split_box_ops(ops, op_points(total))
+
+
+def _even_parts(n, size):
+    """Starts and counts of `n` cut into near-equal parts of at most `size`."""
+    parts = -(-n // size)
+    step = -(-n // parts)
+    return [(a, min(step, n - a)) for a in range(0, n, step)]
+
+
+def _box_parts(n, chunk):
+    """Sub-boxes (start, count) of a box of n points (axis 2 fastest in the kernels' point
+    order, then axis 1) of at most `chunk` points each: whole rows of the fastest axes
+    where they fit, so a warp's lanes read consecutive points along the contiguous axis."""
+    n = [int(v) for v in n]
+    if n[1] * n[2] <= chunk:
+        return [((a, 0, 0), (c, n[1], n[2])) for a, c in _even_parts(n[0], max(1, chunk // max(1, n[1] * n[2])))]
+    if n[2] <= chunk:
+        return [((a, b, 0), (1, c, n[2])) for a in range(n[0]) for b, c in _even_parts(n[1], max(1, chunk // max(1, n[2])))]
+    return [((a, b, c0), (1, 1, c)) for a in range(n[0]) for b in range(n[1]) for c0, c in _even_parts(n[2], chunk)]
+
+
+def split_box_ops(ops, chunk=OP_MAX_POINTS):
+    """Copy, interpolation or restriction ops with every box cut into ops of at most
+    `chunk` points (the same points, the same arithmetic per point)."""
+    ops = np.atleast_1d(np.asarray(ops))
+    if ops.size == 0:
+        return ops
+    dtype = ops.dtype
+    out = []
+    for o in ops:
+        n = [int(v) for v in o["n"]]
+        if n[0] * n[1] * n[2] <= chunk:
+            out.append(np.atleast_1d(o))
+            continue
+        parts = _box_parts(n, chunk)
+        block = np.repeat(np.atleast_1d(o), len(parts))
+        starts = np.array([st for st, _ in parts], dtype=np.int64)
+        block["n"] = np.array([cnt for _, cnt in parts], dtype=np.int32)
+        if "s1" in dtype.names:  # copy: d + p, s1 + m1 p, s2 + m2 p
+            block["d"] += starts.astype(np.int32)
+            block["s1"] += (block["m1"] * starts).astype(np.int32)
+            block["s2"] += (block["m2"] * starts).astype(np.int32)
+        elif "fine_lo" in dtype.names:  # interpolation: fine box d + p
+            block["d"] += starts.astype(np.int32)
+        else:  # restriction: coarse start c, fine start f (2 fine per coarse)
+            block["c"] += starts.astype(np.int32)
+            block["f"] += (2 * starts).astype(np.int32)
+        out.append(block)
+    return np.concatenate(out).astype(dtype)
+
+
 def _concat(arrays, dtype):
     """Records of ``arrays`` in one array of the C layout ``dtype`` (``np.concatenate``
     alone may repack a padded structured dtype)."""
@@ -795,9 +868,9 @@ class Layout:
         return (self._pack(face_ops, _lib.FACE_FLUX_OP), [self._pack(ops, _lib.REFLUX_OP) for ops in phases], offset)
 
     @staticmethod
-    def _pack(ops, dtype, chunk=4096):
-        """Op array; ops larger than `chunk` points are split along their longest axis
-        (one CUDA block runs one op, so large halo slabs need many)."""
+    def _pack(ops, dtype, chunk=OP_MAX_POINTS):
+        """Op array; halo, interpolation and restriction boxes are cut into ops of at most
+        `chunk` points (default `OP_MAX_POINTS`; the engine cuts small lists further)."""
         if not ops:
             return np.zeros(0, dtype)
         for o in ops:
@@ -808,30 +881,7 @@ class Layout:
                     raise ValueError(f"an op of {points} points; the kernels take below 2**31")
                 if not 0 <= int(rec["field_lo"]) <= int(rec["field_hi"]) <= 8:  # the copy kernel holds 8 fields
                     raise ValueError("op fields outside 0..7")
+        packed = np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
         if dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
-            return np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
-        out = []
-        for o in ops:
-            o = np.asarray(o).reshape(())
-            n = [int(v) for v in o["n"]]
-            total = n[0] * n[1] * n[2]
-            if total <= chunk or dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
-                out.append(o)
-                continue
-            axis = int(np.argmax(n))
-            rows = max(1, chunk // max(1, total // n[axis]))
-            for start in range(0, n[axis], rows):
-                part = o.copy()
-                count = min(rows, n[axis] - start)
-                part["n"][axis] = count
-                if dtype == _lib.COPY_OP:
-                    part["d"][axis] += start
-                    part["s1"][axis] += part["m1"][axis] * start
-                    part["s2"][axis] += part["m2"][axis] * start
-                elif dtype == _lib.INTERP_OP:
-                    part["d"][axis] += start
-                else:  # restriction: coarse start c, fine start f (2 fine per coarse)
-                    part["c"][axis] += start
-                    part["f"][axis] += 2 * start
-                out.append(part)
-        return np.array(out, dtype=dtype)
+            return packed
+        return split_box_ops(packed, chunk)
