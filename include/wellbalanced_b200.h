@@ -167,6 +167,12 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
 int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_interp_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
+/* wb_interp_ops and wb_copy_ops of one level in a single launch. Valid only when no op of
+ * the two lists writes a point another op of them writes or reads: the interpolation ops
+ * cover just the halo points no same-level copy fills (wellbalanced_b200.mesh.Layout builds
+ * them so), and the copies read only their sources' computed points. */
+int wb_fill_ops(int precision, void* pool, const void* patches, const void* interp, int ninterp, const void* copies,
+                int ncopies, void* stream);
 
 /* Refluxing, replacing patchwork's FluxRegister (carafe/mhd.py:906-919, 989-990): after
  * a stage, reg += (mean of the fine faces - the coarse face) of every coarse-fine

@@ -58,6 +58,7 @@ SIGNATURES = {
     "wb_copy_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_interp_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_fill_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_int, c_dp],
     "wb_face_flux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp, c_dp],
     "wb_face_flux_ops_physics": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int,
                                  c_double, c_double, c_double, c_dp, c_dp],

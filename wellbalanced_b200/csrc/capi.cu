@@ -375,6 +375,21 @@ int wb_interp_ops(int precision, void* pool, const void* patches, const void* op
                                    static_cast<const InterpOp*>(ops), nops, as_stream(stream));
 }
 
+int wb_fill_ops(int precision, void* pool, const void* patches, const void* interp, int ninterp, const void* copies,
+                int ncopies, void* stream) {
+  set_error("");
+  if (!precision_ok(precision, "fill_ops") || !ptrs_ok({pool, patches}, "fill_ops") || (ninterp > 0 && !interp) ||
+      (ncopies > 0 && !copies) || ninterp < 0 || ncopies < 0)
+    return kBadArgument;
+  if (precision == 32)
+    return launch_fill_ops<float>(static_cast<float*>(pool), static_cast<const PatchDesc*>(patches),
+                                  static_cast<const InterpOp*>(interp), ninterp, static_cast<const CopyOp*>(copies),
+                                  ncopies, as_stream(stream));
+  return launch_fill_ops<double>(static_cast<double*>(pool), static_cast<const PatchDesc*>(patches),
+                                 static_cast<const InterpOp*>(interp), ninterp, static_cast<const CopyOp*>(copies),
+                                 ncopies, as_stream(stream));
+}
+
 int wb_restrict_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream) {
   set_error("");
   if (!precision_ok(precision, "restrict_ops") || !ptrs_ok({pool, patches}, "restrict_ops") || (nops > 0 && !ops))

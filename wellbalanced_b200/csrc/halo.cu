@@ -33,10 +33,9 @@ __device__ __forceinline__ int64_t offset_of(const PatchDesc& P, int i, int j, i
 
 constexpr int kOpThreads = 64;  // threads of the block that runs one op
 
+// The points of one copy op, over the threads of the block.
 template <typename S>
-__global__ void __launch_bounds__(kOpThreads) copy_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
-                                                             const CopyOp* __restrict__ ops) {
-  const CopyOp op = ops[blockIdx.x];
+__device__ __forceinline__ void copy_op(S* __restrict__ pool, const PatchDesc* __restrict__ patches, const CopyOp& op) {
   const PatchDesc D = patches[op.dst];
   const PatchDesc A = patches[op.src1];
   const PatchDesc B = patches[op.src2 >= 0 ? op.src2 : op.src1];
@@ -65,6 +64,12 @@ __global__ void __launch_bounds__(kOpThreads) copy_ops_kernel(S* __restrict__ po
     for (int f = 0; f < 8; ++f)
       if (f >= op.field_lo && f < op.field_hi) pool[D.off + f * D.fstride + od] = v[f];
   }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kOpThreads) copy_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                                             const CopyOp* __restrict__ ops) {
+  copy_op(pool, patches, ops[blockIdx.x]);
 }
 
 // Fine halo points from the coarse patch below. Fine haloed index f along an axis
@@ -150,11 +155,10 @@ __device__ __forceinline__ void interp_point(S* __restrict__ pool, const PatchDe
     if (f >= lo && f < hi) out[f * F.fstride] = acc[f];
 }
 
+// The points of one interpolation op, over the threads of the block.
 template <typename S>
-__global__ void __launch_bounds__(kOpThreads) interp_ops_kernel(S* __restrict__ pool,
-                                                               const PatchDesc* __restrict__ patches,
-                                                               const InterpOp* __restrict__ ops) {
-  const InterpOp op = ops[blockIdx.x];
+__device__ __forceinline__ void interp_op(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                          const InterpOp& op) {
   const PatchDesc F = patches[op.fine];
   const PatchDesc C = patches[op.coarse];
   // 32-bit point index (the host keeps every op below 2^31 points)
@@ -166,6 +170,27 @@ __global__ void __launch_bounds__(kOpThreads) interp_ops_kernel(S* __restrict__ 
     else
       interp_point<S, 2>(pool, F, C, op, t, n1, n2);
   }
+}
+
+template <typename S>
+__global__ void __launch_bounds__(kOpThreads) interp_ops_kernel(S* __restrict__ pool,
+                                                               const PatchDesc* __restrict__ patches,
+                                                               const InterpOp* __restrict__ ops) {
+  interp_op(pool, patches, ops[blockIdx.x]);
+}
+
+// A level's interpolation and same-level copy ops in one launch (blocks [0, ninterp) the
+// interpolation ops, the rest the copies): valid when no op of either list writes a point
+// that another op of the launch writes or reads, as for interpolation ops trimmed to the
+// halo points no sibling covers (the copies read only their sources' computed points).
+template <typename S>
+__global__ void __launch_bounds__(kOpThreads) fill_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                                             const InterpOp* __restrict__ interp, int ninterp,
+                                                             const CopyOp* __restrict__ copies) {
+  if (int(blockIdx.x) < ninterp)
+    interp_op(pool, patches, interp[blockIdx.x]);
+  else
+    copy_op(pool, patches, copies[blockIdx.x - ninterp]);
 }
 
 template <typename S>
@@ -227,6 +252,14 @@ int launch_interp_ops(S* pool, const PatchDesc* patches, const InterpOp* ops, in
   return check_launch("halo interpolation");
 }
 template <typename S>
+int launch_fill_ops(S* pool, const PatchDesc* patches, const InterpOp* interp, int ninterp, const CopyOp* copies,
+                    int ncopies, cudaStream_t stream) {
+  if (ninterp + ncopies > 0)
+    fill_ops_kernel<S><<<ninterp + ncopies, kOpThreads, 0, stream>>>(pool, patches, interp, ninterp, copies);
+  return check_launch("halo fill");
+}
+
+template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream) {
   if (nops > 0) restrict_ops_kernel<S><<<nops, kOpThreads, 0, stream>>>(pool, patches, ops);
   return check_launch("restrict");
@@ -235,6 +268,9 @@ template int launch_copy_ops<float>(float*, const PatchDesc*, const CopyOp*, int
 template int launch_copy_ops<double>(double*, const PatchDesc*, const CopyOp*, int, cudaStream_t);
 template int launch_interp_ops<float>(float*, const PatchDesc*, const InterpOp*, int, cudaStream_t);
 template int launch_interp_ops<double>(double*, const PatchDesc*, const InterpOp*, int, cudaStream_t);
+template int launch_fill_ops<float>(float*, const PatchDesc*, const InterpOp*, int, const CopyOp*, int, cudaStream_t);
+template int launch_fill_ops<double>(double*, const PatchDesc*, const InterpOp*, int, const CopyOp*, int,
+                                     cudaStream_t);
 template int launch_restrict_ops<float>(float*, const PatchDesc*, const RestrictOp*, int, cudaStream_t);
 template int launch_restrict_ops<double>(double*, const PatchDesc*, const RestrictOp*, int, cudaStream_t);
 

@@ -73,6 +73,9 @@ int launch_copy_ops(S* pool, const PatchDesc* patches, const CopyOp* ops, int no
 template <typename S>
 int launch_interp_ops(S* pool, const PatchDesc* patches, const InterpOp* ops, int nops, cudaStream_t stream);
 template <typename S>
+int launch_fill_ops(S* pool, const PatchDesc* patches, const InterpOp* interp, int ninterp, const CopyOp* copies,
+                    int ncopies, cudaStream_t stream);
+template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream);
 template <typename S>
 int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,

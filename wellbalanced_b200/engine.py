@@ -123,6 +123,8 @@ class Engine:
         #: non-ideal terms, None for ideal MHD: 2D (eta, kappa_par, kappa_perp, gx, gy),
         #: 3D (eta, gx, gy, gz)
         self.physics = None
+        #: a level's interpolation and same-level copies in one launch (`wb_fill_ops`)
+        self.fused_fill = True
 
     # low-level launches ----------------------------------------------------------------------
     def _s(self):
@@ -142,12 +144,19 @@ class Engine:
         s = self._s()
         same, nsame, boundary = self.copy_phases[level]
         interp, ninterp = self.interp_levels[level]
-        if ninterp:
-            _lib.call("wb_interp_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp, s)
+        if ninterp and nsame and self.fused_fill:
+            # the layout's interpolation ops skip the points the copies write: one launch
+            _lib.call("wb_fill_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp,
+                      same.data_ptr(), nsame, s)
             self.launches += 1
-        if nsame:
-            _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), same.data_ptr(), nsame, s)
-            self.launches += 1
+        else:
+            if ninterp:
+                _lib.call("wb_interp_ops", prec, pool.data_ptr(), self.patches.data_ptr(), interp.data_ptr(), ninterp,
+                          s)
+                self.launches += 1
+            if nsame:
+                _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), same.data_ptr(), nsame, s)
+                self.launches += 1
         for ops, nops in boundary:
             if nops:
                 _lib.call("wb_copy_ops", prec, pool.data_ptr(), self.patches.data_ptr(), ops.data_ptr(), nops, s)

@@ -239,6 +239,94 @@ def split_box_ops(ops, chunk=OP_MAX_POINTS):
     return np.concatenate(out).astype(dtype)
 
 
+def _free_boxes(free):
+    """Boxes (start, count) covering the True points of a 3-axis boolean array exactly:
+    runs along axis 2, merged over equal runs of consecutive rows of axis 1, then of axis 0."""
+    n0, n1, _ = free.shape
+    planes = []
+    for i0 in range(n0):
+        boxes = []  # (j0, count1, k0, k1)
+        open_ = {}
+        for i1 in range(n1):
+            row = free[i0, i1]
+            runs = []
+            k = 0
+            while k < row.size:
+                if row[k]:
+                    e = k
+                    while e < row.size and row[e]:
+                        e += 1
+                    runs.append((k, e))
+                    k = e
+                else:
+                    k += 1
+            now = {}
+            for run in runs:
+                if run in open_:
+                    j0, c = open_.pop(run)
+                    now[run] = (j0, c + 1)
+                else:
+                    now[run] = (i1, 1)
+            for run, (j0, c) in open_.items():
+                boxes.append((j0, c, run[0], run[1]))
+            open_ = now
+        for run, (j0, c) in open_.items():
+            boxes.append((j0, c, run[0], run[1]))
+        planes.append(sorted(boxes))
+    out = []
+    open_ = {}
+    for i0, boxes in enumerate(planes):
+        now = {}
+        for b in boxes:
+            now[b] = (open_.pop(b)[0], i0) if b in open_ else (i0, i0)
+        for b, (a0, a1) in open_.items():
+            out.append(((a0, b[0], b[2]), (a1 - a0 + 1, b[1], b[3] - b[2])))
+        open_ = now
+    for b, (a0, a1) in open_.items():
+        out.append(((a0, b[0], b[2]), (a1 - a0 + 1, b[1], b[3] - b[2])))
+    return out
+
+
+def trim_interp_ops(interp, same):
+    """Interpolation ops of a level cut to the halo points that none of the level's
+    same-level copy ops writes (the copies overwrite those points after the
+    interpolation, so the fill's result is unchanged): a level's interpolation and copies
+    then write disjoint points and run in one launch (`wb_fill_ops`)."""
+    interp = np.atleast_1d(np.asarray(interp))
+    same = np.atleast_1d(np.asarray(same))
+    if interp.size == 0 or same.size == 0:
+        return interp
+    covers = {}
+    for op in same:
+        key = (int(op["dst"]), int(op["field_lo"]), int(op["field_hi"]))
+        covers.setdefault(key, []).append((op["d"].astype(np.int64), op["n"].astype(np.int64)))
+    out = []
+    for op in interp:
+        boxes = covers.get((int(op["fine"]), int(op["field_lo"]), int(op["field_hi"])))
+        if not boxes:
+            out.append(np.atleast_1d(op))
+            continue
+        d, n = op["d"].astype(np.int64), op["n"].astype(np.int64)
+        free = np.ones(tuple(int(v) for v in n), dtype=bool)
+        for cd, cn in boxes:
+            lo, hi = np.maximum(d, cd), np.minimum(d + n, cd + cn)
+            if np.all(lo < hi):
+                free[lo[0] - d[0]:hi[0] - d[0], lo[1] - d[1]:hi[1] - d[1], lo[2] - d[2]:hi[2] - d[2]] = False
+        if free.all():
+            out.append(np.atleast_1d(op))
+            continue
+        parts = _free_boxes(free)
+        if not parts:
+            continue
+        block = np.repeat(np.atleast_1d(op), len(parts))
+        block["d"] = (d + np.array([st for st, _ in parts], dtype=np.int64)).astype(np.int32)
+        block["n"] = np.array([cnt for _, cnt in parts], dtype=np.int32)
+        out.append(block)
+    if not out:
+        return np.zeros(0, interp.dtype)
+    return np.concatenate(out).astype(interp.dtype)
+
+
 def _concat(arrays, dtype):
     """Records of ``arrays`` in one array of the C layout ``dtype`` (``np.concatenate``
     alone may repack a padded structured dtype)."""
@@ -273,7 +361,8 @@ class Layout:
         self._tiles()
         self._chunks()
         self.copy_phases = self._copy_ops()
-        self.interp_levels = self._interp_ops()
+        self.interp_levels = [trim_interp_ops(ops, same) for ops, (same, _) in zip(self._interp_ops(), self.copy_phases,
+                                                                                    strict=True)]
         self.restrict_levels = self._restrict_ops()
         self.face_flux_ops, self.reflux_phases, self.register_size = self._reflux_ops()
 
