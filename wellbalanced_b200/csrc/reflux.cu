@@ -210,6 +210,7 @@ __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, 
   }
   S qs[4][7];
   S bn = S(0);
+#pragma unroll
   for (int st = 0; st < 4; ++st) {
     int ii = i, jj = j, kk = k;
     if (axis == 0) ii += st - 2;

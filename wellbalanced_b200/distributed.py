@@ -435,6 +435,7 @@ class DistributedEngine(Engine):
     def __init__(self, rank_layout, transport, **options):
         super().__init__(None, layout=rank_layout, **options)
         self.transport = transport
+        self.overlap_fluxes = False  # the flux round's exchange runs on the engine's stream
         self.rounds = {}
         for key, rd in rank_layout.rounds.items():
             ops = size_ops(rd.pack_ops) if rd.pack_ops.size else rd.pack_ops
@@ -468,7 +469,7 @@ class DistributedEngine(Engine):
                 self.exchange(pool, ("restrict", level, g))
                 self._restrict_level(pool, level, g)
 
-    def face_fluxes(self, pool):
+    def face_fluxes(self, pool, stream=None):
         if self.layout.max_level > 0:
             self.exchange(pool, ("flux",))
         Engine.face_fluxes(self, pool)

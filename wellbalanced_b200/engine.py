@@ -125,12 +125,17 @@ class Engine:
         self.physics = None
         #: a level's interpolation and same-level copies in one launch (`wb_fill_ops`)
         self.fused_fill = True
+        #: run stage 1's flux-register kernel on a second stream, beside the restriction
+        #: and halo fill of the stage pool (it reads U, which those do not write)
+        self.overlap_fluxes = True
+        self._flux_stream = None
 
     # low-level launches ----------------------------------------------------------------------
     def _s(self):
-        if self.stream is not None:
-            return self.stream.cuda_stream
-        return torch.cuda.current_stream(self.device).cuda_stream
+        return self._main().cuda_stream
+
+    def _main(self):
+        return self.stream if self.stream is not None else torch.cuda.current_stream(self.device)
 
     def fill(self, pool, levels=None):
         """Halos of every patch of `pool`, level by level (coarse first)."""
@@ -246,20 +251,22 @@ class Engine:
             out[index] = np.frombuffer(np.uint64(bits).tobytes(), dtype=np.float64)[0]
         return out
 
-    def face_fluxes(self, pool):
-        """Register += fine-mean minus coarse fluxes of every coarse-fine interface face."""
+    def face_fluxes(self, pool, stream=None):
+        """Register += fine-mean minus coarse fluxes of every coarse-fine interface face
+        (on `stream`, else the engine's stream)."""
         if self.nface:
+            s = stream.cuda_stream if stream is not None else self._s()
             b = self.mean_field
             if self.physics is not None:
                 eta, kappa_par, kappa_perp = self.physics[:3] if self.ndim == 2 else (self.physics[0], 0.0, 0.0)
             if self.physics is not None and (eta or kappa_par or kappa_perp):
                 _lib.call("wb_face_flux_ops_physics", self.precision, pool.data_ptr(), self.patches.data_ptr(),
                           self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter, eta,
-                          kappa_par, kappa_perp, self.register.data_ptr(), self._s())
+                          kappa_par, kappa_perp, self.register.data_ptr(), s)
             else:
                 _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
                           self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
-                          self.register.data_ptr(), self._s())
+                          self.register.data_ptr(), s)
             self.launches += 1
 
     def reflux(self, pool):
@@ -291,10 +298,20 @@ class Engine:
         U, U1 = self.state, self.stage_pool
         refined = self.layout.max_level > 0
         self.stage(U, None, U1)
-        self.face_fluxes(U)
+        side = None
+        if self.overlap_fluxes and self.nface:
+            # stage 1's register kernel beside the restriction and fill of U1 (small,
+            # latency-bound launches that leave the SMs idle), not beside the stage kernel
+            if self._flux_stream is None:
+                self._flux_stream = torch.cuda.Stream(self.device)
+            side, main = self._flux_stream, self._main()
+            side.wait_stream(main)
+        self.face_fluxes(U, side)
         if refined:
             self.restrict(U1, groups_potential)
         self.fill(U1)
+        if side is not None:
+            main.wait_stream(side)  # stage 1's fluxes have read U before stage 2 writes it
         self.stage(U1, U, U)
         self.face_fluxes(U1)
         self.reflux(U)
