@@ -386,12 +386,37 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
         }
       }
     }
+    // the global values phase C reads (the conserved values of the column's cell in plane
+    // p - 1 and the potentials of its edges in plane p, with their Heun base values in
+    // stage 2), loaded before the barrier so that their latency overlaps the wait
+    const int gj_c = y0 + cj, gk_c = z0 + ck;
+    const bool core_c = p >= x0 && tid < NCORE;
+    const bool do_cell = core_c && p - 1 >= x0 && p - 1 < xe && gj_c < ny && gk_c < nz;
+    const bool do_ex = core_c && p < xe && gj_c < own_ny && gk_c < own_nz;
+    const bool do_ey = core_c && p < xn && gj_c < ny && gk_c < own_nz;
+    const bool do_ez = core_c && p < xn && gj_c < own_ny && gk_c < nz;
+    const int64_t o_cell = int64_t(p - 1 + kHalo) * p0 + int64_t(gj_c + kHalo) * p1 + (gk_c + kHalo);
+    const int64_t o_edge = o_cell + p0;
+    S cv[5], cb[5], ev[3], eb[3];
+#pragma unroll
+    for (int qf = 0; qf < 5; ++qf) {
+      cv[qf] = do_cell ? src[qf * fs + o_cell] : S(0);
+      cb[qf] = do_cell && base_state ? base_state[qf * fs + o_cell] : S(0);
+    }
+    {
+      const bool ok[3] = {do_ex, do_ey, do_ez};
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        ev[e] = ok[e] ? src[(5 + e) * fs + o_edge] : S(0);
+        eb[e] = ok[e] && base_state ? base_state[(5 + e) * fs + o_edge] : S(0);
+      }
+    }
     __syncthreads();
 
     // C: edges and cells ----------------------------------------------------------------
-    if (p >= x0 && tid < NCORE) {
+    if (core_c) {
       const int j = cj, k = ck;
-      const int gj = y0 + j, gk = z0 + k;
+      const int gj = gj_c, gk = gk_c;
       const int sc = (p + 6) % 3, sp = (p + 5) % 3;  // flux slots of planes p and p-1
       const S* Yc = sYZ + (sc * 2 + 0) * 7 * G;
       const S* Zc = sYZ + (sc * 2 + 1) * 7 * G;
@@ -404,8 +429,8 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
       auto gi = [&](int jj, int kk) { return (jj + 1) * GZ + (kk + 1); };
       const int I = p + kHalo, J = gj + kHalo, K = gk + kHalo;
       // cells of plane p-1
-      if (p - 1 >= x0 && p - 1 < xe && gj < ny && gk < nz) {
-        const int64_t o = int64_t(I - 1) * p0 + int64_t(J) * p1 + K;
+      if (do_cell) {
+        const int64_t o = o_cell;
         const int yrow[5] = {0, 3, 1, 2, 4};  // y-sweep rows of (rho, m_x, m_y, m_z, E)
         const int zrow[5] = {0, 2, 3, 1, 4};  // z-sweep rows
 #pragma unroll
@@ -413,50 +438,50 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
           const S div = M::div(fnow[qf] - fprev[qf], dx, idx) +
                         M::div(Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)], dy, idy) +
                         M::div(Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)], dz, idz);
-          S value = src[qf * fs + o] - dt * div;
+          S value = cv[qf] - dt * div;
           if (PHYS) {
             // gravity: rho g on the momentum, m . g on the energy, from the stage's input
             const S g0 = S(a.gravity[0]), g1 = S(a.gravity[1]), g2 = S(a.gravity[2]);
-            if (qf >= 1 && qf <= 3) value += dt * (S(a.gravity[qf - 1]) * src[o]);
-            if (qf == 4) value += dt * (src[fs + o] * g0 + src[2 * fs + o] * g1 + src[3 * fs + o] * g2);
+            if (qf >= 1 && qf <= 3) value += dt * (S(a.gravity[qf - 1]) * cv[0]);
+            if (qf == 4) value += dt * (cv[1] * g0 + cv[2] * g1 + cv[3] * g2);
           }
-          if (base_state) value = (value + base_state[qf * fs + o]) * S(0.5);
+          if (base_state) value = (value + cb[qf]) * S(0.5);
           dst[qf * fs + o] = value;
         }
       }
       // E_x on the x-edges of cell plane p: (a, b) = (y, z)
-      if (p < xe && gj < own_ny && gk < own_nz) {
+      if (do_ex) {
         S ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
                              Zc[6 * G + zi(j - 1, k)], Zc[6 * G + zi(j, k)], Zc[zi(j - 1, k)], Zc[zi(j, k)],
                              Ec[gi(j - 1, k - 1)], Ec[gi(j, k - 1)], Ec[gi(j - 1, k)], Ec[gi(j, k)]);
         if (PHYS) ex += ejx;
-        const int64_t o = 5 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
-        S value = src[o] - dt * ex;
-        if (base_state) value = (value + base_state[o]) * S(0.5);
+        const int64_t o = 5 * fs + o_edge;
+        S value = ev[0] - dt * ex;
+        if (base_state) value = (value + eb[0]) * S(0.5);
         dst[o] = value;
       }
-      if (p < xn) {
+      {
         // E_y on the y-edges of node plane p: (a, b) = (z, x)
-        if (gj < ny && gk < own_nz) {
+        if (do_ey) {
           S ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
                                sX[2 * G + gi(j, k - 1)], sX[2 * G + gi(j, k)], sX[gi(j, k - 1)], sX[gi(j, k)],
                                Ep[G + gi(j, k - 1)], Ep[G + gi(j, k)], Ec[G + gi(j, k - 1)], Ec[G + gi(j, k)]);
           if (PHYS) ey += ejy;
-          const int64_t o = 6 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
-          S value = src[o] - dt * ey;
-          if (base_state) value = (value + base_state[o]) * S(0.5);
+          const int64_t o = 6 * fs + o_edge;
+          S value = ev[1] - dt * ey;
+          if (base_state) value = (value + eb[1]) * S(0.5);
           dst[o] = value;
         }
         // E_z on the z-edges of node plane p: (a, b) = (x, y)
-        if (gj < own_ny && gk < nz) {
+        if (do_ez) {
           S ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
                                Yp[6 * G + yi(j, k)], Yc[6 * G + yi(j, k)], Yp[yi(j, k)], Yc[yi(j, k)],
                                Ep[2 * G + gi(j - 1, k)], Ec[2 * G + gi(j - 1, k)], Ep[2 * G + gi(j, k)],
                                Ec[2 * G + gi(j, k)]);
           if (PHYS) ez += ejz;
-          const int64_t o = 7 * fs + int64_t(I) * p0 + int64_t(J) * p1 + K;
-          S value = src[o] - dt * ez;
-          if (base_state) value = (value + base_state[o]) * S(0.5);
+          const int64_t o = 7 * fs + o_edge;
+          S value = ev[2] - dt * ez;
+          if (base_state) value = (value + eb[2]) * S(0.5);
           dst[o] = value;
         }
       }
