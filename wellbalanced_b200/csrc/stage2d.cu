@@ -62,8 +62,15 @@ __device__ __forceinline__ S temperature(const S* sP, int t) {
 
 // PHYS: the resistive and Braginskii-conductive face terms and gravity sources of the
 // reference (carafe/mhd.py:844-927) in the same kernel; false for ideal MHD.
+// CTAs per SM the launch bounds hold the registers to: three 256-thread CTAs of float32
+// (80 registers a thread, 63 KB of shared memory each), two of float64.
+template <typename S>
+struct Occupancy2D {
+  static constexpr int kBlocks = sizeof(S) == 4 ? 3 : 2;
+};
+
 template <typename S, int LIM, bool PHYS, int TX, int TY>
-__global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
+__global__ void __launch_bounds__(256, Occupancy2D<S>::kBlocks) stage2d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
   constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
   constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
@@ -228,13 +235,37 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
 #pragma unroll
     for (int c = 0; c < 7; ++c) out[c * NF] = F[c];
   }
-  __syncthreads();
-
-  // 3. CT-contact E_z at the nodes, A_z and the cells ---------------------------------
+  // the global values phase 3 reads (each of the thread's cells and nodes: the stage's
+  // input and, in stage 2, the Heun base), loaded before the barrier so that their
+  // latency overlaps the wait
   const S dt = S(a.dt[P.instance]);
   const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
   S* __restrict__ dst = a.dst + P.off;
-  for (int t = threadIdx.x; t < TX * TY; t += blockDim.x) {
+  constexpr int NIT = (TX * TY + 255) / 256;  // phase-3 rounds of the 256 threads
+  S in_cell[NIT][6], in_node[NIT], base_cell[NIT][6], base_node[NIT];
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int t = threadIdx.x + 256 * it;
+    const int ni = t / TY, nj = t % TY;
+    const int gx = x0 + ni, gy = y0 + nj;
+    const bool node_ok = t < TX * TY && gx < own_nx && gy < own_ny;
+    const bool cell_ok = t < TX * TY && gx < nx && gy < ny;
+    const int64_t cell = int64_t(gx + 2) * pitch + (gy + 2);
+    in_node[it] = node_ok ? src[6 * fs + cell] : S(0);
+    base_node[it] = node_ok && base_state ? base_state[6 * fs + cell] : S(0);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      in_cell[it][q] = cell_ok ? src[q * fs + cell] : S(0);
+      base_cell[it][q] = cell_ok && base_state ? base_state[q * fs + cell] : S(0);
+    }
+  }
+  __syncthreads();
+
+  // 3. CT-contact E_z at the nodes, A_z and the cells ---------------------------------
+#pragma unroll
+  for (int it = 0; it < NIT; ++it) {
+    const int t = threadIdx.x + 256 * it;
+    if (t >= TX * TY) break;
     const int ni = t / TY, nj = t % TY;
     const int gx = x0 + ni, gy = y0 + nj;  // interior node / cell indices
     if (gx < own_nx && gy < own_ny) {
@@ -247,8 +278,8 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
                         ((P.flags & kWallLo1) && gy == 0) || ((P.flags & kWallHi1) && gy == ny);
       if (wall) ez = S(0);
       const int64_t node = 6 * fs + int64_t(gx + 2) * pitch + (gy + 2);
-      S value = src[node] - dt * ez;
-      if (base_state) value = (value + base_state[node]) * S(0.5);
+      S value = in_node[it] - dt * ez;
+      if (base_state) value = (value + base_node[it]) * S(0.5);
       dst[node] = value;
     }
     if (gx < nx && gy < ny && ni < TX && nj < TY) {
@@ -259,15 +290,15 @@ __global__ void __launch_bounds__(256) stage2d_kernel(const StageArgs<S> a) {
       for (int q = 0; q < 6; ++q) {
         const S div = M::div(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1], dx, idx) +
                       M::div(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj], dy, idy);
-        S value = src[q * fs + cell] - dt * div;
+        S value = in_cell[it][q] - dt * div;
         if (PHYS) {
           // gravity: rho g on the momentum, m . g on the energy, from the stage's input
           const S gx = S(a.gravity[0]), gy = S(a.gravity[1]);
-          if (q == 1) value += dt * (src[cell] * gx);
-          if (q == 2) value += dt * (src[cell] * gy);
-          if (q == 4) value += dt * (src[fs + cell] * gx + src[2 * fs + cell] * gy);
+          if (q == 1) value += dt * (in_cell[it][0] * gx);
+          if (q == 2) value += dt * (in_cell[it][0] * gy);
+          if (q == 4) value += dt * (in_cell[it][1] * gx + in_cell[it][2] * gy);
         }
-        if (base_state) value = (value + base_state[q * fs + cell]) * S(0.5);
+        if (base_state) value = (value + base_cell[it][q]) * S(0.5);
         dst[q * fs + cell] = value;
       }
       if (a.bflux && P.bflux >= 0) {
