@@ -111,7 +111,7 @@ class Engine:
         self.reflux_ops = _device_bytes(L.reflux_ops, self.device, _lib.REFLUX_OP)
         self.nreflux = int(L.reflux_ops.size)
         counts = [int(ops.size) for ops in L.reflux_phases]
-        starts = np.cumsum([0, *counts[:-1]])
+        starts = np.cumsum([0, *counts])[: len(counts)]
         #: (first op, op count) of each reflux phase in `reflux_ops`
         self.reflux_phases = [(int(a), c) for a, c in zip(starts, counts, strict=True) if c]
         self.register = torch.zeros(max(L.register_size, 1), dtype=torch.float64, device=self.device)

@@ -885,9 +885,11 @@ class Layout:
         in the coarse patch holding that cell, the fine faces in F.
 
         A coarse cell between fine patches takes corrections from several sides, so the
-        RefluxOps come in 2 * ndim phases, one per (axis, side), applied one after the
-        other: two ops of one phase never meet in a cell (the fine patches of a level do
-        not overlap), so each phase is one race-free launch.
+        RefluxOps are grouped into phases applied one after the other, each one race-free
+        launch. Taken per (axis, side), two ops of one group never meet in a cell (the
+        fine patches of a level do not overlap); `_reflux_groups` then merges these 2 ndim
+        groups where no cell is shared, keeping the order of the corrections of every
+        cell (usually fewer launches, the same arithmetic).
         """
         h = self.h
         ncons = 6 if self.ndim == 2 else 5
@@ -954,7 +956,34 @@ class Layout:
                             rop["reg_off"] = offset
                             phases[2 * a + side].append(rop)
                             offset += ncons * length
+        phases = self._reflux_groups(phases)
         return (self._pack(face_ops, _lib.FACE_FLUX_OP), [self._pack(ops, _lib.REFLUX_OP) for ops in phases], offset)
+
+    @staticmethod
+    def _reflux_groups(phases):
+        """Reflux ops regrouped into as few race-free launches as the order of the
+        corrections allows: each op goes to the group after the last group holding an
+        earlier op (in the given order) that shares one of its coarse cells, so every cell
+        takes its corrections in the same order as before."""
+        last = {}  # coarse cell -> group of the latest op that corrected it
+        groups = []
+        for ops in phases:
+            for op in ops:
+                t1, t2 = int(op["t1"]), int(op["t2"])
+                cells = []
+                for s in range(int(op["len"])):
+                    idx = [int(v) for v in op["c"]]
+                    idx[t1] += s // int(op["width"])
+                    if t2 >= 0:
+                        idx[t2] += s % int(op["width"])
+                    cells.append((int(op["coarse"]), *idx))
+                g = 1 + max((last[c] for c in cells if c in last), default=-1)
+                while len(groups) <= g:
+                    groups.append([])
+                groups[g].append(op)
+                for c in cells:
+                    last[c] = g
+        return groups
 
     @staticmethod
     def _pack(ops, dtype, chunk=OP_MAX_POINTS):
