@@ -102,12 +102,17 @@ def load():
     return lib
 
 
+_FUNCTIONS = {}
+
+
 def call(name, *args):
     """Call a C-ABI function; raise WBError on a negative status."""
-    lib = load()
-    status = getattr(lib, name)(*args)
+    fn = _FUNCTIONS.get(name)
+    if fn is None:
+        fn = _FUNCTIONS[name] = getattr(load(), name)
+    status = fn(*args)
     if status != 0:
-        raise WBError(f"{name}: status {status}: {lib.wb_last_error().decode()}")
+        raise WBError(f"{name}: status {status}: {load().wb_last_error().decode()}")
     return status
 
 

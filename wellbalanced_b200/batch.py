@@ -125,10 +125,11 @@ class Batch:
     # stepping ------------------------------------------------------------------------------------
     def _step_launches(self):
         eng = self.engine
-        eng.rate()
-        eng.finalize_dt(self.cfl, advance=True)
         groups = eng.layout.groups
-        eng.heun_step(groups[1:], groups)
+        with eng.launching():
+            eng.rate()
+            eng.finalize_dt(self.cfl, advance=True)
+            eng.heun_step(groups[1:], groups)
 
     def capture(self):
         """Capture one step (all launches) in a CUDA graph; `advance` then replays it. The

@@ -18,6 +18,8 @@ memory and streams only; every numerical kernel is in ``libwb200.so``.
 
 from __future__ import annotations
 
+import contextlib
+
 import numpy as np
 import torch
 
@@ -129,9 +131,13 @@ class Engine:
         #: and halo fill of the stage pool (it reads U, which those do not write)
         self.overlap_fluxes = True
         self._flux_stream = None
+        #: the launching stream's handle while a step issues its launches (looked up once)
+        self._step_stream = None
 
     # low-level launches ----------------------------------------------------------------------
     def _s(self):
+        if self._step_stream is not None:
+            return self._step_stream
         return self._main().cuda_stream
 
     def _main(self):
@@ -295,6 +301,22 @@ class Engine:
 
     def heun_step(self, groups_potential, groups_all):
         """One Heun step with the dt already in self.dt (device), refluxed and restricted."""
+        with self.launching():
+            self._heun_launches(groups_potential, groups_all)
+
+    @contextlib.contextmanager
+    def launching(self):
+        """A run of launches on the engine's stream as it is now (its handle looked up once,
+        not per launch)."""
+        outer = self._step_stream
+        if outer is None:
+            self._step_stream = self._main().cuda_stream
+        try:
+            yield
+        finally:
+            self._step_stream = outer
+
+    def _heun_launches(self, groups_potential, groups_all):
         U, U1 = self.state, self.stage_pool
         refined = self.layout.max_level > 0
         self.stage(U, None, U1)

@@ -329,9 +329,10 @@ class MHD3D:
     def _one_step(self):
         """The launches of one step at the stable dt (dt, time and state on the device)."""
         eng = self.engine
-        eng.rate()
-        eng.finalize_dt(self.cfl, self.resistivity, 0.0, advance=True)
-        eng.heun_step(self._groups_potential, self._groups_all)
+        with eng.launching():
+            eng.rate()
+            eng.finalize_dt(self.cfl, self.resistivity, 0.0, advance=True)
+            eng.heun_step(self._groups_potential, self._groups_all)
 
     def capture(self) -> None:
         """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
