@@ -180,7 +180,8 @@ int wb_fill_ops(int precision, void* pool, const void* patches, const void* inte
  * step, the coarse cells beside the interfaces take U -= sign * 0.5 dt * reg / dx and reg
  * is cleared (struct RefluxOp; dt per instance on the device). The ops of one
  * wb_reflux_apply call run concurrently and must not share a coarse cell: a cell between
- * fine patches takes its corrections from separate calls (one per axis and side). */
+ * fine patches takes its corrections from separate calls (per axis and side, or grouped so
+ * that no call holds two ops of one cell, as wellbalanced_b200.mesh.Layout does). */
 int wb_face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops, double b0x,
                      double b0y, double b0z, double gamma, int limiter, double* reg, void* stream);
 /* The same register update with the non-ideal face terms of wb_stage2d_physics /
