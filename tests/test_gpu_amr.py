@@ -286,3 +286,30 @@ def test_plain_float64_paths_reflux_like_the_oracle():
         for f, name in enumerate(names):
             np.testing.assert_allclose(plain.gather(dp, f), op.field(name).local, rtol=1e-11, atol=1e-12,
                                        err_msg=f"3D level {op.level} {name}")
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fused_level_fill_and_overlapped_fluxes_equal_the_plain_sequence(dims):
+    """The single-launch level fill (`wb_fill_ops`, interpolation ops trimmed to the points
+    no copy writes) and the second stream of the flux register change no bit of a step
+    against separate interpolation and copy launches on one stream."""
+    import torch
+
+    def make():
+        return _pair(precision=32)[1] if dims == 2 else _alfven_pair(precision=32)[1]
+
+    fused, plain = make(), make()
+    plain.engine.fused_fill = False
+    plain.engine.overlap_fluxes = False
+    assert fused.engine.nface > 0
+    pool_a, pool_b = fused.engine.state.clone(), plain.engine.state.clone()
+    fused.engine.fill(pool_a)
+    plain.engine.fill(pool_b)
+    torch.cuda.synchronize()
+    assert torch.equal(pool_a, pool_b)
+    for _ in range(3):
+        fused.advance(1)
+        plain.advance(1)
+    torch.cuda.synchronize()
+    assert fused.time == plain.time
+    assert torch.equal(fused.engine.state, plain.engine.state)
