@@ -71,6 +71,8 @@ class Engine:
             hierarchy, walls=walls, precision=precision, lx=lx, instances=instances)
         L = self.layout
         self.ndim = L.ndim
+        #: finest level of the layout (the hierarchy's property walks every patch)
+        self.max_level = int(L.max_level)
         self.state = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
         self.stage_pool = torch.zeros(L.pool_size, dtype=self.dtype, device=self.device)
         self.patches = _device_bytes(L.rows, self.device, _lib.PATCH)
@@ -131,6 +133,7 @@ class Engine:
         #: and halo fill of the stage pool (it reads U, which those do not write)
         self.overlap_fluxes = True
         self._flux_stream = None
+        self._flux_events = None
         #: the launching stream's handle while a step issues its launches (looked up once)
         self._step_stream = None
 
@@ -175,9 +178,10 @@ class Engine:
 
     def restrict(self, pool, groups):
         """Coarse values under finer patches from the fine ones (finest level first)."""
-        for level in range(self.layout.max_level, 0, -1):
+        key = frozenset(groups)
+        for level in range(self.max_level, 0, -1):
             merged = self.restrict_merged.get(level)
-            if merged is not None and merged[0] == frozenset(groups):
+            if merged is not None and merged[0] == key:
                 ops, nops = merged[1], merged[2]
                 if nops:
                     _lib.call("wb_restrict_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
@@ -318,7 +322,7 @@ class Engine:
 
     def _heun_launches(self, groups_potential, groups_all):
         U, U1 = self.state, self.stage_pool
-        refined = self.layout.max_level > 0
+        refined = self.max_level > 0
         self.stage(U, None, U1)
         side = None
         if self.overlap_fluxes and self.nface:
@@ -326,14 +330,18 @@ class Engine:
             # latency-bound launches that leave the SMs idle), not beside the stage kernel
             if self._flux_stream is None:
                 self._flux_stream = torch.cuda.Stream(self.device)
+                self._flux_events = (torch.cuda.Event(), torch.cuda.Event())
             side, main = self._flux_stream, self._main()
-            side.wait_stream(main)
+            forked, joined = self._flux_events
+            forked.record(main)
+            side.wait_event(forked)
         self.face_fluxes(U, side)
         if refined:
             self.restrict(U1, groups_potential)
         self.fill(U1)
         if side is not None:
-            main.wait_stream(side)  # stage 1's fluxes have read U before stage 2 writes it
+            joined.record(side)
+            main.wait_event(joined)  # stage 1's fluxes have read U before stage 2 writes it
         self.stage(U1, U, U)
         self.face_fluxes(U1)
         self.reflux(U)
