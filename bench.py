@@ -59,6 +59,8 @@ def parse():
     parser.add_argument("--no-accuracy", action="store_true")
     parser.add_argument("--no-plain", action="store_true")
     parser.add_argument("--lx", default="auto", help="turbulence: x-planes per tile (an integer, or auto: tuned)")
+    parser.add_argument("--tile3d", default=None,
+                        help="turbulence with an integer --lx: the stage kernel's TYxTZ tile shape (default 16x16)")
     return parser.parse_args()
 
 
@@ -192,6 +194,10 @@ class Turbulence:
         lx = args.lx if args.lx == "auto" else int(args.lx)
         self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=lx)
         self.engine = self.model.engine
+        if args.tile3d and lx != "auto":
+            from wellbalanced_b200.autotune import _set_tile
+
+            _set_tile(self.engine, tuple(int(v) for v in args.tile3d.split("x")))
         self.lx = self.model.lx
         self.cells = self.n**3
 

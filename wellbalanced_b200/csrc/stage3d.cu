@@ -36,12 +36,20 @@ namespace wb {
 
 // Tile shapes (TY x TZ columns) the kernel is built for, the default first (the only one
 // with the non-ideal terms); the others are candidates of the autotuner: a 8 x 16 tile
-// needs half the shared memory, so twice the CTAs share an SM, at more halo work per cell.
+// needs half the shared memory, so twice the CTAs share an SM, at more halo work per cell;
+// a 16 x 32 tile (float32 only: 191 KB) has less halo work per cell and one CTA per SM.
 template <typename S>
 struct Tile3D {
   static constexpr int TY = 16, TZ = 16;
   static constexpr int kShapes = 2;
-  static constexpr int kShape[kShapes][2] = {{16, 16}, {8, 16}};
+  static constexpr int kShape[3][2] = {{16, 16}, {8, 16}, {16, 16}};
+};
+
+template <>
+struct Tile3D<float> {
+  static constexpr int TY = 16, TZ = 16;
+  static constexpr int kShapes = 3;
+  static constexpr int kShape[3][2] = {{16, 16}, {8, 16}, {16, 32}};
 };
 
 template <int TY, int TZ>
@@ -517,7 +525,10 @@ int launch_limiter3d(const StageArgs<S>& args, int ntiles, bool phys, int shape,
     set_error("stage3d: the non-ideal terms run on the default %dx%d tiles", T::TY, T::TZ);
     return kBadArgument;
   }
-  launch_shape3d<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream);
+  if (shape == 1)
+    launch_shape3d<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream);
+  else if constexpr (T::kShapes > 2)
+    launch_shape3d<S, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream);
   return kOk;
 }
 
