@@ -54,3 +54,8 @@ def test_bad_arguments_are_reported_without_a_device():
     status = lib.wb_stage2d(16, None, None, None, None, None, 0, None, 1.4, 0.0, 0.0, 0, None, None, None)
     assert status == -1
     assert b"precision" in lib.wb_last_error()
+    # the fused level fill: bad precision, NULL pool, a negative count
+    status = lib.wb_fill_ops(16, None, None, None, 0, None, 0, None)
+    assert status == -1 and b"precision" in lib.wb_last_error()
+    status = lib.wb_fill_ops(32, None, None, None, 1, None, 0, None)
+    assert status == -1 and b"NULL" in lib.wb_last_error()
