@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
       S* B3 = sBn + (PHYS ? face_slot<PHYS>(c) : slot) * 3 * NR;
       S* E3 = sEc + slot4 * 3 * G;
       const int I = c + kHalo;
-      for (int r = tid; r < NR; r += blockDim.x) {
+      for (int r = tid; r < NR; r += threads3d<TY, TZ>()) {
         const int j = r / RZ - 2, k = r % RZ - 2;
         const int J = y0 + j + kHalo, K = z0 + k + kHalo;
         S rho = S(1), m0 = S(0), m1 = S(0), m2 = S(0), e = S(1);
