@@ -22,9 +22,11 @@ __global__ void init_keys_n_kernel(unsigned long long* keys, int n) {
   }
 }
 
+constexpr unsigned kRateThreads = 256;  // threads of a rate block (8 rounds: 2048 cells)
+
 // 2D: one block per (patch, chunk of cells); grid.y unused.
 template <typename S>
-__global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
+__global__ void __launch_bounds__(kRateThreads) rate2d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
                                                     int npatches, const int* chunk_patch,
                                                     const int* chunk_start, double b0x, double b0y,
                                                     double gamma, unsigned long long* keys) {
@@ -43,7 +45,7 @@ __global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool,
   const unsigned start = unsigned(chunk_start[blockIdx.x]);
 #pragma unroll 2
   for (int s = 0; s < 8; ++s) {
-    const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
+    const unsigned t = start + unsigned(s) * kRateThreads + threadIdx.x;
     if (t >= total) continue;
     const unsigned row = t / unsigned(ny);
     const int i = int(row) + kHalo, j = int(t - row * unsigned(ny)) + kHalo;
@@ -65,7 +67,7 @@ __global__ void __launch_bounds__(256) rate2d_kernel(const S* __restrict__ pool,
 }
 
 template <typename S>
-__global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
+__global__ void __launch_bounds__(kRateThreads) rate3d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
                                                     int npatches, const int* chunk_patch,
                                                     const int* chunk_start, double b0x, double b0y,
                                                     double b0z, double gamma, unsigned long long* keys) {
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(256) rate3d_kernel(const S* __restrict__ pool,
   const unsigned start = unsigned(chunk_start[blockIdx.x]);
 #pragma unroll 2
   for (int s = 0; s < 8; ++s) {
-    const unsigned t = start + unsigned(s) * blockDim.x + threadIdx.x;
+    const unsigned t = start + unsigned(s) * kRateThreads + threadIdx.x;
     if (t >= total) continue;
     const unsigned line = t / unsigned(nz);
     const unsigned plane = line / unsigned(ny);
@@ -126,10 +128,10 @@ int launch_rate_chunks(const S* state, const PatchDesc* patches, int npatches, i
   init_keys_n_kernel<<<(ninstances + 255) / 256, 256, 0, stream>>>(keys, ninstances);
   if (nchunks > 0) {
     if (ndim == 2)
-      rate2d_kernel<S><<<nchunks, 256, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
+      rate2d_kernel<S><<<nchunks, kRateThreads, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
                                                     gamma, keys);
     else
-      rate3d_kernel<S><<<nchunks, 256, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
+      rate3d_kernel<S><<<nchunks, kRateThreads, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
                                                     b0[2], gamma, keys);
   }
   return check_launch("rate");

@@ -62,6 +62,8 @@ __device__ __forceinline__ S temperature(const S* sP, int t) {
 
 // PHYS: the resistive and Braginskii-conductive face terms and gravity sources of the
 // reference (carafe/mhd.py:844-927) in the same kernel; false for ideal MHD.
+constexpr int kThreads2D = 256;  // threads of a stage2d CTA
+
 // CTAs per SM the launch bounds hold the registers to: three 256-thread CTAs of float32
 // (80 registers a thread, 63 KB of shared memory each), two of float64.
 template <typename S>
@@ -70,7 +72,7 @@ struct Occupancy2D {
 };
 
 template <typename S, int LIM, bool PHYS, int TX, int TY>
-__global__ void __launch_bounds__(256, Occupancy2D<S>::kBlocks) stage2d_kernel(const StageArgs<S> a) {
+__global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_kernel(const StageArgs<S> a) {
   using M = Math<S>;
   constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
   constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
@@ -241,11 +243,11 @@ __global__ void __launch_bounds__(256, Occupancy2D<S>::kBlocks) stage2d_kernel(c
   const S dt = S(a.dt[P.instance]);
   const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
   S* __restrict__ dst = a.dst + P.off;
-  constexpr int NIT = (TX * TY + 255) / 256;  // phase-3 rounds of the 256 threads
+  constexpr int NIT = (TX * TY + kThreads2D - 1) / kThreads2D;  // phase-3 rounds of the threads
   S in_cell[NIT][6], in_node[NIT], base_cell[NIT][6], base_node[NIT];
 #pragma unroll
   for (int it = 0; it < NIT; ++it) {
-    const int t = threadIdx.x + 256 * it;
+    const int t = threadIdx.x + kThreads2D * it;
     const int ni = t / TY, nj = t % TY;
     const int gx = x0 + ni, gy = y0 + nj;
     const bool node_ok = t < TX * TY && gx < own_nx && gy < own_ny;
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(256, Occupancy2D<S>::kBlocks) stage2d_kernel(c
   // 3. CT-contact E_z at the nodes, A_z and the cells ---------------------------------
 #pragma unroll
   for (int it = 0; it < NIT; ++it) {
-    const int t = threadIdx.x + 256 * it;
+    const int t = threadIdx.x + kThreads2D * it;
     if (t >= TX * TY) break;
     const int ni = t / TY, nj = t % TY;
     const int gx = x0 + ni, gy = y0 + nj;  // interior node / cell indices
@@ -327,7 +329,7 @@ void launch_shape(const StageArgs<S>& args, int ntiles, cudaStream_t stream) {
   constexpr int NC = (TX + 4) * (TY + 4), NF = (TX + 1) * (TY + 1);
   const size_t smem = sizeof(S) * (11 * NC + 14 * NF);
   cudaFuncSetAttribute(stage2d_kernel<S, LIM, PHYS, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  stage2d_kernel<S, LIM, PHYS, TX, TY><<<ntiles, 256, smem, stream>>>(args);
+  stage2d_kernel<S, LIM, PHYS, TX, TY><<<ntiles, kThreads2D, smem, stream>>>(args);
 }
 
 // One limiter: the default shape (ideal or non-ideal) or one of the other shapes (ideal).
