@@ -66,10 +66,55 @@ __device__ __forceinline__ void copy_op(S* __restrict__ pool, const PatchDesc* _
   }
 }
 
+// The points of one copy op, two per thread and pass (the loads of both, every field,
+// before the stores; an op never writes a point it reads): for the standalone copy
+// launches, whose ops are large where the lists are (a big box's halos).
+template <typename S>
+__device__ __forceinline__ void copy_op_pairs(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
+                                              const CopyOp& op) {
+  const PatchDesc D = patches[op.dst];
+  const PatchDesc A = patches[op.src1];
+  const PatchDesc B = patches[op.src2 >= 0 ? op.src2 : op.src1];
+  // 32-bit point index (the host keeps every op below 2^31 points)
+  const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
+  const unsigned count = unsigned(op.n[0]) * n1 * n2;
+  for (unsigned t0 = threadIdx.x; t0 < count; t0 += 2 * kOpThreads) {
+    S v[2][8];
+    int64_t od[2];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const unsigned t = t0 + u * kOpThreads;
+      if (t >= count) continue;
+      const unsigned line = t / n2;
+      const int p2 = int(t - line * n2);
+      const int p1 = int(line % n1);
+      const int p0 = int(line / n1);
+      od[u] = offset_of(D, op.d[0] + p0, op.d[1] + p1, op.d[2] + p2);
+      const int64_t o1 = offset_of(A, op.s1[0] + op.m1[0] * p0, op.s1[1] + op.m1[1] * p1, op.s1[2] + op.m1[2] * p2);
+      const int64_t o2 = offset_of(B, op.s2[0] + op.m2[0] * p0, op.s2[1] + op.m2[1] * p1, op.s2[2] + op.m2[2] * p2);
+#pragma unroll
+      for (int f = 0; f < 8; ++f) {
+        if (f >= op.field_lo && f < op.field_hi) {
+          S x = S(op.w1) * pool[A.off + f * A.fstride + o1];
+          if (op.w2 != 0.0) x += S(op.w2) * pool[B.off + f * B.fstride + o2];
+          v[u][f] = f == op.negate ? -x : x;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (t0 + u * kOpThreads >= count) continue;
+#pragma unroll
+      for (int f = 0; f < 8; ++f)
+        if (f >= op.field_lo && f < op.field_hi) pool[D.off + f * D.fstride + od[u]] = v[u][f];
+    }
+  }
+}
+
 template <typename S>
 __global__ void __launch_bounds__(kOpThreads) copy_ops_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
                                                              const CopyOp* __restrict__ ops) {
-  copy_op(pool, patches, ops[blockIdx.x]);
+  copy_op_pairs(pool, patches, ops[blockIdx.x]);
 }
 
 // Fine halo points from the coarse patch below. Fine haloed index f along an axis
