@@ -58,6 +58,8 @@ def parse():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-accuracy", action="store_true")
     parser.add_argument("--no-plain", action="store_true")
+    parser.add_argument("--no-extra", action="store_true",
+                        help="turbulence at one GPU: skip the batch and Harris configurations measured beside it")
     parser.add_argument("--lx", default="auto", help="turbulence: x-planes per tile (an integer, or auto: tuned)")
     parser.add_argument("--tile3d", default=None,
                         help="turbulence with an integer --lx: the stage kernel's TYxTZ tile shape (default 16x16)")
@@ -161,6 +163,7 @@ def _rel_l1(ref, low, patches, steps):
     import torch
 
     out = {"steps": steps,
+           "bound": 1e-5,
            "against": "float64 device step from the same state (float64 step == reference to 1e-12 in the tests)"}
     for key, f in (("density", 0), ("energy", 4)):
         num = den = 0.0
@@ -173,17 +176,27 @@ def _rel_l1(ref, low, patches, steps):
     return out
 
 
+def _drift(before, after):
+    """Largest change of a conserved total relative to the largest total."""
+    scale = max(abs(v) for v in before.values()) or 1.0
+    return max(abs(after[k] - before[k]) for k in before) / scale
+
+
 def describe(timings):
     return {str(k): round(float(v), 4) for k, v in sorted(timings.items())} if timings else None
 
 
 class Turbulence:
-    bytes_per_zone_update = 5 * 8 * 4  # 5 state passes x 8 values (5 cell + 3 edge) x float32
+    @property
+    def bytes_per_zone_update(self):
+        # 5 state passes x 8 values (5 cell + 3 edge) x the state's bytes
+        return 5 * 8 * (4 if self.precision == 32 else 8)
 
     @property
     def kernel(self):
         ty, tz = self.engine.layout.tile_shape
-        return f"wb::stage3d_kernel<float, 2, false, {ty}, {tz}>"
+        state = "float" if self.precision == 32 else "double"
+        return f"wb::stage3d_kernel<{state}, float, 2, false, {ty}, {tz}>"
 
     def __init__(self, args, rank):
         from wellbalanced_b200.mhd3d import MHD3D
@@ -191,8 +204,9 @@ class Turbulence:
         self.n = args.cells
         self.rank = rank
         self.args = args
+        self.precision = getattr(args, "precision", 32)
         lx = args.lx if args.lx == "auto" else int(args.lx)
-        self.model = MHD3D.turbulence(self.n, seed=rank, precision=32, lx=lx)
+        self.model = MHD3D.turbulence(self.n, seed=rank, precision=self.precision, lx=lx)
         self.engine = self.model.engine
         if args.tile3d and lx != "auto":
             from wellbalanced_b200.autotune import _set_tile
@@ -216,8 +230,11 @@ class Turbulence:
 
     @staticmethod
     def describe(args):
+        state = ("float32 state (float64 pressure recovery)" if getattr(args, "precision", 32) == 32 else
+                 "float32 arithmetic on a float64 state (float64 pressure recovery, potential differences, "
+                 "flux differences and updates)")
         return (f"3D decaying turbulence, periodic {args.cells}^3, MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, "
-                "float32 state (float64 pressure recovery), k^-2 seeded fields, Mach 1, |B|_rms 1")
+                f"{state}, k^-2 seeded fields, Mach 1, |B|_rms 1")
 
     def config(self):
         eng = self.engine
@@ -243,17 +260,23 @@ class Turbulence:
                 "steps": steps,
                 "what": "PlainMHD3D: the reference MHD3D dataflow on the device, float64, per-kernel, intermediates in HBM"}
 
-    def accuracy(self, steps=10):
+    #: the configuration's horizon: 100 RK2 steps
+    horizon = 100
+
+    def accuracy(self, steps=None):
         import torch
 
         from wellbalanced_b200.mhd3d import MHD3D
 
+        steps = self.horizon if steps is None else steps
         ref = MHD3D.turbulence(self.n, seed=self.rank, precision=64)
-        low = MHD3D.turbulence(self.n, seed=self.rank, precision=32)
+        low = MHD3D.turbulence(self.n, seed=self.rank, precision=self.precision)
+        before = low.totals()
         for _ in range(steps):
             low.step(ref.step())
         out = _rel_l1(ref, low, list(zip(ref.hierarchy.patches, low.hierarchy.patches, strict=True)), steps)
         out["div_b"] = low.divergence()
+        out["totals_drift"] = _drift(before, low.totals())
         del ref, low
         torch.cuda.empty_cache()
         return out
@@ -335,13 +358,17 @@ class BatchWorkload:
                 "what": f"PlainMHD2D (the reference MHD2D dataflow per kernel, float64) looped over the first {count} "
                         "instances of the batch"}
 
-    def accuracy(self, steps=10):
+    #: the configuration's horizon: 200 steps per instance
+    horizon = 200
+
+    def accuracy(self, steps=None):
         import torch
 
         from wellbalanced_b200.mesh import AMRHierarchy
         from wellbalanced_b200.mhd import MHD2D
         from wellbalanced_b200.problems import orszag_tang_2d, orszag_tang_sizes
 
+        steps = self.horizon if steps is None else steps
         sides, bf, vf = orszag_tang_sizes(self.count, seed=self.rank)
         k = int(max(range(len(sides)), key=lambda i: sides[i]))
         n = int(sides[k])
@@ -352,11 +379,13 @@ class BatchWorkload:
             model.set_conserved(*orszag_tang_2d(n, bf[k], vf[k]))
             models.append(model)
         ref, low = models
+        before = low.totals()
         for _ in range(steps):
             low.step(ref.step())
         out = _rel_l1(ref, low, list(zip(ref.hierarchy.patches, low.hierarchy.patches, strict=True)), steps)
         out["instance"] = f"{n}^2 (instance {k})"
         out["div_b"] = low.divergence()
+        out["totals_drift"] = _drift(before, low.totals())
         del ref, low, models
         torch.cuda.empty_cache()
         return out
@@ -416,13 +445,18 @@ class Harris:
                 "steps": steps,
                 "what": "PlainMHD2D (the reference MHD2D dataflow per kernel, float64) on the same hierarchy"}
 
-    def accuracy(self, steps=10):
+    #: steps of the accuracy comparison (the configuration states no horizon)
+    horizon = 100
+
+    def accuracy(self, steps=None):
         import torch
 
         from wellbalanced_b200.mhd import MHD2D
 
+        steps = self.horizon if steps is None else steps
         ref = _harris_on(_copy_mesh(self.model.hierarchy), MHD2D, 64, self.rank)
         low = _harris_on(_copy_mesh(self.model.hierarchy), MHD2D, 32, self.rank)
+        before = low.totals()
         for _ in range(steps):
             low.step(ref.step())
         base = list(zip(ref.hierarchy.patches_at_level(0), low.hierarchy.patches_at_level(0), strict=True))
@@ -430,6 +464,7 @@ class Harris:
         out["against"] = "float64 device step from the same state on the same hierarchy (base level, restricted)"
         out["div_b"] = low.divergence()
         out["composite_div_b"] = low.composite_divergence()
+        out["totals_drift"] = _drift(before, low.totals())
         del ref, low
         torch.cuda.empty_cache()
         return out
@@ -494,6 +529,12 @@ def cpu_baseline(workload):
                       "1 process"}
 
 
+#: cells a side of the turbulence box each host process steps in the reference arm: large
+#: enough that the two-cell ghost layers are a small share of the work (a third of a 32^3
+#: box's haloed arrays are ghosts, 17% of a 64^3 box's)
+REFERENCE_BOX = 64
+
+
 def reference_arm(args):
     import multiprocessing as mp
 
@@ -503,18 +544,19 @@ def reference_arm(args):
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
-        pool.map(_cpu_sample, [(args.workload, s, 0, 32) for s in range(cores)])  # spin up, import
+        pool.map(_cpu_sample, [(args.workload, s, 0, REFERENCE_BOX) for s in range(cores)])  # spin up, import
         per_step = []
         for step in range(args.warmup + args.steps):
             start = time.perf_counter()
-            results = pool.map(_cpu_sample, [(args.workload, s, 1, 32) for s in range(cores)])
+            results = pool.map(_cpu_sample, [(args.workload, s, 1, REFERENCE_BOX) for s in range(cores)])
             wall = time.perf_counter() - start
             if step >= args.warmup:
                 per_step.append((sum(c for c, _ in results), wall))
     total_cells = sum(c for c, _ in per_step)
     total_time = sum(t for _, t in per_step)
     value = total_cells / total_time
-    sample = {"turbulence": "a 32^3 turbulence box", "batch": "one Orszag-Tang instance of the batch",
+    sample = {"turbulence": f"a {REFERENCE_BOX}^3 turbulence box of the same seeded fields",
+              "batch": "one Orszag-Tang instance of the batch",
               "harris": "the 128x256 Harris base level"}[args.workload]
     line = {
         "impl": "reference",
@@ -647,6 +689,173 @@ def issue_roofline(workload, cells, launch_s, clock_info):
             "warp_instructions_per_cell_launch": per_cell, "sm_mhz": mhz, "sms": sms}
 
 
+def measure(work, args, rank, world, local, barrier, *, steps, warmup, e2e=True, graph=True):
+    """Time `steps` RK2 steps of `work` after `warmup` untimed ones (barrier and device
+    synchronisation on both sides, CUDA events, max over ranks), then the graph replay and
+    the end-to-end leg. Returns the raw figures of the run."""
+    import torch
+    import torch.distributed as dist
+
+    global L2_FLUSH
+    eng = work.engine
+    L2_FLUSH = _flush_buffer(eng, local)
+    work.advance(warmup)
+    torch.cuda.synchronize()
+
+    # timed region: K RK2 steps, state resident in HBM
+    eng.stage_events = []
+    launches0 = eng.launches
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    chunk = getattr(work, "max_steps", None) or steps
+    saved = (eng.state.clone(), eng.time.clone()) if steps > chunk else None
+    seconds, left = 0.0, steps
+    while left > 0:
+        n = min(chunk, left)
+        if L2_FLUSH is None:
+            seconds += _device_seconds(lambda: work.advance(n), 1)
+        else:
+            seconds += _device_seconds(lambda: work.advance(1), n, L2_FLUSH)
+        left -= n
+        if left > 0:
+            work.restore(*saved)  # outside the timed events
+    del saved
+    barrier()
+    clock_info = clocks.stop()
+    launches = eng.launches - launches0
+    stage_ms = [s.elapsed_time(e) for s, e in eng.stage_events]
+    eng.stage_events = None
+    if int(eng.bad.item()):
+        raise FloatingPointError("bad cells during the benchmark")
+    t = torch.tensor([seconds], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    seconds = float(t.item())
+    out = {"seconds": seconds, "value": world * work.cells * steps / seconds, "launches": launches,
+           "stage_ms": stage_ms, "clocks": clock_info, "steps": steps, "warmup": warmup}
+    out["graph_ms"] = work.graph_timing(min(steps, 50)) if graph and hasattr(work, "graph_timing") else None
+
+    # end to end with host buffers: per step, the state pool is copied in from pinned host
+    # memory, advanced one step and copied back
+    out["e2e"] = None
+    if e2e:
+        pool = eng.state
+        host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
+        host.copy_(pool)
+        torch.cuda.synchronize()
+        e2e_steps = max(3, min(steps, 20))
+        barrier()
+        torch.cuda.synchronize()
+
+        def round_trip():
+            pool.copy_(host, non_blocking=True)
+            work.advance(1)
+            host.copy_(pool, non_blocking=True)
+
+        e2e_seconds = _device_seconds(round_trip, e2e_steps, L2_FLUSH)
+        barrier()
+        t2 = torch.tensor([e2e_seconds], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        nbytes = host.numel() * host.element_size()
+        out["e2e"] = {
+            "value": world * work.cells * e2e_steps / float(t2.item()),
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(nbytes),
+            "d2h_bytes_per_step": int(nbytes),
+            "path": "state pool copied in from pinned host memory, one step, copied back (every step)",
+        }
+    return out
+
+
+def roofline(name, work, run):
+    """The stage kernel's HBM roofline of a measured run (rank 0)."""
+    peak, peak_kind = peaks()
+    cells = work.cells
+    launch_s = statistics.mean(run["stage_ms"]) / 1e3 if run["stage_ms"] else float("nan")
+    per_launch = work.bytes_per_zone_update / 2 * cells
+    achieved = per_launch / launch_s / 1e9
+    return {
+        "bound": "hbm",
+        "achieved": achieved,
+        "peak": peak,
+        "unit": "GB/s",
+        "frac": achieved / peak,
+        # the committed ncu figures are of the float32-state kernels
+        "traffic": profile_traffic(name, cells) if getattr(work, "precision", 32) == 32 else None,
+        "kernel": work.kernel,
+        "algorithmic_bytes_per_launch": per_launch,
+        "mean_launch_ms": 1e3 * launch_s,
+        "peak_kind": peak_kind,
+        "issue": issue_roofline(name, cells, launch_s, run["clocks"]) if getattr(work, "precision", 32) == 32 else None,
+    }
+
+
+def workload_config(work, world, args, steps):
+    eng = work.engine
+    config = work.config()
+    config["parallelism"] = f"replicas x{world}"
+    limit = getattr(work, "max_steps", None)
+    if limit and steps > limit:
+        config["timed_runs"] = (f"{-(-steps // limit)} runs of at most {limit} steps, each from the state "
+                                "after warm-up (restored outside the timed events)")
+    pool_gb = eng.state.numel() * eng.state.element_size() / 1e9
+    if L2_FLUSH is None:
+        config["l2"] = "inputs larger than L2 (state pool {:.2f} GB per copy)".format(pool_gb)
+    else:
+        config["l2"] = ("L2 flushed before every timed step, outside its CUDA events (a {:.0f} MB write; "
+                        "state pool {:.3f} GB per copy, smaller than L2)").format(L2_FLUSH.numel() * 4 / 1e6, pool_gb)
+    return config
+
+
+#: the configurations measured beside the headline in the default run: (workload, state
+#: precision, steps, warm-up); the float32-state headline's twin with a float64 state
+#: meets the L1 bound over the longest horizons (Orszag-Tang 256^2 to t = 0.5)
+EXTRA_WORKLOADS = {"turbulence_mixed": ("turbulence", "mixed", 20, 3), "batch": ("batch", 32, 20, 3),
+                   "harris": ("harris", 32, 50, 5)}
+
+
+def extra_workload(name, args, rank, world, local, barrier):
+    """One more configuration measured in the same run (value, roofline, graph replay,
+    plain float64 step, accuracy over its horizon), as a `workloads` entry."""
+    import copy
+
+    import torch
+
+    kind, precision, steps, warmup = EXTRA_WORKLOADS[name]
+    args = copy.copy(args)
+    args.precision = precision
+    work = WORKLOADS[kind](args, rank)
+    run = measure(work, args, rank, world, local, barrier, steps=steps, warmup=warmup, e2e=False)
+    entry = {
+        "value": run["value"],
+        "unit": UNIT,
+        "ms_per_step": 1e3 * run["seconds"] / steps,
+        "steps": steps,
+        "warmup": warmup,
+        "gpu_launches": run["launches"],
+        "launches_per_step": run["launches"] / steps,
+        "config": workload_config(work, world, args, steps),
+        "roofline": roofline(kind, work, run),
+        "precision": precision,
+        "clocks": run["clocks"],
+    }
+    if run["graph_ms"] is not None:
+        entry["graph"] = {"ms_per_step": run["graph_ms"], "value": world * work.cells / (run["graph_ms"] / 1e3),
+                          "what": "the same steps replayed from one captured CUDA graph"}
+    if rank == 0 and not args.no_plain and kind != args.workload:
+        entry["plain_fp64"] = work.plain()
+        entry["plain_fp64"]["speedup_of_value"] = run["value"] / world / entry["plain_fp64"]["value"]
+    if rank == 0 and not args.no_accuracy:
+        entry["accuracy"] = work.accuracy()
+    del work
+    torch.cuda.empty_cache()
+    return entry
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -671,101 +880,28 @@ def main():
             dist.barrier()
 
     work = WORKLOADS[args.workload](args, rank)
-    eng = work.engine
-    global L2_FLUSH
-    L2_FLUSH = _flush_buffer(eng, local)
-    work.advance(args.warmup)
-    torch.cuda.synchronize()
-
-    # timed region: K RK2 steps, state resident in HBM
-    eng.stage_events = []
-    launches0 = eng.launches
-    clocks = Clocks(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.3)
-    chunk = getattr(work, "max_steps", None) or args.steps
-    saved = (eng.state.clone(), eng.time.clone()) if args.steps > chunk else None
-    seconds, left = 0.0, args.steps
-    while left > 0:
-        n = min(chunk, left)
-        if L2_FLUSH is None:
-            seconds += _device_seconds(lambda: work.advance(n), 1)
-        else:
-            seconds += _device_seconds(lambda: work.advance(1), n, L2_FLUSH)
-        left -= n
-        if left > 0:
-            work.restore(*saved)  # outside the timed events
-    del saved
-    barrier()
-    clock_info = clocks.stop()
-    launches = eng.launches - launches0
-    stage_ms = [s.elapsed_time(e) for s, e in eng.stage_events]
-    eng.stage_events = None
-    if int(eng.bad.item()):
-        raise FloatingPointError("bad cells during the benchmark")
-    t = torch.tensor([seconds], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    seconds = float(t.item())
-    cells = work.cells
-    value = world * cells * args.steps / seconds
-
-    graph_ms = work.graph_timing(min(args.steps, 50)) if hasattr(work, "graph_timing") else None
-
-    # end to end with host buffers: per step, the state pool is copied in from pinned host
-    # memory, advanced one step and copied back
-    e2e = None
-    if not args.no_e2e:
-        pool = eng.state
-        host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
-        host.copy_(pool)
-        torch.cuda.synchronize()
-        e2e_steps = max(3, min(args.steps, 20))
-        barrier()
-        torch.cuda.synchronize()
-
-        def round_trip():
-            pool.copy_(host, non_blocking=True)
-            work.advance(1)
-            host.copy_(pool, non_blocking=True)
-
-        e2e_seconds = _device_seconds(round_trip, e2e_steps, L2_FLUSH)
-        barrier()
-        t2 = torch.tensor([e2e_seconds], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        nbytes = host.numel() * host.element_size()
-        e2e = {
-            "value": world * cells * e2e_steps / float(t2.item()),
-            "unit": UNIT,
-            "h2d_bytes_per_step": int(nbytes),
-            "d2h_bytes_per_step": int(nbytes),
-            "path": "state pool copied in from pinned host memory, one step, copied back (every step)",
-        }
-
+    run = measure(work, args, rank, world, local, barrier, steps=args.steps, warmup=args.warmup,
+                  e2e=not args.no_e2e)
+    value, seconds = run["value"], run["seconds"]
     plain = work.plain() if rank == 0 and not args.no_plain else None
     accuracy = work.accuracy() if rank == 0 and not args.no_accuracy else None
+    config = workload_config(work, world, args, args.steps) if rank == 0 else None
+    line_roofline = roofline(args.workload, work, run) if rank == 0 else None
+    graph = None
+    if run["graph_ms"] is not None:
+        graph = {"ms_per_step": run["graph_ms"], "value": world * work.cells / (run["graph_ms"] / 1e3),
+                 "what": "the same steps replayed from one captured CUDA graph"}
+
+    # the other configurations, measured in the same run at one GPU (the headline's
+    # scaling lines carry the headline workload only)
+    extras = {}
+    if world == 1 and args.workload == "turbulence" and not args.no_extra:
+        del work
+        torch.cuda.empty_cache()
+        for name in EXTRA_WORKLOADS:
+            extras[name] = extra_workload(name, args, rank, world, local, barrier)
 
     if rank == 0:
-        peak, peak_kind = peaks()
-        launch_s = statistics.mean(stage_ms) / 1e3 if stage_ms else float("nan")
-        per_launch = work.bytes_per_zone_update / 2 * cells
-        achieved = per_launch / launch_s / 1e9
-        config = work.config()
-        config["parallelism"] = f"replicas x{world}"
-        limit = getattr(work, "max_steps", None)
-        if limit and args.steps > limit:
-            config["timed_runs"] = (f"{-(-args.steps // limit)} runs of at most {limit} steps, each from the state "
-                                    "after warm-up (restored outside the timed events)")
-        pool_gb = eng.state.numel() * eng.state.element_size() / 1e9
-        if L2_FLUSH is None:
-            config["l2"] = "inputs larger than L2 (state pool {:.2f} GB per copy)".format(pool_gb)
-        else:
-            config["l2"] = ("L2 flushed before every timed step, outside its CUDA events (a {:.0f} MB write; "
-                            "state pool {:.3f} GB per copy, smaller than L2)").format(
-                L2_FLUSH.numel() * 4 / 1e6, pool_gb)
         line = {
             "metric": METRIC,
             "value": value,
@@ -780,34 +916,23 @@ def main():
             "dtype": "f32",
             "data": "synthetic",
             "config": config,
-            "roofline": {
-                "bound": "hbm",
-                "achieved": achieved,
-                "peak": peak,
-                "unit": "GB/s",
-                "frac": achieved / peak,
-                "traffic": profile_traffic(args.workload, cells),
-                "kernel": work.kernel,
-                "algorithmic_bytes_per_launch": per_launch,
-                "mean_launch_ms": 1e3 * launch_s,
-                "peak_kind": peak_kind,
-                "issue": issue_roofline(args.workload, cells, launch_s, clock_info),
-            },
-            "gpu_launches": launches,
-            "clocks": clock_info,
+            "roofline": line_roofline,
+            "gpu_launches": run["launches"],
+            "clocks": run["clocks"],
         }
-        if graph_ms is not None:
-            line["graph"] = {"ms_per_step": graph_ms, "value": world * cells / (graph_ms / 1e3),
-                             "what": "the same steps replayed from one captured CUDA graph"}
+        if graph is not None:
+            line["graph"] = graph
         if baseline is not None:
             line["cpu_baseline"] = baseline
-        if e2e is not None:
-            line["e2e"] = e2e
+        if run["e2e"] is not None:
+            line["e2e"] = run["e2e"]
         if accuracy is not None:
             line["accuracy"] = accuracy
         if plain is not None:
             line["plain_fp64"] = plain
             line["plain_fp64"]["speedup_of_value"] = value / world / plain["value"]
+        if extras:
+            line["workloads"] = extras
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -92,7 +92,13 @@ int wb_mhd_conductive(const double* prim, const double* bxf, const double* byf, 
  * (struct PatchDesc[]), replacing carafe/mhd.py:889-927 (_advance) for MHD2D and
  * carafe/mhd3d.py:635-671 for MHD3D, with the Heun combine of mhd.py:983-988:
  *   base == NULL: dst = src - dt L(src);   else dst = (src - dt L(src) + base) / 2.
- * `precision`: 32 (float state) or 64 (double state); src/base/dst are pools of that type.
+ * `precision`: 32 (float state and arithmetic), 64 (double state and arithmetic) or
+ * WB_MATH32_STATE64 (a double state advanced with float arithmetic: primitive variables
+ * and face fields formed in double and rounded to float, reconstruction / HLLD / CT in
+ * float, flux differences and the updates of U, A and the Heun combine in double);
+ * src/base/dst are pools of the state's type. */
+#define WB_MATH32_STATE64 6432
+/*
  * dt: device double per instance. bad: device counter of bad cells (added to).
  * bflux: device double array of boundary-face fluxes (NULL to skip).
  * lx (3D only): cell planes per tile along x. */
@@ -159,6 +165,23 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
                    double gamma, const double* inv_dx2_sum, double* time, const double* end, double* dt,
                    int advance, void* stream);
 
+/* wb_rate that also reduces the smallest density of every (instance, level):
+ * level_keys[instance * nlevels + level] (order-preserving keys, nlevels * ninstances).
+ * With wb_finalize_dt_levels it takes the diffusion limit level by level, each level's
+ * smallest density with that level's spacing, as carafe/mhd.py:942-960 does patch by
+ * patch (patches of one level share their spacing). A patch whose instance or level lies
+ * outside the key arrays is skipped (as in wb_rate). */
+int wb_rate_levels(int precision, int ndim, const void* state, const void* patches, int npatches,
+                   const int* chunk_patch, const int* chunk_start, int nchunks, double b0x, double b0y,
+                   double b0z, double gamma, unsigned long long* keys, int ninstances,
+                   unsigned long long* level_keys, int nlevels, void* stream);
+/* wb_finalize_dt with the diffusion limit min over levels l of 0.5 / (D_l * inv_dx2_levels[i
+ * * nlevels + l]), D_l = max(eta, (gamma - 1) kappa / min rho of level l); levels with
+ * inv_dx2_levels 0 hold no patch of the instance and are skipped. */
+int wb_finalize_dt_levels(const unsigned long long* keys, int ninstances, double cfl, double eta, double kappa,
+                          double gamma, const unsigned long long* level_keys, const double* inv_dx2_levels,
+                          int nlevels, double* time, const double* end, double* dt, int advance, void* stream);
+
 /* Halo and restriction op lists (struct CopyOp / InterpOp / RestrictOp), replacing
  * patchwork's exchange_halos and restrict (carafe/mhd.py:744-777, 981, 991). An op covers
  * fewer than 2^31 points of fields 0..7, and never writes a point it reads. One 64-thread
@@ -224,10 +247,13 @@ int wb_mlp_adam(float* params, float* grads, float* m, float* v, int count, floa
  * instances (64 KiB per device), and the result is decoded into `out` (device float64,
  * 2 * ninstances): out[2k] = largest rate, out[2k+1] = smallest density of instance k.
  * - ninstances > 4096 returns WB_TOO_LARGE with a message (use wb_rate for more);
- * - every patch's instance index must be below ninstances (as for wb_rate);
+ * - a patch whose instance index is not below ninstances is skipped and makes every
+ *   value of `out` NaN (a call that cannot give the rate of every instance gives none);
  * - nothing must start at zero: each call initialises the slots it uses;
  * - the first call on a device resolves the scratch address (cudaGetSymbolAddress) and
  *   caches it; make that call before any stream capture that includes this function;
+ *   the cached address belongs to the device's primary context and does not survive
+ *   cudaDeviceReset (do not call this function after a reset in the same process);
  * - all calls on a device share the scratch: calls in flight at the same time (other
  *   streams, other threads) race and may return wrong values. */
 int wb_rate_static(int precision, int ndim, const void* state, const void* patches, int npatches,

@@ -1,8 +1,9 @@
 """Generate the golden vectors of the oracle from the reference itself.
 
-Run in a container holding the reference checkout (default ``/root/reference``)::
+Run in a container holding the reference checkout, given by ``--reference`` or the
+``WB_REFERENCE`` environment variable (the checkout's root, holding ``src/carafe``)::
 
-    python tests/golden/make_golden.py [--reference PATH] [--full]
+    python tests/golden/make_golden.py --reference PATH [--full]
 
 The reference's own ``carafe.mhd.MHD2D`` / ``carafe.mhd3d.MHD3D`` and its kernels
 (``carafe/kernels/<name>/<name>_numpy.py`` and ``_pyccel.py`` run as plain Python) are
@@ -15,6 +16,7 @@ the Orszag–Tang vortex on 256^2 cells to t = 0.5 (about 11 minutes on one core
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import time
 from pathlib import Path
@@ -418,10 +420,13 @@ def full_golden(out):
 
 def main():
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("WB_REFERENCE"),
+                        help="the reference checkout's root (default: $WB_REFERENCE)")
     parser.add_argument("--full", action="store_true")
     parser.add_argument("--only", default=None)
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give the reference checkout with --reference PATH or WB_REFERENCE")
     reference_stubs.install(f"{args.reference}/src")
     jobs = {
         "kernels": kernels_golden,

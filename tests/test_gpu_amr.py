@@ -48,6 +48,45 @@ def _pair(cells=16, precision=64, **options):
     return oracle, device
 
 
+def test_refined_2d_conduction_step_takes_each_levels_density_with_its_spacing():
+    """The conduction limit of the time step (carafe/mhd.py:942-960) pairs each patch's
+    smallest density with that patch's own spacing. The thinnest gas sits on the coarse
+    level, outside the fine patch: the device's own dt (no dt passed) equals the
+    oracle's stable_step on every step, not the stricter limit of the coarse density at
+    the fine spacing."""
+    from oracle.mesh import Hierarchy
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    cells = 16
+    box = ((cells - cells // 2, cells + cells // 2), (cells // 2, 3 * cells // 2))
+    oh = Hierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), (True, True))
+    oh.add_patch(1, box)
+    dh = AMRHierarchy((2 * cells, cells), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True))
+    dh.add_patch(1, box)
+    options = dict(conduction=(0.5, 0.1), mean_field=(0.1, 0.05))
+    oracle = OracleMHD2D(oh, limiter="minmod", **options)
+    device = MHD2D(dh, limiter="minmod", precision=64, **options)
+    state = dict(
+        density=lambda x, y: 1.0 - 0.6 * np.exp(-((x - 0.8) ** 2 + y**2) / 0.01),
+        velocity=(0.2, 0.1, 0.0),
+        pressure=1.0,
+        vector_potential=lambda x, y: 0.05 * np.cos(np.pi * x),
+    )
+    for model in (oracle, device):
+        model.set_state(state["density"], state["velocity"], state["pressure"],
+                        vector_potential=state["vector_potential"])
+    for _ in range(4):
+        expect = oracle.step()
+        got = device.step()
+        assert got == pytest.approx(expect, rel=1e-13)
+    # the coarse density at the fine spacing would have given a step 2.5x shorter
+    rho_min = min(float(np.min(p.field(oracle.names["density"]).local)) for p in oh.patches)
+    fine = sum(d**-2 for d in oh.spacing(1))
+    assert got > 1.5 * oracle.cfl * 0.5 / ((oracle.gamma - 1.0) * 0.5 / rho_min * fine)
+
+
 def test_refined_2d_matches_the_oracle_patch_by_patch():
     oracle, device = _pair()
     for _ in range(12):

@@ -126,16 +126,20 @@ def test_a_multi_patch_level_matches_the_reference():
     np.testing.assert_allclose(model.state()["density"], golden["split_density"], rtol=1e-12, atol=1e-12)
 
 
-def test_float32_orszag_tang_error_against_the_float64_reference(runs2d):
+@pytest.mark.parametrize("precision", [32, "mixed"])
+def test_float32_orszag_tang_error_against_the_float64_reference(runs2d, precision):
+    """Orszag-Tang 64^2 to t = 0.5 with float32 arithmetic (float32 or float64 state)
+    against the reference's float64 run: relative L1 of density and energy within 1e-5,
+    div B at round-off."""
     from wellbalanced_b200.mhd import MHD2D
 
-    model = MHD2D.orszag_tang(64, limiter="mc", cfl=0.4, precision=32)
+    model = MHD2D.orszag_tang(64, limiter="mc", cfl=0.4, precision=precision)
     model.run(0.5)
     state = model.state()
     err_rho = rel_l1(state["density"], runs2d["ot64_mc_density"])
     err_e = rel_l1(state["energy"], runs2d["ot64_mc_energy"])
-    print(f"float32 OT 64^2 to t=0.5: rel L1 rho {err_rho:.3e}, E {err_e:.3e}, steps {model.steps}")
-    assert err_rho < 1e-4 and err_e < 1e-4
+    print(f"{precision} OT 64^2 to t=0.5: rel L1 rho {err_rho:.3e}, E {err_e:.3e}, steps {model.steps}")
+    assert err_rho < 1e-5 and err_e < 1e-5
     assert model.divergence() < 1e-12
 
 
@@ -488,7 +492,7 @@ def test_every_2d_tile_shape_gives_the_same_steps():
     from wellbalanced_b200.autotune import tune_tile2d
     from wellbalanced_b200.mhd import MHD2D
 
-    for precision in (32, 64):
+    for precision in (32, 64, "mixed"):
         reference = MHD2D.orszag_tang(40, precision=precision, limiter="mc")
         for _ in range(3):
             reference.step()
@@ -537,16 +541,16 @@ def test_every_3d_tile_shape_gives_the_same_steps():
                                       lambda x, y, z: 0.1 * np.cos(k * y)))
         return m
 
-    for precision in (32, 64):
+    for precision in (32, 64, "mixed"):
         reference = model(precision)
         for _ in range(3):
             reference.step()
-        for tile in _lib.tile_shapes(3, precision):
+        for tile in _lib.tile_shapes(3, _lib.precision_code(precision)):
             m = model(precision, tile)
             assert m.engine.layout.tile_shape == tile
             for _ in range(3):
                 m.step()
-            tol = 1e-5 if precision == 32 else 1e-12
+            tol = 1e-12 if precision == 64 else 1e-5
             assert torch.allclose(m.engine.state, reference.engine.state, rtol=tol, atol=tol * 0.1), (precision, tile)
 
 
@@ -571,12 +575,13 @@ def test_saved_state_resumes_bitwise():
         assert torch.equal(model.engine.state, after)
 
 
-@pytest.mark.parametrize("precision", [64, 32])
+@pytest.mark.parametrize("precision", [64, 32, "mixed"])
 def test_alfven_wave_converges_at_second_order(precision):
     """The reference's convergence tests (tests/unit/test_mhd.py:78-86,
     tests/unit/test_mhd3d.py:13-21): the circularly polarised Alfven wave after one period
     at 8 and 16 cells, unlimited slopes; the error of B_y falls by 2^1.85 (2D) / 2^1.8
-    (3D), div B stays at round-off. float32 runs the same bound."""
+    (3D), div B stays at round-off (the curl of the stored potential, taken in float64:
+    1e-14 as the reference's bound for a float64 potential, 1e-12 for a float32 one)."""
     from wellbalanced_b200.mhd import MHD2D
     from wellbalanced_b200.mhd3d import MHD3D
 
@@ -587,26 +592,77 @@ def test_alfven_wave_converges_at_second_order(precision):
             model.run(model.period)
             by = model.dataset()["magnetic_field_y"].values
             errors.append(float(np.mean(np.abs(by - exact["magnetic_field_y"].values))))
-            assert model.divergence() < (1e-14 if precision == 64 else 1e-6), cls.__name__
+            assert model.divergence() < (1e-12 if precision == 32 else 1e-14), cls.__name__
         assert np.log2(errors[0] / errors[1]) > order, (cls.__name__, errors)
 
 
 def test_config1_orszag_tang_256_to_half_time_against_the_reference_run():
     """Config 1 at its full size and horizon (256^2, MC, CFL 0.4, t = 0.5: 1441 steps)
-    against the reference's own run of it (committed fixture): float64 equal to rounding,
-    float32 (float64 pressure recovery) within its measured 1.7e-5 / 2.2e-5 relative L1 of
-    density / energy (correctly rounded float32 division and square root give the same
-    1.7e-5: the gap is the float32 state and arithmetic, not the fast reciprocals)."""
+    against the reference's own run of it (committed fixture).
+
+    * float64: equal to rounding (1e-12).
+    * "mixed" (float32 reconstruction, HLLD and CT; float64 state, pressure recovery and
+      updates): relative L1 of density and energy within 1e-5.
+    * float32 state: the rounding of the stored state to float32 after every stage is by
+      itself 1.06e-5 (density) / 1.28e-5 (energy) at this horizon (the reference's float64
+      arithmetic with the state rounded to float32 after each stage, a NumPy restatement of
+      this run), so a float32 state cannot meet 1e-5 over the whole horizon; it is held to
+      2e-5 here (measured 1.7e-5 / 2.2e-5), and the float64 state of "mixed" is what meets
+      the bound."""
     from wellbalanced_b200.mhd import MHD2D
 
     golden = np.load(GOLDEN / "ot256_full.npz")
-    for precision, bound in ((64, 1e-12), (32, 5e-5)):
+    for precision, bound in ((64, 1e-12), ("mixed", 1e-5), (32, 2e-5)):
         model = MHD2D.orszag_tang(256, limiter="mc", cfl=0.4, precision=precision)
         model.run(float(golden["time"]))
         assert model.steps == int(golden["steps"])
         state = model.state()
         err_rho = rel_l1(state["density"], golden["density"])
         err_e = rel_l1(state["energy"], golden["energy"])
-        print(f"config 1, float{precision}: rel L1 rho {err_rho:.3e}, E {err_e:.3e}")
+        print(f"config 1, precision {precision}: rel L1 rho {err_rho:.3e}, E {err_e:.3e}")
         assert err_rho < bound and err_e < bound, (precision, err_rho, err_e)
-        assert model.divergence() < 1e-12
+        assert model.divergence() < (1e-12 if precision == 32 else 1e-14)
+
+
+def test_mixed_precision_3d_turbulence_error_div_b_and_totals(runs3d):
+    """float32 arithmetic on a float64 state, 3D: the reference's float64 turbulence run to
+    1e-5 (relative L1), div B at the float64 round-off of the stored potential, and the
+    conserved totals kept to float64 round-off (the state is the accumulator)."""
+    model = _turbulence("mixed")
+    before = model.totals()
+    for dt in runs3d["turb16_dts"]:
+        model.step(float(dt))
+    state = model.state()
+    err_rho = rel_l1(state["density"], runs3d["turb16_density"])
+    err_e = rel_l1(state["energy"], runs3d["turb16_energy"])
+    print(f"mixed turbulence 16^3, 4 steps: rel L1 rho {err_rho:.3e}, E {err_e:.3e}")
+    assert err_rho < 1e-5 and err_e < 1e-5
+    assert model.divergence() < 1e-14
+    after = model.totals()
+    for key in before:
+        assert abs(after[key] - before[key]) < 1e-13 * max(1.0, abs(before[key])), key
+
+
+def test_mixed_precision_refined_2d_keeps_totals_and_composite_div_b():
+    """float32 arithmetic on a float64 state on a refined hierarchy: the flux register
+    recomputes the interface fluxes with the stage kernel's float32 arithmetic, so the
+    composite totals stay at float64 round-off, as in float64 (tests/unit/test_mhd.py:164-211
+    of the reference)."""
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    mesh = AMRHierarchy((32, 16), ((-1.0, 1.0), (-0.5, 0.5)), periodic=(True, True))
+    mesh.add_patch(1, ((16, 48), (8, 24)))
+    model = MHD2D(mesh, limiter="mc", precision="mixed", mean_field=(0.1, 0.05))
+    model.set_state(lambda x, y: 1.0 + 0.5 * np.exp(-((x + 0.3) ** 2 + y**2) / 0.02), (2.0, 1.0, 0.3),
+                    lambda x, y: 1.0 + 0.2 * np.cos(np.pi * x),
+                    vector_potential=lambda x, y: 0.1 * np.maximum(0.3 - np.hypot(x, y), 0.0),
+                    bz=lambda x, y: 0.1 * np.sin(np.pi * x))
+    before = model.totals()
+    for _ in range(10):
+        model.step()
+    after = model.totals()
+    for key in before:
+        assert abs(after[key] - before[key]) < 1e-13 * max(1.0, abs(before[key])), key
+    assert model.divergence() < 1e-14
+    assert model.composite_divergence() < 1e-14

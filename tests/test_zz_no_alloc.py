@@ -89,3 +89,18 @@ def test_more_instances_than_the_scratch_holds_are_rejected():
     status, _ = _rate_static(batch.engine, ninstances=4097, out=out)
     assert status == -4
     assert "4096 instances" in _lib.load().wb_last_error().decode()
+
+
+def test_a_patch_beyond_the_instance_count_makes_every_value_nan():
+    """A patch whose instance index is not below the count given is skipped by the rate
+    kernel (nothing is written outside the instances' slots) and the whole output is NaN;
+    the next call with the right count is correct again."""
+    batch = _scaled_batch(1.0)
+    status, out = _rate_static(batch.engine, ninstances=2)
+    assert status == 0
+    torch.cuda.synchronize()
+    assert np.all(np.isnan(out.cpu().numpy()))
+    status, out = _rate_static(batch.engine)
+    assert status == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy().reshape(-1, 2), _existing(batch.engine))

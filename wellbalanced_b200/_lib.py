@@ -47,6 +47,10 @@ SIGNATURES = {
     "wb_rate": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp,
                 c_int, c_dp],
     "wb_finalize_dt": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_rate_levels": [c_int, c_int, c_dp, c_dp, c_int, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double,
+                       c_dp, c_int, c_dp, c_int, c_dp],
+    "wb_finalize_dt_levels": [c_dp, c_int, c_double, c_double, c_double, c_double, c_dp, c_dp, c_int, c_dp, c_dp,
+                              c_dp, c_int, c_dp],
     "wb_tag_features": [c_int, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_double, c_double, c_double, c_double, c_dp,
                         c_dp, c_dp, c_dp],
     "wb_mlp_forward": [c_dp, ctypes.c_int64, c_dp, c_dp, c_dp],
@@ -72,6 +76,30 @@ EXPORTS = ("wb_version", "wb_last_error", *SIGNATURES)
 
 class WBError(RuntimeError):
     """A failure reported by the C ABI (status and wb_last_error text)."""
+
+
+#: The precision code of a float64 state advanced with float32 arithmetic
+#: (``WB_MATH32_STATE64``): reconstruction, HLLD and CT in float32; the conserved and
+#: potential updates (the conservation and div B accumulators), the Heun combine, the
+#: pressure recovery and the face fields' potential differences in float64.
+MATH32_STATE64 = 6432
+
+#: Codes of the ``precision`` keyword: 32 (float32 state and arithmetic), 64 (float64),
+#: "mixed" (float32 arithmetic on a float64 state).
+PRECISIONS = {32: 32, 64: 64, "mixed": MATH32_STATE64, MATH32_STATE64: MATH32_STATE64}
+
+
+def precision_code(value) -> int:
+    """The C-ABI precision code of a ``precision`` keyword (32, 64 or "mixed")."""
+    try:
+        return PRECISIONS[value]
+    except (KeyError, TypeError):
+        raise ValueError(f"precision is 32, 64 or 'mixed', not {value!r}") from None
+
+
+def state_bits(code) -> int:
+    """Bits of a state value under a precision code (the mixed code keeps float64 state)."""
+    return 32 if code == 32 else 64
 
 
 def load():
@@ -126,7 +154,7 @@ def tile_shapes(ndim, precision) -> list[tuple[int, int]]:
     3D), the default first."""
     lib = load()
     buf = (ctypes.c_int * 32)()
-    count = lib.wb_tile_shapes(int(ndim), int(precision), buf, 16)
+    count = lib.wb_tile_shapes(int(ndim), precision_code(precision), buf, 16)
     if count < 0:
         raise WBError(f"wb_tile_shapes: status {count}: {lib.wb_last_error().decode()}")
     return [(buf[2 * i], buf[2 * i + 1]) for i in range(min(count, 16))]

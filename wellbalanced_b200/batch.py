@@ -16,6 +16,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from wellbalanced_b200 import _lib
 from wellbalanced_b200.engine import Engine
 from wellbalanced_b200.mesh import HALO, AMRHierarchy, Layout
 from wellbalanced_b200.mhd import LIMITER_CODES
@@ -36,7 +37,7 @@ class Batch:
         self.gamma = float(gamma)
         self.limiter = limiter
         self.cfl = float(cfl)
-        self.precision = int(precision)
+        self.precision = _lib.precision_code(precision)
         parts = {}
         layouts = []
         self.hierarchies = []

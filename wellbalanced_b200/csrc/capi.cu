@@ -64,13 +64,19 @@ bool ptrs_ok(std::initializer_list<const void*> ptrs, const char* what) {
   return true;
 }
 
+// Precision codes: 32 (float32 state and arithmetic), 64 (float64), and
+// WB_MATH32_STATE64 (a float64 state advanced with float32 arithmetic). Kernels that only
+// move or reduce the state (halos, restriction, reflux, rate) take the state's type.
 bool precision_ok(int precision, const char* what) {
-  if (precision != 32 && precision != 64) {
-    set_error("%s: precision must be 32 or 64, got %d", what, precision);
+  if (precision != 32 && precision != 64 && precision != kMath32State64) {
+    set_error("%s: precision must be 32, 64 or %d, got %d", what, kMath32State64, precision);
     return false;
   }
   return true;
 }
+
+// the tile-shape table of a precision code
+int shape_mode(int precision) { return precision == 32 ? 0 : (precision == 64 ? 1 : kMath32State64); }
 
 }  // namespace
 
@@ -183,7 +189,8 @@ static int stage2d(int precision, const void* src, const void* base, void* dst, 
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, bflux, 0};
-  return launch_stage2d<double>(a, ntiles, limiter, tx, ty, as_stream(stream));
+  return precision == 64 ? launch_stage2d<double, double>(a, ntiles, limiter, tx, ty, as_stream(stream))
+                         : launch_stage2d<double, float>(a, ntiles, limiter, tx, ty, as_stream(stream));
 }
 
 int wb_stage2d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
@@ -191,7 +198,7 @@ int wb_stage2d(int precision, const void* src, const void* base, void* dst, cons
                unsigned long long* bad, double* bflux, void* stream) {
   set_error("");
   int tx, ty;
-  tile_shape_2d(precision == 64, &tx, &ty);
+  tile_shape_2d(shape_mode(precision), &tx, &ty);
   return stage2d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, limiter, tx, ty, bad, bflux,
                  stream);
 }
@@ -211,7 +218,8 @@ int wb_tile_shapes(int ndim, int precision, int* shapes, int max) {
     set_error("tile_shapes: ndim must be 2 or 3");
     return kBadArgument;
   }
-  return ndim == 2 ? tile_shapes_2d(precision == 64, shapes, max) : tile_shapes_3d(precision == 64, shapes, max);
+  return ndim == 2 ? tile_shapes_2d(shape_mode(precision), shapes, max)
+                   : tile_shapes_3d(shape_mode(precision), shapes, max);
 }
 
 int wb_stage2d_physics(int precision, const void* src, const void* base, void* dst, const void* patches,
@@ -227,7 +235,7 @@ int wb_stage2d_physics(int precision, const void* src, const void* base, void* d
     return kBadArgument;
   }
   int tx, ty;  // the non-ideal kernel runs on the default tiles
-  tile_shape_2d(precision == 64, &tx, &ty);
+  tile_shape_2d(shape_mode(precision), &tx, &ty);
   if (precision == 32) {
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
@@ -239,7 +247,8 @@ int wb_stage2d_physics(int precision, const void* src, const void* base, void* d
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, 0.0}, bad, nullptr, 0};
   a.eta = eta, a.kappa_par = kappa_par, a.kappa_perp = kappa_perp, a.gravity[0] = gx, a.gravity[1] = gy;
-  return launch_stage2d<double>(a, ntiles, limiter, tx, ty, as_stream(stream));
+  return precision == 64 ? launch_stage2d<double, double>(a, ntiles, limiter, tx, ty, as_stream(stream))
+                         : launch_stage2d<double, float>(a, ntiles, limiter, tx, ty, as_stream(stream));
 }
 
 static int stage3d(int precision, const void* src, const void* base, void* dst, const void* patches,
@@ -260,7 +269,8 @@ static int stage3d(int precision, const void* src, const void* base, void* dst, 
   StageArgs<double> a{static_cast<const double*>(src), static_cast<const double*>(base), static_cast<double*>(dst),
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, bflux, lx};
-  return launch_stage3d<double>(a, ntiles, limiter, ty, tz, as_stream(stream));
+  return precision == 64 ? launch_stage3d<double, double>(a, ntiles, limiter, ty, tz, as_stream(stream))
+                         : launch_stage3d<double, float>(a, ntiles, limiter, ty, tz, as_stream(stream));
 }
 
 int wb_stage3d(int precision, const void* src, const void* base, void* dst, const void* patches, const void* tiles,
@@ -268,7 +278,7 @@ int wb_stage3d(int precision, const void* src, const void* base, void* dst, cons
                unsigned long long* bad, double* bflux, void* stream) {
   set_error("");
   int ty, tz;
-  tile_shape_3d(precision == 64, &ty, &tz);
+  tile_shape_3d(shape_mode(precision), &ty, &tz);
   return stage3d(precision, src, base, dst, patches, tiles, ntiles, dt, gamma, b0x, b0y, b0z, limiter, lx, ty, tz,
                  bad, bflux, stream);
 }
@@ -294,7 +304,7 @@ int wb_stage3d_physics(int precision, const void* src, const void* base, void* d
     return kBadArgument;
   }
   int ty, tz;  // the non-ideal kernel runs on the default tiles
-  tile_shape_3d(precision == 64, &ty, &tz);
+  tile_shape_3d(shape_mode(precision), &ty, &tz);
   if (precision == 32) {
     StageArgs<float> a{static_cast<const float*>(src), static_cast<const float*>(base), static_cast<float*>(dst),
                        static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
@@ -306,7 +316,8 @@ int wb_stage3d_physics(int precision, const void* src, const void* base, void* d
                       static_cast<const PatchDesc*>(patches), static_cast<const Tile*>(tiles), dt, gamma,
                       1.0 / (gamma - 1.0), {b0x, b0y, b0z}, bad, nullptr, lx};
   a.eta = eta, a.gravity[0] = gx, a.gravity[1] = gy, a.gravity[2] = gz;
-  return launch_stage3d<double>(a, ntiles, limiter, ty, tz, as_stream(stream));
+  return precision == 64 ? launch_stage3d<double, double>(a, ntiles, limiter, ty, tz, as_stream(stream))
+                         : launch_stage3d<double, float>(a, ntiles, limiter, ty, tz, as_stream(stream));
 }
 
 int wb_tile_shape(int ndim, int precision, int* a, int* b) {
@@ -316,9 +327,9 @@ int wb_tile_shape(int ndim, int precision, int* a, int* b) {
     return kBadArgument;
   }
   if (ndim == 2)
-    tile_shape_2d(precision == 64, a, b);
+    tile_shape_2d(shape_mode(precision), a, b);
   else
-    tile_shape_3d(precision == 64, a, b);
+    tile_shape_3d(shape_mode(precision), a, b);
   return kOk;
 }
 
@@ -351,6 +362,49 @@ int wb_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, d
   }
   return launch_finalize_dt(keys, ninstances, cfl, eta, kappa, gamma, inv_dx2_sum, time, end, dt, advance,
                             as_stream(stream));
+}
+
+int wb_rate_levels(int precision, int ndim, const void* state, const void* patches, int npatches,
+                   const int* chunk_patch, const int* chunk_start, int nchunks, double b0x, double b0y, double b0z,
+                   double gamma, unsigned long long* keys, int ninstances, unsigned long long* level_keys,
+                   int nlevels, void* stream) {
+  set_error("");
+  if (!precision_ok(precision, "rate_levels") || !ptrs_ok({state, patches, keys, level_keys}, "rate_levels"))
+    return kBadArgument;
+  if ((ndim != 2 && ndim != 3) || ninstances <= 0 || nlevels <= 0 || nchunks < 0 ||
+      (nchunks > 0 && (!chunk_patch || !chunk_start))) {
+    set_error("rate_levels: bad ndim / ninstances / nlevels / work list");
+    return kBadArgument;
+  }
+  if (int64_t(ninstances) * nlevels >= (int64_t(1) << 31)) {
+    set_error("rate_levels: %d instances x %d levels exceed 2^31 keys", ninstances, nlevels);
+    return kTooLarge;
+  }
+  const double b0[3] = {b0x, b0y, b0z};
+  if (precision == 32)
+    return launch_rate_chunks<float>(static_cast<const float*>(state), static_cast<const PatchDesc*>(patches), npatches,
+                                     ndim, chunk_patch, chunk_start, nchunks, b0, gamma, keys, ninstances,
+                                     as_stream(stream), level_keys, nlevels);
+  return launch_rate_chunks<double>(static_cast<const double*>(state), static_cast<const PatchDesc*>(patches),
+                                    npatches, ndim, chunk_patch, chunk_start, nchunks, b0, gamma, keys, ninstances,
+                                    as_stream(stream), level_keys, nlevels);
+}
+
+int wb_finalize_dt_levels(const unsigned long long* keys, int ninstances, double cfl, double eta, double kappa,
+                          double gamma, const unsigned long long* level_keys, const double* inv_dx2_levels,
+                          int nlevels, double* time, const double* end, double* dt, int advance, void* stream) {
+  set_error("");
+  if (!ptrs_ok({keys, level_keys, inv_dx2_levels, dt}, "finalize_dt_levels")) return kBadArgument;
+  if (nlevels <= 0) {
+    set_error("finalize_dt_levels: nlevels must be positive");
+    return kBadArgument;
+  }
+  if ((end || advance) && !time) {
+    set_error("finalize_dt_levels: time is required with end or advance");
+    return kBadArgument;
+  }
+  return launch_finalize_dt(keys, ninstances, cfl, eta, kappa, gamma, nullptr, time, end, dt, advance,
+                            as_stream(stream), level_keys, inv_dx2_levels, nlevels);
 }
 
 int wb_copy_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream) {
@@ -414,6 +468,10 @@ static int face_flux_ops(int precision, const void* pool, const void* patches, c
     return launch_face_flux_ops<float>(static_cast<const float*>(pool), static_cast<const PatchDesc*>(patches),
                                        static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, reg,
                                        as_stream(stream));
+  if (precision == kMath32State64)
+    return launch_face_flux_ops<double, float>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
+                                               static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics,
+                                               reg, as_stream(stream));
   return launch_face_flux_ops<double>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
                                       static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, reg,
                                       as_stream(stream));

@@ -14,12 +14,38 @@ __global__ void init_keys_kernel(unsigned long long* keys) {
   keys[1] = double_to_key(__longlong_as_double(0x7ff0000000000000ll));
 }
 
-__global__ void init_keys_n_kernel(unsigned long long* keys, int n) {
+// Reduction identities of n instances' (max rate, min density) keys and, when
+// level_keys is given, of their per-level density minima (n x nlevels keys).
+__global__ void init_keys_n_kernel(unsigned long long* keys, int n, unsigned long long* level_keys, int nlevels) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
     keys[2 * i] = double_to_key(0.0);
     keys[2 * i + 1] = double_to_key(__longlong_as_double(0x7ff0000000000000ll));
   }
+  if (level_keys && i < n * nlevels) level_keys[i] = double_to_key(__longlong_as_double(0x7ff0000000000000ll));
+}
+
+// Where a rate block reduces: the instance's key pair and, optionally, the density-minimum
+// key of the patch's level. A patch whose instance or level lies outside the key arrays
+// is skipped (its block reduces nothing) and flagged in `error` (nullable).
+struct RateSlots {
+  unsigned long long* keys;        // [2 * ninstances]
+  int ninstances;
+  unsigned long long* level_keys;  // [ninstances * nlevels] or null
+  int nlevels;
+  unsigned* error;                 // nullable
+};
+
+__device__ __forceinline__ bool rate_slot(const PatchDesc& P, const RateSlots& r, unsigned long long** keys,
+                                          unsigned long long** level_min) {
+  const bool ok = P.instance >= 0 && P.instance < r.ninstances && (!r.level_keys || (P.level >= 0 && P.level < r.nlevels));
+  if (!ok) {
+    if (r.error && threadIdx.x == 0) atomicOr(r.error, 1u);
+    return false;
+  }
+  *keys = r.keys + 2 * P.instance;
+  *level_min = r.level_keys ? r.level_keys + P.instance * r.nlevels + P.level : nullptr;
+  return true;
 }
 
 constexpr unsigned kRateThreads = 256;  // threads of a rate block (8 rounds: 2048 cells)
@@ -29,9 +55,11 @@ template <typename S>
 __global__ void __launch_bounds__(kRateThreads) rate2d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
                                                     int npatches, const int* chunk_patch,
                                                     const int* chunk_start, double b0x, double b0y,
-                                                    double gamma, unsigned long long* keys) {
+                                                    double gamma, const RateSlots slots) {
   const int pi = chunk_patch[blockIdx.x];
   const PatchDesc P = patches[pi];
+  unsigned long long *keys, *level_min;
+  if (!rate_slot(P, slots, &keys, &level_min)) return;  // uniform over the block
   const int nx = P.n[0], ny = P.n[1];
   const S* src = pool + P.off;
   const int64_t pitch = P.pitch0, fs = P.fstride;
@@ -63,16 +91,18 @@ __global__ void __launch_bounds__(kRateThreads) rate2d_kernel(const S* __restric
     largest = rmax(largest, rate);
     smallest = rmin(smallest, r);
   }
-  block_reduce_keys(double(largest), double(smallest), keys + 2 * P.instance);
+  block_reduce_keys(double(largest), double(smallest), keys, level_min);
 }
 
 template <typename S>
 __global__ void __launch_bounds__(kRateThreads) rate3d_kernel(const S* __restrict__ pool, const PatchDesc* patches,
                                                     int npatches, const int* chunk_patch,
                                                     const int* chunk_start, double b0x, double b0y,
-                                                    double b0z, double gamma, unsigned long long* keys) {
+                                                    double b0z, double gamma, const RateSlots slots) {
   const int pi = chunk_patch[blockIdx.x];
   const PatchDesc P = patches[pi];
+  unsigned long long *keys, *level_min;
+  if (!rate_slot(P, slots, &keys, &level_min)) return;  // uniform over the block
   const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
   const S* src = pool + P.off;
   const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
@@ -116,7 +146,7 @@ __global__ void __launch_bounds__(kRateThreads) rate3d_kernel(const S* __restric
     largest = rmax(largest, rate);
     smallest = rmin(smallest, r);
   }
-  block_reduce_keys(double(largest), double(smallest), keys + 2 * P.instance);
+  block_reduce_keys(double(largest), double(smallest), keys, level_min);
 }
 
 // The work list of the rate kernels is derived from the patch table on the host and
@@ -124,34 +154,59 @@ __global__ void __launch_bounds__(kRateThreads) rate3d_kernel(const S* __restric
 template <typename S>
 int launch_rate_chunks(const S* state, const PatchDesc* patches, int npatches, int ndim, const int* chunk_patch,
                        const int* chunk_start, int nchunks, const double* b0, double gamma,
-                       unsigned long long* keys, int ninstances, cudaStream_t stream) {
-  init_keys_n_kernel<<<(ninstances + 255) / 256, 256, 0, stream>>>(keys, ninstances);
+                       unsigned long long* keys, int ninstances, cudaStream_t stream,
+                       unsigned long long* level_keys, int nlevels, unsigned* error) {
+  const int slots_n = level_keys ? max(ninstances, ninstances * nlevels) : ninstances;
+  init_keys_n_kernel<<<(slots_n + 255) / 256, 256, 0, stream>>>(keys, ninstances, level_keys, nlevels);
+  const RateSlots slots{keys, ninstances, level_keys, nlevels, error};
   if (nchunks > 0) {
     if (ndim == 2)
       rate2d_kernel<S><<<nchunks, kRateThreads, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
-                                                    gamma, keys);
+                                                    gamma, slots);
     else
       rate3d_kernel<S><<<nchunks, kRateThreads, 0, stream>>>(state, patches, npatches, chunk_patch, chunk_start, b0[0], b0[1],
-                                                    b0[2], gamma, keys);
+                                                    b0[2], gamma, slots);
   }
   return check_launch("rate");
 }
 
 template int launch_rate_chunks<float>(const float*, const PatchDesc*, int, int, const int*, const int*, int,
-                                       const double*, double, unsigned long long*, int, cudaStream_t);
+                                       const double*, double, unsigned long long*, int, cudaStream_t,
+                                       unsigned long long*, int, unsigned*);
 template int launch_rate_chunks<double>(const double*, const PatchDesc*, int, int, const int*, const int*, int,
-                                        const double*, double, unsigned long long*, int, cudaStream_t);
+                                        const double*, double, unsigned long long*, int, cudaStream_t,
+                                        unsigned long long*, int, unsigned*);
 
+// dt of instance i: cfl times the smaller of the fast-wave crossing time 1 / rate and the
+// explicit diffusion limit 0.5 / (D (dx^-2 + dy^-2 [+ dz^-2])), D = max(eta, (gamma - 1)
+// kappa / rho_min). With per-level keys the limit is taken level by level, each level's
+// smallest density with that level's spacing, as the reference takes it patch by patch
+// (carafe/mhd.py:942-960: patches of one level share the spacing, so the smallest
+// density of the level decides); without them, the instance's smallest density with its
+// finest spacing.
 __global__ void finalize_dt_kernel(const unsigned long long* keys, int n, double cfl, double eta, double kappa,
-                                   double gamma, const double* inv_dx2_sum, double* time, const double* end,
+                                   double gamma, const double* inv_dx2_sum, const unsigned long long* level_keys,
+                                   const double* inv_dx2_levels, int nlevels, double* time, const double* end,
                                    double* dt, int advance) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double rate = key_to_double(keys[2 * i]);
-  const double rho_min = key_to_double(keys[2 * i + 1]);
   double smallest = 1.0 / rate;
-  const double diffusivity = fmax(eta, (gamma - 1.0) * kappa / rho_min);
-  if (diffusivity > 0.0) smallest = fmin(smallest, 0.5 / (diffusivity * inv_dx2_sum[i]));
+  if (eta > 0.0 || kappa > 0.0) {
+    if (level_keys) {
+      for (int l = 0; l < nlevels; ++l) {
+        const double inv = inv_dx2_levels[i * nlevels + l];
+        if (!(inv > 0.0)) continue;  // no patch of the instance on this level
+        const double rho_min = key_to_double(level_keys[i * nlevels + l]);
+        const double diffusivity = fmax(eta, (gamma - 1.0) * kappa / rho_min);
+        if (diffusivity > 0.0) smallest = fmin(smallest, 0.5 / (diffusivity * inv));
+      }
+    } else {
+      const double rho_min = key_to_double(keys[2 * i + 1]);
+      const double diffusivity = fmax(eta, (gamma - 1.0) * kappa / rho_min);
+      if (diffusivity > 0.0) smallest = fmin(smallest, 0.5 / (diffusivity * inv_dx2_sum[i]));
+    }
+  }
   double step = cfl * smallest;
   if (end) {
     const double remaining = end[i] - time[i];
@@ -164,10 +219,12 @@ __global__ void finalize_dt_kernel(const unsigned long long* keys, int n, double
 
 int launch_finalize_dt(const unsigned long long* keys, int ninstances, double cfl, double eta, double kappa,
                        double gamma, const double* inv_dx2_sum, double* time, const double* end, double* dt,
-                       int advance_time, cudaStream_t stream) {
+                       int advance_time, cudaStream_t stream, const unsigned long long* level_keys,
+                       const double* inv_dx2_levels, int nlevels) {
   if (ninstances > 0)
     finalize_dt_kernel<<<(ninstances + 255) / 256, 256, 0, stream>>>(keys, ninstances, cfl, eta, kappa, gamma,
-                                                                     inv_dx2_sum, time, end, dt, advance_time);
+                                                                     inv_dx2_sum, level_keys, inv_dx2_levels,
+                                                                     nlevels, time, end, dt, advance_time);
   return check_launch("finalize_dt");
 }
 

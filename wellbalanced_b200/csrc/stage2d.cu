@@ -10,6 +10,8 @@
 //      (A -= dt E_z), with the Heun combine in stage 2 (carafe/mhd.py:889-927, 965-994).
 // The primitive variables and fluxes never reach HBM; each stage reads its input state
 // (and, in stage 2, the start state at the cell itself) and writes the new state once.
+#include <type_traits>
+
 #include "layout.cuh"
 #include "numerics.cuh"
 #include "stage.cuh"
@@ -17,23 +19,31 @@
 
 namespace wb {
 
-// Tile shapes (TX x TY cells) the 2D stage kernel is built for; the first of each precision
-// is the default and the only one with the non-ideal terms. The others are candidates of
-// the autotuner (more tiles for small patches, less halo overhead for large ones).
-template <typename S>
+// Tile shapes (TX x TY cells) the 2D stage kernel is built for, per (state type S,
+// arithmetic type R); the first of each is the default and the only one with the
+// non-ideal terms. The others are candidates of the autotuner (more tiles for small
+// patches, less halo overhead for large ones).
+template <typename S, typename R = S>
 struct Tile2D;
 
 template <>
-struct Tile2D<float> {
+struct Tile2D<float, float> {
   static constexpr int TX = 16, TY = 32;
   static constexpr int kShapes = 4;
   static constexpr int kShape[kShapes][2] = {{16, 32}, {8, 32}, {16, 16}, {32, 16}};
 };
 template <>
-struct Tile2D<double> {
+struct Tile2D<double, double> {
   static constexpr int TX = 8, TY = 32;
   static constexpr int kShapes = 3;
   static constexpr int kShape[kShapes][2] = {{8, 32}, {8, 16}, {16, 16}};
+};
+// float64 state, float32 arithmetic: the float32 shapes (shared memory holds float32)
+template <>
+struct Tile2D<double, float> {
+  static constexpr int TX = 16, TY = 32;
+  static constexpr int kShapes = 3;
+  static constexpr int kShape[kShapes][2] = {{16, 32}, {8, 32}, {16, 16}};
 };
 
 template <typename S>
@@ -65,34 +75,46 @@ __device__ __forceinline__ S temperature(const S* sP, int t) {
 constexpr int kThreads2D = 256;  // threads of a stage2d CTA
 
 // CTAs per SM the launch bounds hold the registers to: three 256-thread CTAs of float32
-// (80 registers a thread, 63 KB of shared memory each), two of float64.
-template <typename S>
+// (80 registers a thread, 63 KB of shared memory each), two of float64 and of the float64
+// state with float32 arithmetic (its stage input and Heun base are held in float64).
+template <typename S, typename R = S>
 struct Occupancy2D {
   static constexpr int kBlocks = sizeof(S) == 4 ? 3 : 2;
 };
 
-template <typename S, int LIM, bool PHYS, int TX, int TY>
-__global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_kernel(const StageArgs<S> a) {
-  using M = Math<S>;
+// S: the state's type (loads, the conserved and potential updates, the Heun combine);
+// R: the arithmetic of the reconstruction, HLLD and CT (float32 or float64). With a
+// float64 state and float32 arithmetic (S = double, R = float) the primitive variables
+// and face fields are formed in float64 from the float64 state (face fields from float64
+// differences of the potential; pressure in float64) and rounded to float32 for the face
+// work; the flux differences, the updates U -= dt div F and A -= dt E and the Heun combine
+// are float64.
+template <typename S, typename R, int LIM, bool PHYS, int TX, int TY>
+__global__ void __launch_bounds__(kThreads2D, (Occupancy2D<S, R>::kBlocks)) stage2d_kernel(const StageArgs<S> a) {
+  using M = Math<R>;
+  // phase 1 (cells -> primitive variables) in the state's type; a float64 state with
+  // float32 arithmetic takes float32-seeded float64 reciprocals there
+  using W = S;
+  using MW = typename std::conditional<std::is_same<S, R>::value, Math<S>, MathRefined>::type;
+  constexpr bool kMixed = !std::is_same<S, R>::value;
   constexpr int CX = TX + 4, CY = TY + 4, NC = CX * CY;
   constexpr int FX = TX + 1, FY = TY + 1, NF = FX * FY;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sP = reinterpret_cast<S*>(smem_raw);  // [8][NC] primitive variables
-  S* sBx = sP + 8 * NC;                     // [NC] x-face field at each cell's lower x-face
-  S* sBy = sBx + NC;                        // [NC] y-face field at each cell's lower y-face
-  S* sE = sBy + NC;                         // [NC] cell E_z
-  S* sFx = sE + NC;                         // [7][NF] x-face fluxes, face (fi, fj) at fi*FY + fj+1
-  S* sFy = sFx + 7 * NF;                    // [7][NF] y-face fluxes, face (fi, fj) at (fi+1)*FY + fj
+  R* sP = reinterpret_cast<R*>(smem_raw);  // [8][NC] primitive variables
+  R* sBx = sP + 8 * NC;                     // [NC] x-face field at each cell's lower x-face
+  R* sBy = sBx + NC;                        // [NC] y-face field at each cell's lower y-face
+  R* sE = sBy + NC;                         // [NC] cell E_z
+  R* sFx = sE + NC;                         // [7][NF] x-face fluxes, face (fi, fj) at fi*FY + fj+1
+  R* sFy = sFx + 7 * NF;                    // [7][NF] y-face fluxes, face (fi, fj) at (fi+1)*FY + fj
 
   const Tile tile = a.tiles[blockIdx.x];
   const PatchDesc P = a.patches[tile.patch];
   const int nx = P.n[0], ny = P.n[1];
   const int64_t pitch = P.pitch0, fs = P.fstride;
   const S* __restrict__ src = a.src + P.off;
-  const S dx = S(P.dx[0]), dy = S(P.dx[1]);
-  const S idx = M::inv(dx), idy = M::inv(dy);
-  const S b0x = S(a.b0[0]), b0y = S(a.b0[1]);
-  const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
+  const R dx = R(P.dx[0]), dy = R(P.dx[1]);
+  const R idx = M::inv(dx), idy = M::inv(dy);
+  const R gamma = R(a.gamma), inv_gm1 = R(a.inv_gm1);
   const int x0 = tile.x0, y0 = tile.y0;
   const int own_nx = nx + ((P.flags & kOwnLast0) ? 1 : 0);
   const int own_ny = ny + ((P.flags & kOwnLast1) ? 1 : 0);
@@ -111,48 +133,53 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
 
   // 1. cells and nodes -> primitive variables -------------------------------------
   unsigned bad = 0;
-  for (int t = threadIdx.x; t < NC; t += blockDim.x) {
-    const int li = t / CY, lj = t - (t / CY) * CY;
-    const int gi = x0 + li, gj = y0 + lj;  // haloed indices
-    S r = S(1), m0 = S(0), m1 = S(0), m2 = S(0), e = S(1), bz = S(0);
-    S bxl = S(0), bxh = S(0), byl = S(0), byh = S(0);
-    const bool valid = gi < nx + 4 && gj < ny + 4;
-    if (valid) {
-      const int64_t c = int64_t(gi) * pitch + gj;
-      r = src[c];
-      m0 = src[fs + c];
-      m1 = src[2 * fs + c];
-      m2 = src[3 * fs + c];
-      e = src[4 * fs + c];
-      bz = src[5 * fs + c];
-      const S* A = src + 6 * fs;
-      const S a00 = A[c], a01 = A[c + 1], a10 = A[c + pitch], a11 = A[c + pitch + 1];
-      bxl = M::div(a01 - a00, dy, idy) + b0x;
-      bxh = M::div(a11 - a10, dy, idy) + b0x;
-      byl = -M::div(a10 - a00, dx, idx) + b0y;
-      byh = -M::div(a11 - a01, dx, idx) + b0y;
+  {
+    const W wdx = W(P.dx[0]), wdy = W(P.dx[1]);
+    const W widx = MW::inv(wdx), widy = MW::inv(wdy);
+    const W b0x = W(a.b0[0]), b0y = W(a.b0[1]);
+    for (int t = threadIdx.x; t < NC; t += blockDim.x) {
+      const int li = t / CY, lj = t - (t / CY) * CY;
+      const int gi = x0 + li, gj = y0 + lj;  // haloed indices
+      W r = W(1), m0 = W(0), m1 = W(0), m2 = W(0), e = W(1), bz = W(0);
+      W bxl = W(0), bxh = W(0), byl = W(0), byh = W(0);
+      const bool valid = gi < nx + 4 && gj < ny + 4;
+      if (valid) {
+        const int64_t c = int64_t(gi) * pitch + gj;
+        r = src[c];
+        m0 = src[fs + c];
+        m1 = src[2 * fs + c];
+        m2 = src[3 * fs + c];
+        e = src[4 * fs + c];
+        bz = src[5 * fs + c];
+        const S* A = src + 6 * fs;
+        const W a00 = A[c], a01 = A[c + 1], a10 = A[c + pitch], a11 = A[c + pitch + 1];
+        bxl = MW::div(a01 - a00, wdy, widy) + b0x;
+        bxh = MW::div(a11 - a10, wdy, widy) + b0x;
+        byl = -MW::div(a10 - a00, wdx, widx) + b0y;
+        byh = -MW::div(a11 - a01, wdx, widx) + b0y;
+      }
+      const W ir = MW::inv(r);
+      const W u = MW::div(m0, r, ir), v = MW::div(m1, r, ir), w = MW::div(m2, r, ir);
+      const W bx = W(0.5) * (bxl + bxh), by = W(0.5) * (byl + byh);
+      W p = recover_pressure<W>(r, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
+      if (!valid) p = W(1);
+      sP[t] = R(r);
+      sP[NC + t] = R(u);
+      sP[2 * NC + t] = R(v);
+      sP[3 * NC + t] = R(w);
+      sP[4 * NC + t] = R(p);
+      sP[5 * NC + t] = R(bx);
+      sP[6 * NC + t] = R(by);
+      sP[7 * NC + t] = R(bz);
+      sBx[t] = R(bxl);
+      sBy[t] = R(byl);
+      sE[t] = R(bx * v - by * u);
+      // the tile's own cells
+      const int ci = li - 2, cj = lj - 2;
+      if (valid && ci >= 0 && ci < TX && cj >= 0 && cj < TY && x0 + ci < nx && y0 + cj < ny &&
+          bad_cell(r, u, v, w, p, bx, by, bz))
+        ++bad;
     }
-    const S ir = M::inv(r);
-    const S u = M::div(m0, r, ir), v = M::div(m1, r, ir), w = M::div(m2, r, ir);
-    const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh);
-    S p = recover_pressure<S>(r, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
-    if (!valid) p = S(1);
-    sP[t] = r;
-    sP[NC + t] = u;
-    sP[2 * NC + t] = v;
-    sP[3 * NC + t] = w;
-    sP[4 * NC + t] = p;
-    sP[5 * NC + t] = bx;
-    sP[6 * NC + t] = by;
-    sP[7 * NC + t] = bz;
-    sBx[t] = bxl;
-    sBy[t] = byl;
-    sE[t] = bx * v - by * u;
-    // the tile's own cells
-    const int ci = li - 2, cj = lj - 2;
-    if (valid && ci >= 0 && ci < TX && cj >= 0 && cj < TY && x0 + ci < nx && y0 + cj < ny &&
-        bad_cell(r, u, v, w, p, bx, by, bz))
-      ++bad;
   }
   if (bad) atomicAdd(a.bad, (unsigned long long)bad);
   __syncthreads();
@@ -162,7 +189,7 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
     const bool xface = t < NF;
     const int u = xface ? t : t - NF;
     int fi, fj, base, step;
-    S bn;
+    R bn;
     int comp[7];
     if (xface) {
       fi = u / FY;           // face fi: between cells fi-1 and fi (tile-relative)
@@ -179,43 +206,43 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
       bn = sBy[(fi + 2) * CY + fj + 2];
       comp[0] = 0; comp[1] = 2; comp[2] = 1; comp[3] = 3; comp[4] = 4; comp[5] = 5; comp[6] = 7;
     }
-    S q0[7], q1[7], q2[7], q3[7];
+    R q0[7], q1[7], q2[7], q3[7];
 #pragma unroll
     for (int c = 0; c < 7; ++c) {
-      const S* row = sP + comp[c] * NC + base;
+      const R* row = sP + comp[c] * NC + base;
       q0[c] = row[0];
       q1[c] = row[step];
       q2[c] = row[2 * step];
       q3[c] = row[3 * step];
     }
-    S L[7], Rt[7], F[7];
+    R L[7], Rt[7], F[7];
     reconstruct<LIM>(q0, q1, q2, q3, L, Rt);
     hlld_flux(L, Rt, bn, gamma, inv_gm1, F);
     if (PHYS) {
       // the cells beside the face (local indices) and the step to their transverse neighbours
       const int ca = base + step, cb = base + 2 * step, across = xface ? 1 : CY;
-      const S ht = xface ? dy : dx, iht = xface ? idy : idx;  // spacing across the face's normal
-      S slope_a = S(0), slope_b = S(0);
+      const R ht = xface ? dy : dx, iht = xface ? idy : idx;  // spacing across the face's normal
+      R slope_a = R(0), slope_b = R(0);
       if (a.kappa_par != 0.0 || a.kappa_perp != 0.0) {
         // MC-limited transverse temperature slopes of the two cells
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
           const int c = side == 0 ? ca : cb;
-          const S t0 = temperature<S, NC>(sP, c - across), t1 = temperature<S, NC>(sP, c),
-                  t2 = temperature<S, NC>(sP, c + across);
+          const R t0 = temperature<R, NC>(sP, c - across), t1 = temperature<R, NC>(sP, c),
+                  t2 = temperature<R, NC>(sP, c + across);
           (side == 0 ? slope_a : slope_b) = limited_slope<2>(M::div(t2 - t1, ht, iht), M::div(t1 - t0, ht, iht));
         }
       }
-      S jz_0 = S(0), jz_1 = S(0);
+      R jz_0 = R(0), jz_1 = R(0);
       if (a.eta != 0.0) {
-        jz_0 = node_current<S, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy);
-        jz_1 = xface ? node_current<S, CY>(sBx, sBy, fi, fj + 1, dx, idx, dy, idy)
-                     : node_current<S, CY>(sBx, sBy, fi + 1, fj, dx, idx, dy, idy);
+        jz_0 = node_current<R, CY>(sBx, sBy, fi, fj, dx, idx, dy, idy);
+        jz_1 = xface ? node_current<R, CY>(sBx, sBy, fi, fj + 1, dx, idx, dy, idy)
+                     : node_current<R, CY>(sBx, sBy, fi + 1, fj, dx, idx, dy, idy);
       }
       const int bt_row = xface ? 6 : 5;  // the in-plane tangential field
-      nonideal_face_terms(xface, bn, temperature<S, NC>(sP, ca), temperature<S, NC>(sP, cb), slope_a, slope_b,
+      nonideal_face_terms(xface, bn, temperature<R, NC>(sP, ca), temperature<R, NC>(sP, cb), slope_a, slope_b,
                           sP[bt_row * NC + ca], sP[bt_row * NC + cb], sP[7 * NC + ca], sP[7 * NC + cb], jz_0, jz_1,
-                          xface ? dx : dy, xface ? idx : idy, S(a.eta), S(a.kappa_par), S(a.kappa_perp), F);
+                          xface ? dx : dy, xface ? idx : idy, R(a.eta), R(a.kappa_par), R(a.kappa_perp), F);
     }
     // walls: nothing but the pressure crosses (carafe/mhd.py:874-886)
     bool wall;
@@ -227,13 +254,13 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
       wall = ((P.flags & kWallLo1) && g == 0) || ((P.flags & kWallHi1) && g == ny);
     }
     if (wall) {
-      F[0] = S(0);
-      F[2] = S(0);
-      F[3] = S(0);
-      F[4] = S(0);
-      F[6] = S(0);
+      F[0] = R(0);
+      F[2] = R(0);
+      F[3] = R(0);
+      F[4] = R(0);
+      F[6] = R(0);
     }
-    S* out = xface ? sFx + fi * FY + (fj + 1) : sFy + (fi + 1) * FY + fj;
+    R* out = xface ? sFx + fi * FY + (fj + 1) : sFy + (fi + 1) * FY + fj;
 #pragma unroll
     for (int c = 0; c < 7; ++c) out[c * NF] = F[c];
   }
@@ -241,6 +268,8 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
   // input and, in stage 2, the Heun base), loaded before the barrier so that their
   // latency overlaps the wait
   const S dt = S(a.dt[P.instance]);
+  // the inverse spacings of the float64 flux differences (mixed precision only)
+  const S sidx = kMixed ? S(1) / S(P.dx[0]) : S(0), sidy = kMixed ? S(1) / S(P.dx[1]) : S(0);
   const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
   S* __restrict__ dst = a.dst + P.off;
   constexpr int NIT = (TX * TY + kThreads2D - 1) / kThreads2D;  // phase-3 rounds of the threads
@@ -271,16 +300,16 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
     const int ni = t / TY, nj = t % TY;
     const int gx = x0 + ni, gy = y0 + nj;  // interior node / cell indices
     if (gx < own_nx && gy < own_ny) {
-      S ez = ct_node(sFx[5 * NF + ni * FY + nj], sFx[5 * NF + ni * FY + nj + 1], sFx[ni * FY + nj],
+      R ez = ct_node(sFx[5 * NF + ni * FY + nj], sFx[5 * NF + ni * FY + nj + 1], sFx[ni * FY + nj],
                      sFx[ni * FY + nj + 1], sFy[5 * NF + ni * FY + nj], sFy[5 * NF + (ni + 1) * FY + nj],
                      sFy[ni * FY + nj], sFy[(ni + 1) * FY + nj], sE[(ni + 1) * CY + nj + 1],
                      sE[(ni + 2) * CY + nj + 1], sE[(ni + 1) * CY + nj + 2], sE[(ni + 2) * CY + nj + 2]);
-      if (PHYS && a.eta != 0.0) ez += S(a.eta) * node_current<S, CY>(sBx, sBy, ni, nj, dx, idx, dy, idy);
+      if (PHYS && a.eta != 0.0) ez += R(a.eta) * node_current<R, CY>(sBx, sBy, ni, nj, dx, idx, dy, idy);
       const bool wall = ((P.flags & kWallLo0) && gx == 0) || ((P.flags & kWallHi0) && gx == nx) ||
                         ((P.flags & kWallLo1) && gy == 0) || ((P.flags & kWallHi1) && gy == ny);
-      if (wall) ez = S(0);
+      if (wall) ez = R(0);
       const int64_t node = 6 * fs + int64_t(gx + 2) * pitch + (gy + 2);
-      S value = in_node[it] - dt * ez;
+      S value = in_node[it] - dt * S(ez);
       if (base_state) value = (value + base_node[it]) * S(0.5);
       dst[node] = value;
     }
@@ -290,8 +319,15 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
       const int yrow[6] = {0, 2, 1, 3, 4, 6};
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        const S div = M::div(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1], dx, idx) +
-                      M::div(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj], dy, idy);
+        S div;
+        if constexpr (kMixed) {
+          // float64 flux differences of the float32 fluxes
+          div = (S(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1]) - S(sFx[xrow[q] * NF + ni * FY + nj + 1])) * sidx +
+                (S(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1]) - S(sFy[yrow[q] * NF + (ni + 1) * FY + nj])) * sidy;
+        } else {
+          div = M::div(sFx[xrow[q] * NF + (ni + 1) * FY + nj + 1] - sFx[xrow[q] * NF + ni * FY + nj + 1], dx, idx) +
+                M::div(sFy[yrow[q] * NF + (ni + 1) * FY + nj + 1] - sFy[yrow[q] * NF + (ni + 1) * FY + nj], dy, idy);
+        }
         S value = in_cell[it][q] - dt * div;
         if (PHYS) {
           // gravity: rho g on the momentum, m . g on the energy, from the stage's input
@@ -324,23 +360,24 @@ __global__ void __launch_bounds__(kThreads2D, Occupancy2D<S>::kBlocks) stage2d_k
   }
 }
 
-template <typename S, int LIM, bool PHYS, int TX, int TY>
+template <typename S, typename R, int LIM, bool PHYS, int TX, int TY>
 void launch_shape(const StageArgs<S>& args, int ntiles, cudaStream_t stream) {
   constexpr int NC = (TX + 4) * (TY + 4), NF = (TX + 1) * (TY + 1);
-  const size_t smem = sizeof(S) * (11 * NC + 14 * NF);
-  cudaFuncSetAttribute(stage2d_kernel<S, LIM, PHYS, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  stage2d_kernel<S, LIM, PHYS, TX, TY><<<ntiles, kThreads2D, smem, stream>>>(args);
+  const size_t smem = sizeof(R) * (11 * NC + 14 * NF);
+  cudaFuncSetAttribute(stage2d_kernel<S, R, LIM, PHYS, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       int(smem));
+  stage2d_kernel<S, R, LIM, PHYS, TX, TY><<<ntiles, kThreads2D, smem, stream>>>(args);
 }
 
 // One limiter: the default shape (ideal or non-ideal) or one of the other shapes (ideal).
-template <typename S, int LIM>
+template <typename S, typename R, int LIM>
 int launch_limiter(const StageArgs<S>& args, int ntiles, bool phys, int shape, cudaStream_t stream) {
-  using T = Tile2D<S>;
+  using T = Tile2D<S, R>;
   if (shape == 0) {
     if (phys)
-      launch_shape<S, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+      launch_shape<S, R, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
     else
-      launch_shape<S, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+      launch_shape<S, R, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
     return kOk;
   }
   if (phys) {
@@ -348,21 +385,23 @@ int launch_limiter(const StageArgs<S>& args, int ntiles, bool phys, int shape, c
     return kBadArgument;
   }
   switch (shape) {
-    case 1: launch_shape<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream); break;
-    case 2: launch_shape<S, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream); break;
+    case 1: launch_shape<S, R, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream); break;
+    case 2: launch_shape<S, R, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream); break;
     default:
-      if constexpr (T::kShapes > 3) launch_shape<S, LIM, false, T::kShape[3][0], T::kShape[3][1]>(args, ntiles, stream);
+      if constexpr (T::kShapes > 3)
+        launch_shape<S, R, LIM, false, T::kShape[3][0], T::kShape[3][1]>(args, ntiles, stream);
       break;
   }
   return kOk;
 }
 
-template <typename S>
+template <typename S, typename R>
 int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, int tx, int ty, cudaStream_t stream) {
   if (ntiles <= 0) return kOk;
+  using T = Tile2D<S, R>;
   int shape = -1;
-  for (int i = 0; i < Tile2D<S>::kShapes; ++i)
-    if (Tile2D<S>::kShape[i][0] == tx && Tile2D<S>::kShape[i][1] == ty) shape = i;
+  for (int i = 0; i < T::kShapes; ++i)
+    if (T::kShape[i][0] == tx && T::kShape[i][1] == ty) shape = i;
   if (shape < 0) {
     set_error("stage2d: no %dx%d tile shape for this precision", tx, ty);
     return kBadArgument;
@@ -371,10 +410,10 @@ int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, int tx, in
                     args.gravity[1] != 0.0;
   int status;
   switch (limiter) {
-    case 0: status = launch_limiter<S, 0>(args, ntiles, phys, shape, stream); break;
-    case 1: status = launch_limiter<S, 1>(args, ntiles, phys, shape, stream); break;
-    case 2: status = launch_limiter<S, 2>(args, ntiles, phys, shape, stream); break;
-    case 3: status = launch_limiter<S, 3>(args, ntiles, phys, shape, stream); break;
+    case 0: status = launch_limiter<S, R, 0>(args, ntiles, phys, shape, stream); break;
+    case 1: status = launch_limiter<S, R, 1>(args, ntiles, phys, shape, stream); break;
+    case 2: status = launch_limiter<S, R, 2>(args, ntiles, phys, shape, stream); break;
+    case 3: status = launch_limiter<S, R, 3>(args, ntiles, phys, shape, stream); break;
     default:
       set_error("limiter code %d is not one of 0..3", limiter);
       return kBadArgument;
@@ -383,21 +422,31 @@ int launch_stage2d(const StageArgs<S>& args, int ntiles, int limiter, int tx, in
   return check_launch("stage2d");
 }
 
-template int launch_stage2d<float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
-template int launch_stage2d<double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+template int launch_stage2d<float, float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
+template int launch_stage2d<double, double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+template int launch_stage2d<double, float>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
 
-int tile_shapes_2d(int fp64, int* shapes, int max) {
-  const int count = fp64 ? Tile2D<double>::kShapes : Tile2D<float>::kShapes;
-  for (int i = 0; i < count && i < max; ++i) {
-    shapes[2 * i] = fp64 ? Tile2D<double>::kShape[i][0] : Tile2D<float>::kShape[i][0];
-    shapes[2 * i + 1] = fp64 ? Tile2D<double>::kShape[i][1] : Tile2D<float>::kShape[i][1];
+template <typename T>
+static int copy_shapes(int* shapes, int max) {
+  for (int i = 0; i < T::kShapes && i < max; ++i) {
+    shapes[2 * i] = T::kShape[i][0];
+    shapes[2 * i + 1] = T::kShape[i][1];
   }
-  return count;
+  return T::kShapes;
 }
 
-void tile_shape_2d(int fp64, int* tx, int* ty) {
-  *tx = fp64 ? Tile2D<double>::TX : Tile2D<float>::TX;
-  *ty = fp64 ? Tile2D<double>::TY : Tile2D<float>::TY;
+int tile_shapes_2d(int mode, int* shapes, int max) {
+  if (mode == kMath32State64) return copy_shapes<Tile2D<double, float>>(shapes, max);
+  return mode ? copy_shapes<Tile2D<double>>(shapes, max) : copy_shapes<Tile2D<float>>(shapes, max);
+}
+
+void tile_shape_2d(int mode, int* tx, int* ty) {
+  if (mode == kMath32State64) {
+    *tx = Tile2D<double, float>::TX, *ty = Tile2D<double, float>::TY;
+    return;
+  }
+  *tx = mode ? Tile2D<double>::TX : Tile2D<float>::TX;
+  *ty = mode ? Tile2D<double>::TY : Tile2D<float>::TY;
 }
 
 }  // namespace wb

@@ -27,6 +27,8 @@
 // on the edges around its faces, adds eta (J x B) to the energy flux of its x-, y- and
 // z-faces and hands eta J of its column's three edges to C (E += eta J); C adds rho g and
 // m . g to the cells.
+#include <type_traits>
+
 #include "layout.cuh"
 #include "numerics.cuh"
 #include "stage.cuh"
@@ -38,7 +40,9 @@ namespace wb {
 // with the non-ideal terms); the others are candidates of the autotuner: a 8 x 16 tile
 // needs half the shared memory, so twice the CTAs share an SM, at more halo work per cell;
 // a 16 x 32 tile (float32 only: 191 KB) has less halo work per cell and one CTA per SM.
-template <typename S>
+// R is the arithmetic type (shared memory holds R): float32 arithmetic on a float64
+// state takes the float32 shapes.
+template <typename S, typename R = S>
 struct Tile3D {
   static constexpr int TY = 16, TZ = 16;
   static constexpr int kShapes = 2;
@@ -46,7 +50,14 @@ struct Tile3D {
 };
 
 template <>
-struct Tile3D<float> {
+struct Tile3D<float, float> {
+  static constexpr int TY = 16, TZ = 16;
+  static constexpr int kShapes = 3;
+  static constexpr int kShape[3][2] = {{16, 16}, {8, 16}, {16, 32}};
+};
+
+template <>
+struct Tile3D<double, float> {
   static constexpr int TY = 16, TZ = 16;
   static constexpr int kShapes = 3;
   static constexpr int kShape[3][2] = {{16, 16}, {8, 16}, {16, 32}};
@@ -96,30 +107,38 @@ __device__ __forceinline__ int face_slot(int plane) {
   return PHYS ? (plane + 6) % 3 : (plane + 4) & 1;  // plane >= -3
 }
 
-template <typename S, int LIM, bool PHYS, int TY, int TZ>
-__global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY, TZ>::kBlocks))
+// S: the state's type (loads, the conserved and potential updates, the Heun combine);
+// R: the arithmetic of the reconstruction, HLLD and CT. With a float64 state and float32
+// arithmetic (S = double, R = float) phase A forms the primitive variables and face fields
+// in float64 from the float64 state (face fields from float64 differences of the edge
+// potential, pressure in float64) and rounds them to float32 for the face work; phase C
+// takes float64 flux differences and updates U, A and the Heun combine in float64.
+template <typename S, typename R, int LIM, bool PHYS, int TY, int TZ>
+__global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY, TZ>::kBlocks))
     stage3d_kernel(const StageArgs<S> a) {
-  using M = Math<S>;
+  using M = Math<R>;
+  using W = S;  // phase A's arithmetic: the state's type
+  using MW = typename std::conditional<std::is_same<S, R>::value, Math<S>, MathRefined>::type;
+  constexpr bool kMixed = !std::is_same<S, R>::value;
   constexpr int RZ = TZ + 4, NR = (TY + 4) * (TZ + 4);  // plane region j, k in [-2, T+2)
   constexpr int GZ = TZ + 1, G = (TY + 1) * (TZ + 1);    // face / column grids
   constexpr int NCORE = TY * TZ;
   constexpr int NB = face_slots<PHYS>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  S* sP = reinterpret_cast<S*>(smem_raw);  // [2 slots][8][NR] primitive variables
-  S* sBn = sP + 2 * 8 * NR;                 // [NB slots][3][NR] field at each cell's lower faces
-  S* sEc = sBn + NB * 3 * NR;               // [4 slots][3][G] cell E_x, E_y, E_z
-  S* sYZ = sEc + 4 * 3 * G;                 // [3 slots][2 dirs][7][G] y- and z-face fluxes
-  S* sX = sYZ + 3 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
+  R* sP = reinterpret_cast<R*>(smem_raw);  // [2 slots][8][NR] primitive variables
+  R* sBn = sP + 2 * 8 * NR;                 // [NB slots][3][NR] field at each cell's lower faces
+  R* sEc = sBn + NB * 3 * NR;               // [4 slots][3][G] cell E_x, E_y, E_z
+  R* sYZ = sEc + 4 * 3 * G;                 // [3 slots][2 dirs][7][G] y- and z-face fluxes
+  R* sX = sYZ + 3 * 2 * 7 * G;              // [3][G] x-face mass, B_y and B_z fluxes
 
   const Tile tile = a.tiles[blockIdx.x];
   const PatchDesc P = a.patches[tile.patch];
   const int nx = P.n[0], ny = P.n[1], nz = P.n[2];
   const int64_t p0 = P.pitch0, p1 = P.pitch1, fs = P.fstride;
   const S* __restrict__ src = a.src + P.off;
-  const S dx = S(P.dx[0]), dy = S(P.dx[1]), dz = S(P.dx[2]);
-  const S idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
-  const S b0x = S(a.b0[0]), b0y = S(a.b0[1]), b0z = S(a.b0[2]);
-  const S gamma = S(a.gamma), inv_gm1 = S(a.inv_gm1);
+  const R dx = R(P.dx[0]), dy = R(P.dx[1]), dz = R(P.dx[2]);
+  const R idx = M::inv(dx), idy = M::inv(dy), idz = M::inv(dz);
+  const R gamma = R(a.gamma), inv_gm1 = R(a.inv_gm1);
   const int x0 = tile.x0, y0 = tile.y0, z0 = tile.z0;
   const int own_nx = nx + ((P.flags & kOwnLast0) ? 1 : 0);
   const int own_ny = ny + ((P.flags & kOwnLast1) ? 1 : 0);
@@ -157,32 +176,32 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
   const int y_g = yj * GZ + (yk + 1);
   const int z_g = (zj + 1) * GZ + zk;
 
-  S q[3][7];    // x-stencil of the column: planes p-1 .. p+1 (x-frame rows)
-  S slope[7];   // limited x-slope of plane p-1 (computed one plane earlier)
+  R q[3][7];    // x-stencil of the column: planes p-1 .. p+1 (x-frame rows)
+  R slope[7];   // limited x-slope of plane p-1 (computed one plane earlier)
 #pragma unroll
   for (int s = 0; s < 3; ++s)
 #pragma unroll
-    for (int c = 0; c < 7; ++c) q[s][c] = S(1);
+    for (int c = 0; c < 7; ++c) q[s][c] = R(1);
 #pragma unroll
-  for (int c = 0; c < 7; ++c) slope[c] = S(0);
-  S fprev[5] = {S(0), S(0), S(0), S(0), S(0)};
-  S fnow[5] = {S(0), S(0), S(0), S(0), S(0)};
-  S ejx = S(0), ejy = S(0), ejz = S(0);  // eta J on the column's edges (PHYS)
+  for (int c = 0; c < 7; ++c) slope[c] = R(0);
+  R fprev[5] = {R(0), R(0), R(0), R(0), R(0)};
+  R fnow[5] = {R(0), R(0), R(0), R(0), R(0)};
+  R ejx = R(0), ejy = R(0), ejz = R(0);  // eta J on the column's edges (PHYS)
   // PHYS: the field at the lower `axis`-face of cell (plane, j, k) of the tile, and the
   // current J_c = d_a B_b - d_b B_a ((c, a, b) cyclic) on the c-edge whose lower corner
   // is that cell (carafe/mhd3d.py:579-590); planes p-1 .. p+1 are held during B2
-  auto face = [&](int plane, int axis, int j, int k) -> S {
+  auto face = [&](int plane, int axis, int j, int k) -> R {
     return sBn[(face_slot<PHYS>(plane) * 3 + axis) * NR + (j + 2) * RZ + (k + 2)];
   };
-  auto jx_at = [&](int plane, int j, int k) -> S {
+  auto jx_at = [&](int plane, int j, int k) -> R {
     return M::div(face(plane, 2, j, k) - face(plane, 2, j - 1, k), dy, idy) -
            M::div(face(plane, 1, j, k) - face(plane, 1, j, k - 1), dz, idz);
   };
-  auto jy_at = [&](int plane, int j, int k) -> S {
+  auto jy_at = [&](int plane, int j, int k) -> R {
     return M::div(face(plane, 0, j, k) - face(plane, 0, j, k - 1), dz, idz) -
            M::div(face(plane, 2, j, k) - face(plane - 1, 2, j, k), dx, idx);
   };
-  auto jz_at = [&](int plane, int j, int k) -> S {
+  auto jz_at = [&](int plane, int j, int k) -> R {
     return M::div(face(plane, 1, j, k) - face(plane - 1, 1, j, k), dx, idx) -
            M::div(face(plane, 0, j, k) - face(plane, 0, j - 1, k), dy, idy);
   };
@@ -190,6 +209,13 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
   const S* __restrict__ base_state = a.base ? a.base + P.off : nullptr;
   S* __restrict__ dst = a.dst + P.off;
   unsigned bad = 0;
+  // phase A's spacings and mean field in the state's type
+  const W wdx = W(P.dx[0]), wdy = W(P.dx[1]), wdz = W(P.dx[2]);
+  const W widx = MW::inv(wdx), widy = MW::inv(wdy), widz = MW::inv(wdz);
+  const W b0x = W(a.b0[0]), b0y = W(a.b0[1]), b0z = W(a.b0[2]);
+  // the inverse spacings of the float64 flux differences (mixed precision only)
+  const S sidx = kMixed ? S(1) / S(P.dx[0]) : S(0), sidy = kMixed ? S(1) / S(P.dx[1]) : S(0),
+          sidz = kMixed ? S(1) / S(P.dx[2]) : S(0);
 
   for (int p = x0 - 3; p <= xe; ++p) {
     // prefetch into L2 what phase C of the next plane reads from global memory: the
@@ -208,15 +234,15 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
       const int c = p + 1;
       const int slot = (c + 4) & 1;
       const int slot4 = (c + 8) & 3;
-      S* P8 = sP + slot * 8 * NR;
-      S* B3 = sBn + (PHYS ? face_slot<PHYS>(c) : slot) * 3 * NR;
-      S* E3 = sEc + slot4 * 3 * G;
+      R* P8 = sP + slot * 8 * NR;
+      R* B3 = sBn + (PHYS ? face_slot<PHYS>(c) : slot) * 3 * NR;
+      R* E3 = sEc + slot4 * 3 * G;
       const int I = c + kHalo;
       for (int r = tid; r < NR; r += threads3d<TY, TZ>()) {
         const int j = r / RZ - 2, k = r % RZ - 2;
         const int J = y0 + j + kHalo, K = z0 + k + kHalo;
-        S rho = S(1), m0 = S(0), m1 = S(0), m2 = S(0), e = S(1);
-        S bxl = S(0), bxh = S(0), byl = S(0), byh = S(0), bzl = S(0), bzh = S(0);
+        W rho = W(1), m0 = W(0), m1 = W(0), m2 = W(0), e = W(1);
+        W bxl = W(0), bxh = W(0), byl = W(0), byh = W(0), bzl = W(0), bzh = W(0);
         const bool valid = J < ny + 4 && K < nz + 4 && I < nx + 4;
         if (valid) {
           const int64_t o = int64_t(I) * p0 + int64_t(J) * p1 + K;
@@ -229,36 +255,36 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
           const S* Ay = src + 6 * fs;
           const S* Az = src + 7 * fs;
           // x-faces at nodes I and I+1: dA_z/dy - dA_y/dz + B0x
-          bxl = M::div(Az[o + p1] - Az[o], dy, idy) - M::div(Ay[o + 1] - Ay[o], dz, idz) + b0x;
-          bxh = M::div(Az[o + p0 + p1] - Az[o + p0], dy, idy) - M::div(Ay[o + p0 + 1] - Ay[o + p0], dz, idz) + b0x;
+          bxl = MW::div(Az[o + p1] - Az[o], wdy, widy) - MW::div(Ay[o + 1] - Ay[o], wdz, widz) + b0x;
+          bxh = MW::div(Az[o + p0 + p1] - Az[o + p0], wdy, widy) - MW::div(Ay[o + p0 + 1] - Ay[o + p0], wdz, widz) + b0x;
           // y-faces at nodes J and J+1: dA_x/dz - dA_z/dx + B0y
-          byl = M::div(Ax[o + 1] - Ax[o], dz, idz) - M::div(Az[o + p0] - Az[o], dx, idx) + b0y;
-          byh = M::div(Ax[o + p1 + 1] - Ax[o + p1], dz, idz) - M::div(Az[o + p1 + p0] - Az[o + p1], dx, idx) + b0y;
+          byl = MW::div(Ax[o + 1] - Ax[o], wdz, widz) - MW::div(Az[o + p0] - Az[o], wdx, widx) + b0y;
+          byh = MW::div(Ax[o + p1 + 1] - Ax[o + p1], wdz, widz) - MW::div(Az[o + p1 + p0] - Az[o + p1], wdx, widx) + b0y;
           // z-faces at nodes K and K+1: dA_y/dx - dA_x/dy + B0z
-          bzl = M::div(Ay[o + p0] - Ay[o], dx, idx) - M::div(Ax[o + p1] - Ax[o], dy, idy) + b0z;
-          bzh = M::div(Ay[o + p0 + 1] - Ay[o + 1], dx, idx) - M::div(Ax[o + p1 + 1] - Ax[o + 1], dy, idy) + b0z;
+          bzl = MW::div(Ay[o + p0] - Ay[o], wdx, widx) - MW::div(Ax[o + p1] - Ax[o], wdy, widy) + b0z;
+          bzh = MW::div(Ay[o + p0 + 1] - Ay[o + 1], wdx, widx) - MW::div(Ax[o + p1 + 1] - Ax[o + 1], wdy, widy) + b0z;
         }
-        const S irho = M::inv(rho);
-        const S u = M::div(m0, rho, irho), v = M::div(m1, rho, irho), w = M::div(m2, rho, irho);
-        const S bx = S(0.5) * (bxl + bxh), by = S(0.5) * (byl + byh), bz = S(0.5) * (bzl + bzh);
-        S pr = recover_pressure<S>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
-        if (!valid) pr = S(1);
-        P8[r] = rho;
-        P8[NR + r] = u;
-        P8[2 * NR + r] = v;
-        P8[3 * NR + r] = w;
-        P8[4 * NR + r] = pr;
-        P8[5 * NR + r] = bx;
-        P8[6 * NR + r] = by;
-        P8[7 * NR + r] = bz;
-        B3[r] = bxl;
-        B3[NR + r] = byl;
-        B3[2 * NR + r] = bzl;
+        const W irho = MW::inv(rho);
+        const W u = MW::div(m0, rho, irho), v = MW::div(m1, rho, irho), w = MW::div(m2, rho, irho);
+        const W bx = W(0.5) * (bxl + bxh), by = W(0.5) * (byl + byh), bz = W(0.5) * (bzl + bzh);
+        W pr = recover_pressure<W>(rho, m0, m1, m2, e, bx, by, bz, u, v, w, a.gamma);
+        if (!valid) pr = W(1);
+        P8[r] = R(rho);
+        P8[NR + r] = R(u);
+        P8[2 * NR + r] = R(v);
+        P8[3 * NR + r] = R(w);
+        P8[4 * NR + r] = R(pr);
+        P8[5 * NR + r] = R(bx);
+        P8[6 * NR + r] = R(by);
+        P8[7 * NR + r] = R(bz);
+        B3[r] = R(bxl);
+        B3[NR + r] = R(byl);
+        B3[2 * NR + r] = R(bzl);
         if (j >= -1 && j < TY && k >= -1 && k < TZ) {
           const int g = (j + 1) * GZ + (k + 1);
-          E3[g] = by * w - bz * v;          // E_x
-          E3[G + g] = bz * u - bx * w;      // E_y
-          E3[2 * G + g] = bx * v - by * u;  // E_z
+          E3[g] = R(by * w - bz * v);          // E_x
+          E3[G + g] = R(bz * u - bx * w);      // E_y
+          E3[2 * G + g] = R(bx * v - by * u);  // E_z
         }
         if (valid && c >= x0 && c < xe && j >= 0 && j < TY && k >= 0 && k < TZ && y0 + j < ny &&
             z0 + k < nz && bad3(rho, u, v, w, pr, bx, by, bz))
@@ -269,26 +295,26 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
     // the same barrier interval as the loads of plane p + 1 ------------------------------
     {
       const int slot = (p + 4) & 1, slot3 = (p + 6) % 3;
-      const S* Pp = sP + slot * 8 * NR;
-      const S* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : slot) * 3 * NR;
+      const R* Pp = sP + slot * 8 * NR;
+      const R* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : slot) * 3 * NR;
       const bool need_yz = p >= x0 - 1 && (p < xe || xn > xe);
       if (need_yz) {
-        S* Y7 = sYZ + (slot3 * 2 + 0) * 7 * G;
-        S* Z7 = sYZ + (slot3 * 2 + 1) * 7 * G;
+        R* Y7 = sYZ + (slot3 * 2 + 0) * 7 * G;
+        R* Z7 = sYZ + (slot3 * 2 + 1) * 7 * G;
         {
           // y-face between cells (yj-1, yk) and (yj, yk): frame (y, z, x)
           const int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
           const int r0 = (yj - 2 + 2) * RZ + (yk + 2);
-          S a0[7], a1[7], a2[7], a3[7];
+          R a0[7], a1[7], a2[7], a3[7];
 #pragma unroll
           for (int cc = 0; cc < 7; ++cc) {
-            const S* row = Pp + yrow[cc] * NR + r0;
+            const R* row = Pp + yrow[cc] * NR + r0;
             a0[cc] = row[0];
             a1[cc] = row[RZ];
             a2[cc] = row[2 * RZ];
             a3[cc] = row[3 * RZ];
           }
-          S L[7], Rt[7], F[7];
+          R L[7], Rt[7], F[7];
           reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
           hlld_flux(L, Rt, Bp[NR + (yj + 2) * RZ + (yk + 2)], gamma, inv_gm1, F);
 #pragma unroll
@@ -298,16 +324,16 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
           // z-face between cells (zj, zk-1) and (zj, zk): frame (z, x, y)
           const int zrow[7] = {0, 3, 1, 2, 4, 5, 6};
           const int r0 = (zj + 2) * RZ + (zk - 2 + 2);
-          S a0[7], a1[7], a2[7], a3[7];
+          R a0[7], a1[7], a2[7], a3[7];
 #pragma unroll
           for (int cc = 0; cc < 7; ++cc) {
-            const S* row = Pp + zrow[cc] * NR + r0;
+            const R* row = Pp + zrow[cc] * NR + r0;
             a0[cc] = row[0];
             a1[cc] = row[1];
             a2[cc] = row[2];
             a3[cc] = row[3];
           }
-          S L[7], Rt[7], F[7];
+          R L[7], Rt[7], F[7];
           reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
           hlld_flux(L, Rt, Bp[2 * NR + (zj + 2) * RZ + (zk + 2)], gamma, inv_gm1, F);
 #pragma unroll
@@ -320,7 +346,7 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
     // B2: x-face of plane p (needs plane p + 1 for its stencil) --------------------------
     {
       const int c = p + 1;
-      const S* Pn = sP + ((c + 4) & 1) * 8 * NR;
+      const R* Pn = sP + ((c + 4) & 1) * 8 * NR;
 #pragma unroll
       for (int s = 0; s < 2; ++s)
 #pragma unroll
@@ -331,24 +357,24 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
         for (int cc = 0; cc < 7; ++cc) q[2][cc] = Pn[xrow[cc] * NR + col_r];
       }
       // the slope of plane p, kept for face p + 1: each cell's x-slope is formed once
-      S now[7];
+      R now[7];
 #pragma unroll
       for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q[1][cc] - q[0][cc], q[2][cc] - q[1][cc]);
-      const S* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : ((p + 4) & 1)) * 3 * NR;
+      const R* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : ((p + 4) & 1)) * 3 * NR;
       if (p >= x0) {
-        S L[7], Rt[7], F[7];
+        R L[7], Rt[7], F[7];
         reconstruct_sloped(q[0], q[1], slope, now, L, Rt);
         hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
         if (PHYS && a.eta != 0.0 && tid < NCORE) {
           // eta (J_y B_z - J_z B_y) on the x-face: J of its two y- and two z-edges, B of
           // the four y- and z-faces around it (carafe/mhd3d.py:590-600)
-          const S eta = S(a.eta);
-          const S jb = S(0.5) * (jy_at(p, cj, ck) + jy_at(p, cj, ck + 1));
-          const S jc = S(0.5) * (jz_at(p, cj, ck) + jz_at(p, cj + 1, ck));
-          const S bc = S(0.5) * (S(0.5) * (face(p - 1, 2, cj, ck) + face(p, 2, cj, ck)) +
-                                 S(0.5) * (face(p - 1, 2, cj, ck + 1) + face(p, 2, cj, ck + 1)));
-          const S bb = S(0.5) * (S(0.5) * (face(p - 1, 1, cj, ck) + face(p, 1, cj, ck)) +
-                                 S(0.5) * (face(p - 1, 1, cj + 1, ck) + face(p, 1, cj + 1, ck)));
+          const R eta = R(a.eta);
+          const R jb = R(0.5) * (jy_at(p, cj, ck) + jy_at(p, cj, ck + 1));
+          const R jc = R(0.5) * (jz_at(p, cj, ck) + jz_at(p, cj + 1, ck));
+          const R bc = R(0.5) * (R(0.5) * (face(p - 1, 2, cj, ck) + face(p, 2, cj, ck)) +
+                                 R(0.5) * (face(p - 1, 2, cj, ck + 1) + face(p, 2, cj, ck + 1)));
+          const R bb = R(0.5) * (R(0.5) * (face(p - 1, 1, cj, ck) + face(p, 1, cj, ck)) +
+                                 R(0.5) * (face(p - 1, 1, cj + 1, ck) + face(p, 1, cj + 1, ck)));
           F[4] += eta * (jb * bc - jc * bb);
         }
         // x-face walls: none in 3D (the reference's MHD3D has periodic and outflow faces)
@@ -361,28 +387,28 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
 #pragma unroll
       for (int cc = 0; cc < 7; ++cc) slope[cc] = now[cc];
       if (PHYS && a.eta != 0.0 && p >= x0) {
-        const S eta = S(a.eta);
+        const R eta = R(a.eta);
         if (p < xe) {
           // eta (J_z B_x - J_x B_z) on the y-face (cell p, node yj, cell yk) and
           // eta (J_x B_y - J_y B_x) on the z-face (cell p, cell zj, node zk), added to the
           // energy fluxes this thread formed in B1 (read by C one plane later)
           const int sl3 = (p + 6) % 3;
           if (yk >= 0) {
-            const S jb = S(0.5) * (jz_at(p, yj, yk) + jz_at(p + 1, yj, yk));
-            const S jc = S(0.5) * (jx_at(p, yj, yk) + jx_at(p, yj, yk + 1));
-            const S bc = S(0.5) * (S(0.5) * (face(p, 0, yj - 1, yk) + face(p, 0, yj, yk)) +
-                                   S(0.5) * (face(p + 1, 0, yj - 1, yk) + face(p + 1, 0, yj, yk)));
-            const S bb = S(0.5) * (S(0.5) * (face(p, 2, yj - 1, yk) + face(p, 2, yj, yk)) +
-                                   S(0.5) * (face(p, 2, yj - 1, yk + 1) + face(p, 2, yj, yk + 1)));
+            const R jb = R(0.5) * (jz_at(p, yj, yk) + jz_at(p + 1, yj, yk));
+            const R jc = R(0.5) * (jx_at(p, yj, yk) + jx_at(p, yj, yk + 1));
+            const R bc = R(0.5) * (R(0.5) * (face(p, 0, yj - 1, yk) + face(p, 0, yj, yk)) +
+                                   R(0.5) * (face(p + 1, 0, yj - 1, yk) + face(p + 1, 0, yj, yk)));
+            const R bb = R(0.5) * (R(0.5) * (face(p, 2, yj - 1, yk) + face(p, 2, yj, yk)) +
+                                   R(0.5) * (face(p, 2, yj - 1, yk + 1) + face(p, 2, yj, yk + 1)));
             sYZ[(sl3 * 2 + 0) * 7 * G + 4 * G + y_g] += eta * (jb * bc - jc * bb);
           }
           if (zj >= 0) {
-            const S jb = S(0.5) * (jx_at(p, zj, zk) + jx_at(p, zj + 1, zk));
-            const S jc = S(0.5) * (jy_at(p, zj, zk) + jy_at(p + 1, zj, zk));
-            const S bc = S(0.5) * (S(0.5) * (face(p, 1, zj, zk - 1) + face(p, 1, zj, zk)) +
-                                   S(0.5) * (face(p, 1, zj + 1, zk - 1) + face(p, 1, zj + 1, zk)));
-            const S bb = S(0.5) * (S(0.5) * (face(p, 0, zj, zk - 1) + face(p, 0, zj, zk)) +
-                                   S(0.5) * (face(p + 1, 0, zj, zk - 1) + face(p + 1, 0, zj, zk)));
+            const R jb = R(0.5) * (jx_at(p, zj, zk) + jx_at(p, zj + 1, zk));
+            const R jc = R(0.5) * (jy_at(p, zj, zk) + jy_at(p + 1, zj, zk));
+            const R bc = R(0.5) * (R(0.5) * (face(p, 1, zj, zk - 1) + face(p, 1, zj, zk)) +
+                                   R(0.5) * (face(p, 1, zj + 1, zk - 1) + face(p, 1, zj + 1, zk)));
+            const R bb = R(0.5) * (R(0.5) * (face(p, 0, zj, zk - 1) + face(p, 0, zj, zk)) +
+                                   R(0.5) * (face(p + 1, 0, zj, zk - 1) + face(p + 1, 0, zj, zk)));
             sYZ[(sl3 * 2 + 1) * 7 * G + 4 * G + z_g] += eta * (jb * bc - jc * bb);
           }
         }
@@ -426,12 +452,12 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
       const int j = cj, k = ck;
       const int gj = gj_c, gk = gk_c;
       const int sc = (p + 6) % 3, sp = (p + 5) % 3;  // flux slots of planes p and p-1
-      const S* Yc = sYZ + (sc * 2 + 0) * 7 * G;
-      const S* Zc = sYZ + (sc * 2 + 1) * 7 * G;
-      const S* Yp = sYZ + (sp * 2 + 0) * 7 * G;
-      const S* Zp = sYZ + (sp * 2 + 1) * 7 * G;
-      const S* Ec = sEc + ((p + 8) & 3) * 3 * G;
-      const S* Ep = sEc + ((p + 7) & 3) * 3 * G;
+      const R* Yc = sYZ + (sc * 2 + 0) * 7 * G;
+      const R* Zc = sYZ + (sc * 2 + 1) * 7 * G;
+      const R* Yp = sYZ + (sp * 2 + 0) * 7 * G;
+      const R* Zp = sYZ + (sp * 2 + 1) * 7 * G;
+      const R* Ec = sEc + ((p + 8) & 3) * 3 * G;
+      const R* Ep = sEc + ((p + 7) & 3) * 3 * G;
       auto yi = [&](int fj, int kk) { return fj * GZ + (kk + 1); };
       auto zi = [&](int jj, int fk) { return (jj + 1) * GZ + fk; };
       auto gi = [&](int jj, int kk) { return (jj + 1) * GZ + (kk + 1); };
@@ -443,9 +469,17 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
         const int zrow[5] = {0, 2, 3, 1, 4};  // z-sweep rows
 #pragma unroll
         for (int qf = 0; qf < 5; ++qf) {
-          const S div = M::div(fnow[qf] - fprev[qf], dx, idx) +
-                        M::div(Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)], dy, idy) +
-                        M::div(Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)], dz, idz);
+          S div;
+          if constexpr (kMixed) {
+            // float64 flux differences of the float32 fluxes
+            div = (S(fnow[qf]) - S(fprev[qf])) * sidx +
+                  (S(Yp[yrow[qf] * G + yi(j + 1, k)]) - S(Yp[yrow[qf] * G + yi(j, k)])) * sidy +
+                  (S(Zp[zrow[qf] * G + zi(j, k + 1)]) - S(Zp[zrow[qf] * G + zi(j, k)])) * sidz;
+          } else {
+            div = M::div(fnow[qf] - fprev[qf], dx, idx) +
+                  M::div(Yp[yrow[qf] * G + yi(j + 1, k)] - Yp[yrow[qf] * G + yi(j, k)], dy, idy) +
+                  M::div(Zp[zrow[qf] * G + zi(j, k + 1)] - Zp[zrow[qf] * G + zi(j, k)], dz, idz);
+          }
           S value = cv[qf] - dt * div;
           if (PHYS) {
             // gravity: rho g on the momentum, m . g on the energy, from the stage's input
@@ -459,36 +493,36 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
       }
       // E_x on the x-edges of cell plane p: (a, b) = (y, z)
       if (do_ex) {
-        S ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
+        R ex = ct_node(Yc[5 * G + yi(j, k - 1)], Yc[5 * G + yi(j, k)], Yc[yi(j, k - 1)], Yc[yi(j, k)],
                              Zc[6 * G + zi(j - 1, k)], Zc[6 * G + zi(j, k)], Zc[zi(j - 1, k)], Zc[zi(j, k)],
                              Ec[gi(j - 1, k - 1)], Ec[gi(j, k - 1)], Ec[gi(j - 1, k)], Ec[gi(j, k)]);
         if (PHYS) ex += ejx;
         const int64_t o = 5 * fs + o_edge;
-        S value = ev[0] - dt * ex;
+        S value = ev[0] - dt * S(ex);
         if (base_state) value = (value + eb[0]) * S(0.5);
         dst[o] = value;
       }
       {
         // E_y on the y-edges of node plane p: (a, b) = (z, x)
         if (do_ey) {
-          S ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
+          R ey = ct_node(Zp[5 * G + zi(j, k)], Zc[5 * G + zi(j, k)], Zp[zi(j, k)], Zc[zi(j, k)],
                                sX[2 * G + gi(j, k - 1)], sX[2 * G + gi(j, k)], sX[gi(j, k - 1)], sX[gi(j, k)],
                                Ep[G + gi(j, k - 1)], Ep[G + gi(j, k)], Ec[G + gi(j, k - 1)], Ec[G + gi(j, k)]);
           if (PHYS) ey += ejy;
           const int64_t o = 6 * fs + o_edge;
-          S value = ev[1] - dt * ey;
+          S value = ev[1] - dt * S(ey);
           if (base_state) value = (value + eb[1]) * S(0.5);
           dst[o] = value;
         }
         // E_z on the z-edges of node plane p: (a, b) = (x, y)
         if (do_ez) {
-          S ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
+          R ez = ct_node(sX[G + gi(j - 1, k)], sX[G + gi(j, k)], sX[gi(j - 1, k)], sX[gi(j, k)],
                                Yp[6 * G + yi(j, k)], Yc[6 * G + yi(j, k)], Yp[yi(j, k)], Yc[yi(j, k)],
                                Ep[2 * G + gi(j - 1, k)], Ec[2 * G + gi(j - 1, k)], Ep[2 * G + gi(j, k)],
                                Ec[2 * G + gi(j, k)]);
           if (PHYS) ez += ejz;
           const int64_t o = 7 * fs + o_edge;
-          S value = ev[2] - dt * ez;
+          S value = ev[2] - dt * S(ez);
           if (base_state) value = (value + eb[2]) * S(0.5);
           dst[o] = value;
         }
@@ -504,21 +538,22 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<S, PHYS, TY,
   if (bad) atomicAdd(a.bad, (unsigned long long)bad);
 }
 
-template <typename S, int LIM, bool PHYS, int TY, int TZ>
+template <typename S, typename R, int LIM, bool PHYS, int TY, int TZ>
 void launch_shape3d(const StageArgs<S>& args, int ntiles, cudaStream_t stream) {
-  constexpr size_t smem = smem3d<S, PHYS, TY, TZ>();
-  cudaFuncSetAttribute(stage3d_kernel<S, LIM, PHYS, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  stage3d_kernel<S, LIM, PHYS, TY, TZ><<<ntiles, threads3d<TY, TZ>(), smem, stream>>>(args);
+  constexpr size_t smem = smem3d<R, PHYS, TY, TZ>();
+  cudaFuncSetAttribute(stage3d_kernel<S, R, LIM, PHYS, TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       int(smem));
+  stage3d_kernel<S, R, LIM, PHYS, TY, TZ><<<ntiles, threads3d<TY, TZ>(), smem, stream>>>(args);
 }
 
-template <typename S, int LIM>
+template <typename S, typename R, int LIM>
 int launch_limiter3d(const StageArgs<S>& args, int ntiles, bool phys, int shape, cudaStream_t stream) {
-  using T = Tile3D<S>;
+  using T = Tile3D<S, R>;
   if (shape == 0) {
     if (phys)
-      launch_shape3d<S, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+      launch_shape3d<S, R, LIM, true, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
     else
-      launch_shape3d<S, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
+      launch_shape3d<S, R, LIM, false, T::kShape[0][0], T::kShape[0][1]>(args, ntiles, stream);
     return kOk;
   }
   if (phys) {
@@ -526,22 +561,23 @@ int launch_limiter3d(const StageArgs<S>& args, int ntiles, bool phys, int shape,
     return kBadArgument;
   }
   if (shape == 1)
-    launch_shape3d<S, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream);
+    launch_shape3d<S, R, LIM, false, T::kShape[1][0], T::kShape[1][1]>(args, ntiles, stream);
   else if constexpr (T::kShapes > 2)
-    launch_shape3d<S, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream);
+    launch_shape3d<S, R, LIM, false, T::kShape[2][0], T::kShape[2][1]>(args, ntiles, stream);
   return kOk;
 }
 
-template <typename S>
+template <typename S, typename R>
 int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, int ty, int tz, cudaStream_t stream) {
   if (ntiles <= 0) return kOk;
   if (args.lx <= 0) {
     set_error("stage3d: lx must be positive");
     return kBadArgument;
   }
+  using T = Tile3D<S, R>;
   int shape = -1;
-  for (int i = 0; i < Tile3D<S>::kShapes; ++i)
-    if (Tile3D<S>::kShape[i][0] == ty && Tile3D<S>::kShape[i][1] == tz) shape = i;
+  for (int i = 0; i < T::kShapes; ++i)
+    if (T::kShape[i][0] == ty && T::kShape[i][1] == tz) shape = i;
   if (shape < 0) {
     set_error("stage3d: no %dx%d tile shape", ty, tz);
     return kBadArgument;
@@ -549,10 +585,10 @@ int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, int ty, in
   const bool phys = args.eta != 0.0 || args.gravity[0] != 0.0 || args.gravity[1] != 0.0 || args.gravity[2] != 0.0;
   int status;
   switch (limiter) {
-    case 0: status = launch_limiter3d<S, 0>(args, ntiles, phys, shape, stream); break;
-    case 1: status = launch_limiter3d<S, 1>(args, ntiles, phys, shape, stream); break;
-    case 2: status = launch_limiter3d<S, 2>(args, ntiles, phys, shape, stream); break;
-    case 3: status = launch_limiter3d<S, 3>(args, ntiles, phys, shape, stream); break;
+    case 0: status = launch_limiter3d<S, R, 0>(args, ntiles, phys, shape, stream); break;
+    case 1: status = launch_limiter3d<S, R, 1>(args, ntiles, phys, shape, stream); break;
+    case 2: status = launch_limiter3d<S, R, 2>(args, ntiles, phys, shape, stream); break;
+    case 3: status = launch_limiter3d<S, R, 3>(args, ntiles, phys, shape, stream); break;
     default:
       set_error("limiter code %d is not one of 0..3", limiter);
       return kBadArgument;
@@ -561,21 +597,31 @@ int launch_stage3d(const StageArgs<S>& args, int ntiles, int limiter, int ty, in
   return check_launch("stage3d");
 }
 
-template int launch_stage3d<float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
-template int launch_stage3d<double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+template int launch_stage3d<float, float>(const StageArgs<float>&, int, int, int, int, cudaStream_t);
+template int launch_stage3d<double, double>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
+template int launch_stage3d<double, float>(const StageArgs<double>&, int, int, int, int, cudaStream_t);
 
-int tile_shapes_3d(int fp64, int* shapes, int max) {
-  const int count = fp64 ? Tile3D<double>::kShapes : Tile3D<float>::kShapes;
-  for (int i = 0; i < count && i < max; ++i) {
-    shapes[2 * i] = fp64 ? Tile3D<double>::kShape[i][0] : Tile3D<float>::kShape[i][0];
-    shapes[2 * i + 1] = fp64 ? Tile3D<double>::kShape[i][1] : Tile3D<float>::kShape[i][1];
+template <typename T>
+static int copy_shapes3d(int* shapes, int max) {
+  for (int i = 0; i < T::kShapes && i < max; ++i) {
+    shapes[2 * i] = T::kShape[i][0];
+    shapes[2 * i + 1] = T::kShape[i][1];
   }
-  return count;
+  return T::kShapes;
 }
 
-void tile_shape_3d(int fp64, int* ty, int* tz) {
-  *ty = fp64 ? Tile3D<double>::TY : Tile3D<float>::TY;
-  *tz = fp64 ? Tile3D<double>::TZ : Tile3D<float>::TZ;
+int tile_shapes_3d(int mode, int* shapes, int max) {
+  if (mode == kMath32State64) return copy_shapes3d<Tile3D<double, float>>(shapes, max);
+  return mode ? copy_shapes3d<Tile3D<double>>(shapes, max) : copy_shapes3d<Tile3D<float>>(shapes, max);
+}
+
+void tile_shape_3d(int mode, int* ty, int* tz) {
+  if (mode == kMath32State64) {
+    *ty = Tile3D<double, float>::TY, *tz = Tile3D<double, float>::TZ;
+    return;
+  }
+  *ty = mode ? Tile3D<double>::TY : Tile3D<float>::TY;
+  *tz = mode ? Tile3D<double>::TZ : Tile3D<float>::TZ;
 }
 
 }  // namespace wb

@@ -15,6 +15,7 @@
 
 #include "layout.cuh"
 #include "numerics.cuh"
+#include "stage.cuh"
 #include "wb_internal.cuh"
 
 namespace wb {
@@ -402,13 +403,13 @@ extern "C" int wb_tag_features(int precision, const void* pool, const void* patc
                                                          static_cast<const PatchDesc*>(patches), chunk_patch,
                                                          chunk_start, row_start, b0x, b0y, b0z, gamma, mean,
                                                          inv_std, out);
-  else if (precision == 64)
+  else if (precision == 64 || precision == kMath32State64)  // a float64 state
     tag_features3d_kernel<double><<<nchunks, 256, 0, s>>>(static_cast<const double*>(pool),
                                                           static_cast<const PatchDesc*>(patches), chunk_patch,
                                                           chunk_start, row_start, b0x, b0y, b0z, gamma, mean,
                                                           inv_std, out);
   else {
-    set_error("tag_features: precision is 32 or 64, not %d", precision);
+    set_error("tag_features: precision is 32, 64 or %d, not %d", kMath32State64, precision);
     return kBadArgument;
   }
   return check_launch("tag_features");

@@ -50,9 +50,11 @@ __device__ __forceinline__ double key_to_double(unsigned long long k) {
 // keys[0] = key(0) (running max of a non-negative rate), keys[1] = key(+inf) (running min)
 __global__ void init_keys_kernel(unsigned long long* keys);
 
-// Block-wide max of `largest` and min of `smallest`, one atomic per warp.
+// Block-wide max of `largest` and min of `smallest`, one atomic per warp; the min also
+// into *level_min when given.
 __device__ __forceinline__ void block_reduce_keys(double largest, double smallest,
-                                                  unsigned long long* keys) {
+                                                  unsigned long long* keys,
+                                                  unsigned long long* level_min = nullptr) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     largest = fmax(largest, __shfl_xor_sync(0xffffffffu, largest, o));
@@ -61,6 +63,7 @@ __device__ __forceinline__ void block_reduce_keys(double largest, double smalles
   if ((threadIdx.x & 31) == 0) {
     atomicMax(&keys[0], double_to_key(largest));
     atomicMin(&keys[1], double_to_key(smallest));
+    if (level_min) atomicMin(level_min, double_to_key(smallest));
   }
 }
 

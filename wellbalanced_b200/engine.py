@@ -26,7 +26,7 @@ import torch
 from wellbalanced_b200 import _lib
 from wellbalanced_b200.mesh import Layout, _concat, size_ops
 
-_DTYPES = {32: torch.float32, 64: torch.float64}
+_DTYPES = {32: torch.float32, 64: torch.float64, _lib.MATH32_STATE64: torch.float64}
 
 
 def _ptr(t):
@@ -56,8 +56,7 @@ class Engine:
 
     def __init__(self, hierarchy, *, precision=32, walls=None, limiter=1, gamma=5.0 / 3.0, mean_field=(0.0, 0.0, 0.0),
                  instances=None, device="cuda", lx=32, stream=None, layout=None):
-        if precision not in (32, 64):
-            raise ValueError("precision is 32 or 64")
+        precision = _lib.precision_code(precision)
         if not torch.cuda.is_available():
             raise RuntimeError("wellbalanced_b200 needs a CUDA device (there is no CPU path)")
         _lib.load()
@@ -82,6 +81,14 @@ class Engine:
         self.chunk_start = torch.from_numpy(L.chunk_start).to(self.device)
         self.nchunks = int(L.chunk_patch.size)
         self.inv_dx2_sum = torch.from_numpy(L.inv_dx2_sum).to(self.device)
+        levels = np.ascontiguousarray(getattr(L, "inv_dx2_levels", L.inv_dx2_sum[:, None]), dtype=np.float64)
+        #: levels of the per-(instance, level) diffusion limit
+        self.nlevels = int(levels.shape[1])
+        self.inv_dx2_levels = torch.from_numpy(levels.reshape(-1)).to(self.device)
+        self.level_keys = torch.zeros(max(self.nlevels * L.ninstances, 1), dtype=torch.int64, device=self.device)
+        #: reduce the smallest density per level (set by the solvers when a diffusion limit
+        #: applies on a refined hierarchy: each level's own density and spacing decide)
+        self.per_level_dt = False
         # op lists on the device, each cut for the op kernels by its size (`size_ops`)
         def upload(ops, dtype):
             ops = size_ops(ops) if np.asarray(ops).size else np.zeros(0, dtype)
@@ -240,15 +247,27 @@ class Engine:
     def rate(self, pool=None):
         pool = self.state if pool is None else pool
         b = self.mean_field
-        _lib.call("wb_rate", self.precision, self.ndim, pool.data_ptr(), self.patches.data_ptr(),
-                  self.layout.npatches, self.chunk_patch.data_ptr(), self.chunk_start.data_ptr(), self.nchunks,
-                  b[0], b[1], b[2], self.gamma, self.keys.data_ptr(), self.ninstances, self._s())
+        if self.per_level_dt:
+            _lib.call("wb_rate_levels", self.precision, self.ndim, pool.data_ptr(), self.patches.data_ptr(),
+                      self.layout.npatches, self.chunk_patch.data_ptr(), self.chunk_start.data_ptr(), self.nchunks,
+                      b[0], b[1], b[2], self.gamma, self.keys.data_ptr(), self.ninstances,
+                      self.level_keys.data_ptr(), self.nlevels, self._s())
+        else:
+            _lib.call("wb_rate", self.precision, self.ndim, pool.data_ptr(), self.patches.data_ptr(),
+                      self.layout.npatches, self.chunk_patch.data_ptr(), self.chunk_start.data_ptr(), self.nchunks,
+                      b[0], b[1], b[2], self.gamma, self.keys.data_ptr(), self.ninstances, self._s())
         self.launches += 2 if self.nchunks else 1
 
     def finalize_dt(self, cfl, eta=0.0, kappa=0.0, *, clip_to_end=False, advance=False):
-        _lib.call("wb_finalize_dt", self.keys.data_ptr(), self.ninstances, float(cfl), float(eta), float(kappa),
-                  self.gamma, self.inv_dx2_sum.data_ptr(), self.time.data_ptr(),
-                  self.end.data_ptr() if clip_to_end else None, self.dt.data_ptr(), int(advance), self._s())
+        end = self.end.data_ptr() if clip_to_end else None
+        if self.per_level_dt:
+            _lib.call("wb_finalize_dt_levels", self.keys.data_ptr(), self.ninstances, float(cfl), float(eta),
+                      float(kappa), self.gamma, self.level_keys.data_ptr(), self.inv_dx2_levels.data_ptr(),
+                      self.nlevels, self.time.data_ptr(), end, self.dt.data_ptr(), int(advance), self._s())
+        else:
+            _lib.call("wb_finalize_dt", self.keys.data_ptr(), self.ninstances, float(cfl), float(eta), float(kappa),
+                      self.gamma, self.inv_dx2_sum.data_ptr(), self.time.data_ptr(), end, self.dt.data_ptr(),
+                      int(advance), self._s())
         self.launches += 1
 
     def rate_values(self):

@@ -488,7 +488,7 @@ class Layout:
         columns in 3D (one of the shapes `_lib.tile_shapes` lists)."""
         tile = tuple(int(v) for v in tile)
         if tile not in _lib.tile_shapes(self.ndim, self.precision):
-            raise ValueError(f"no {self.ndim}D tile shape {tile} for float{self.precision}")
+            raise ValueError(f"no {self.ndim}D tile shape {tile} for precision code {self.precision}")
         self.tile = self.tile_shape = tile
         self._cut_tiles()
 
@@ -522,12 +522,16 @@ class Layout:
                 start.append(s)
         self.chunk_patch = np.array(patch, dtype=np.int32)
         self.chunk_start = np.array(start, dtype=np.int32)
-        # finest sum of inverse squared spacings per instance (diffusion limit)
+        # finest sum of inverse squared spacings per instance (diffusion limit), and the
+        # sum of each (instance, level) holding a patch (0 where it holds none)
         inv = np.zeros(self.ninstances)
+        levels = np.zeros((self.ninstances, self.h.max_level + 1))
         for p in self.h.patches:
             s = sum(d**-2 for d in self.h.spacing(p.level))
             inv[self.instances[p.index]] = max(inv[self.instances[p.index]], s)
+            levels[self.instances[p.index], p.level] = s
         self.inv_dx2_sum = inv
+        self.inv_dx2_levels = levels
 
     # same-level copies and physical boundaries ----------------------------------------------
     def _computed_box(self, p, g):
@@ -788,7 +792,7 @@ class Layout:
         out.tile = getattr(first, "tile", None)
         out.default_tile = getattr(first, "default_tile", first.tile_shape)
         out.walls = first.walls
-        rows, tiles, chunk_patch, chunk_start, inv = [], [], [], [], []
+        rows, tiles, chunk_patch, chunk_start, inv, inv_levels = [], [], [], [], [], []
         same_levels, boundary_levels, interp_levels = {}, {}, {}
         restrict_levels, face_ops = {}, []
         reflux_phases = [[] for _ in range(2 * first.ndim)]
@@ -807,6 +811,7 @@ class Layout:
             chunk_patch.append(part.chunk_patch + patch_shift)
             chunk_start.append(part.chunk_start)
             inv.append(part.inv_dx2_sum[:1])
+            inv_levels.append(part.inv_dx2_levels[0])
 
             def shifted(ops, fields):
                 ops = ops.copy()
@@ -844,6 +849,10 @@ class Layout:
         out.chunk_patch = np.concatenate(chunk_patch).astype(np.int32)
         out.chunk_start = np.concatenate(chunk_start).astype(np.int32)
         out.inv_dx2_sum = np.concatenate(inv)
+        width = max(len(row) for row in inv_levels)
+        out.inv_dx2_levels = np.zeros((len(layouts), width))
+        for k, row in enumerate(inv_levels):
+            out.inv_dx2_levels[k, : len(row)] = row
         nlevels = max(len(part.copy_phases) for part in layouts)
         naxes = first.ndim
         out.copy_phases = []

@@ -7,8 +7,11 @@ Same constructor keywords, test problems and methods as the reference
 stage kernels of ``libwb200.so`` (``wb_stage2d``) with the halo, restriction and
 flux-register op lists (`wellbalanced_b200.engine`).
 
-Extra keyword ``precision``: 64 (float64 state and arithmetic, the reference's) or 32
-(float32 state and arithmetic, the pressure recovery in float64).
+Extra keyword ``precision``: 64 (float64 state and arithmetic, the reference's), 32
+(float32 state and arithmetic, the pressure recovery in float64) or "mixed" (float32
+reconstruction, HLLD and CT on a float64 state: the conserved and potential updates, the
+pressure recovery, the face fields' potential differences and the flux differences in
+float64).
 
 Numerics as the reference: MUSCL/PLM reconstruction with the limiter of
 ``carafe.limiters``, HLLD, CT-contact electric field on the nodes, Heun (SSP-RK2),
@@ -23,6 +26,8 @@ from typing import Any
 
 import numpy as np
 import torch
+
+from wellbalanced_b200 import _lib
 
 from wellbalanced_b200.dataset import Dataset, Variable
 from wellbalanced_b200.engine import Engine
@@ -41,8 +46,8 @@ class MHD2D:
     """2.5D ideal MHD on the device (see the module docstring).
 
     Args: as ``carafe.mhd.MHD2D`` (hierarchy, gamma, mean_field, resistivity, limiter,
-    cfl, conduction, gravity, boundaries, prefix), plus ``precision`` (32 or 64) and
-    ``device``.
+    cfl, conduction, gravity, boundaries, prefix), plus ``precision`` (32, 64 or "mixed")
+    and ``device``.
     """
 
     def __init__(
@@ -58,7 +63,7 @@ class MHD2D:
         gravity: tuple[float, float] = (0.0, 0.0),
         boundaries: dict[str, str] | None = None,
         prefix: str = "mhd_",
-        precision: int = 64,
+        precision: int | str = 64,
         device: str = "cuda",
         tile: tuple[int, int] | str | None = None,
     ) -> None:
@@ -100,7 +105,7 @@ class MHD2D:
         self.names = {name: prefix + name for name in CONSERVED}
         self.potential = prefix + "az"
         self.periodic = tuple(hierarchy.periodic)
-        self.precision = int(precision)
+        self.precision = _lib.precision_code(precision)
         self.device = device
         # tile shape of the stage kernel: None (the default), (tx, ty), or "auto" (tuned
         # when the state is first set; ideal MHD only)
@@ -134,6 +139,9 @@ class MHD2D:
         physics = (self.resistivity, self.conduction[0], self.conduction[1], self.gravity[0], self.gravity[1])
         if any(physics):
             self.engine.physics = tuple(float(v) for v in physics)
+        # the conduction limit depends on the density: on a refined hierarchy each level's
+        # smallest density goes with that level's spacing (carafe/mhd.py:942-960)
+        self.engine.per_level_dt = self.engine.max_level > 0 and max(self.conduction) > 0.0
         if self.tile is not None and self._fused:
             if self.engine.physics is not None and self.tile != self.engine.layout.default_tile:
                 raise ValueError("resistivity, conduction and gravity run on the default tile shape")

@@ -5,7 +5,8 @@ Same constructor keywords, test problems and methods as the reference
 the vector potential on the edges) lives in device pools; a step is the fused 3D stage
 kernel of ``libwb200.so`` (``wb_stage3d``: primitives, MUSCL + HLLD along the three
 axes, CT-contact edge fields, cell and edge updates in one pass per stage) with the halo
-and restriction op lists. ``precision`` 64 (the reference's arithmetic) or 32.
+and restriction op lists. ``precision`` 64 (the reference's arithmetic), 32, or "mixed"
+(float32 reconstruction, HLLD and CT on a float64 state).
 """
 
 from __future__ import annotations
@@ -14,6 +15,8 @@ from typing import Any
 
 import numpy as np
 import torch
+
+from wellbalanced_b200 import _lib
 
 from wellbalanced_b200.dataset import Dataset, Variable
 from wellbalanced_b200.engine import Engine
@@ -44,7 +47,7 @@ class MHD3D:
         cfl: float = 0.3,
         gravity: tuple[float, float, float] = (0.0, 0.0, 0.0),
         prefix: str = "mhd_",
-        precision: int = 64,
+        precision: int | str = 64,
         device: str = "cuda",
         lx: int | str = 32,
     ) -> None:
@@ -72,7 +75,7 @@ class MHD3D:
         self.names = {name: prefix + name for name in CONSERVED_3D}
         self.potential = tuple(prefix + name for name in ("ax", "ay", "az"))
         self.periodic = tuple(hierarchy.periodic)
-        self.precision = int(precision)
+        self.precision = _lib.precision_code(precision)
         self.device = device
         # x-planes per tile of the stage kernel; "auto": tuned when the state is first set
         self._auto_lx = lx == "auto"
