@@ -12,9 +12,10 @@ Workloads (``--workload``; one zone-update = one cell advanced by one full RK2 s
   per kernel (the timed steps launch directly; the same steps replayed from a CUDA graph
   are reported beside them).
 * ``harris``: a 2D Harris current sheet on [-1, 1] x [-2, 2], base 128 x 256, periodic in
-  x and outflow in y, refined three times on the current (|J| dx > 0.01, patches of at
-  most 32 cells a side: 177 patches), float32 with float64 refluxing; every level
-  advances at the finest CFL 0.4 step, all patches in one launch per kernel.
+  x and outflow in y, refined three times on the current (|J| dx > 1e-4, boxes of at most
+  16 cells a side: ~1800 uneven patches), float32 with float64 refluxing; every level
+  advances at the finest CFL 0.4 step, all patches in one launch per kernel, the small
+  ops between the stages in two op programs per step.
 
 With N GPUs (torchrun) every rank advances its own copy of the workload (replicas,
 seeded by rank: weak scaling, no data-path collective); `value` is the zone-updates of
@@ -70,8 +71,11 @@ def parse():
 HARRIS_BASE = (128, 256)
 HARRIS_BOUNDS = ((-1.0, 1.0), (-2.0, 2.0))
 HARRIS_LEVELS = 3
-HARRIS_THRESHOLD = 0.01
-HARRIS_PATCH = 16  # coarse cells a side, so refined patches of at most 32 cells
+#: the refinement rule of the Harris workload: |J| dx above 1e-4 (the current sheet and its
+#: seeded perturbation out to |y| ~ 0.3), clustered into boxes of at most 8 coarse cells a
+#: side (refined patches of 4-16 cells): ~1800 uneven patches over three levels
+HARRIS_THRESHOLD = 1e-4
+HARRIS_PATCH = 8  # coarse cells a side, so refined patches of at most 16 cells
 
 
 def _harris_model(cls, precision, seed, *, levels=HARRIS_LEVELS, base=HARRIS_BASE, **options):
@@ -225,6 +229,7 @@ class Turbulence:
 
     def restore(self, state, time):
         self.engine.state.copy_(state)
+        self.engine.dt_ready = False
         self.engine.time.copy_(time)
         self.model.time = float(time[0].item())
 
@@ -752,6 +757,7 @@ def measure(work, args, rank, world, local, barrier, *, steps, warmup, e2e=True,
 
         def round_trip():
             pool.copy_(host, non_blocking=True)
+            eng.dt_ready = False  # the step's dt from the state copied in
             work.advance(1)
             host.copy_(pool, non_blocking=True)
 

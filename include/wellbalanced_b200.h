@@ -218,7 +218,89 @@ int wb_face_flux_ops_physics(int precision, const void* pool, const void* patche
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,
                     const double* dt, void* stream);
 
-/* Sizes of the engine structs, for callers that mirror them. */
+/* ---- 3. op programs ------------------------------------------------------------------ */
+
+/* The small-op phases between two stage kernels of a refined step in one launch: reflux
+ * (wb_reflux_apply), restriction (wb_restrict_ops), the halo fill of every level
+ * (wb_fill_ops / wb_copy_ops) and the stable step (wb_rate, wb_finalize_dt): patchwork's
+ * exchange_halos, FluxRegister.reflux and restrict, and stable_step, as
+ * carafe/mhd.py:889-994 (and carafe/mhd3d.py:635-754) call them between and after the
+ * stages. The register's face fluxes (wb_face_flux_ops) keep their own launch. A program
+ * is a list of segments, each one op list of one kind on one of two pools; the segments
+ * of one phase run together (their ops must touch disjoint points), the phases one after
+ * the other. Each item runs the arithmetic of the standalone kernel of its kind, so the
+ * results are those of the standalone launches, bit for bit. `counters`: device array of
+ * 3 + (phases) unsigned words, zero before the first call; every call leaves them zero
+ * except word 2, the error bits (2: a phase wait ran out after a second; 1: a rate chunk's
+ * instance or level lay outside the keys), which the caller reads and clears. Calls that
+ * share one `counters` array must not overlap on the GPU. `segments` and `params` are host
+ * memory (copied into the launch); the op records, work lists, pools and the arrays
+ * `params` points at are device memory. */
+#define WB_PROGRAM_MAX_SEGMENTS 64
+enum {
+  WB_SEG_COPY = 0,        /* ops: struct CopyOp[count] */
+  WB_SEG_INTERP = 1,      /* ops: struct InterpOp[count] */
+  WB_SEG_RESTRICT = 2,    /* ops: struct RestrictOp[count] */
+  WB_SEG_REFLUX = 3,      /* ops: struct RefluxOp[count]; params: reg, dt */
+  WB_SEG_INIT_KEYS = 4,   /* one item: the keys' (and level keys') reduction identities */
+  WB_SEG_RATE = 5,        /* ops: int chunk_patch[count], aux: int chunk_start[count] (as wb_rate) */
+  WB_SEG_FINALIZE_DT = 6, /* one item: wb_finalize_dt (wb_finalize_dt_levels when level_keys is set) */
+  WB_SEG_ADVANCE_TIME = 7 /* one item: time[i] += dt[i] */
+};
+typedef struct wb_program_segment {
+  int32_t kind;  /* WB_SEG_* */
+  int32_t pool;  /* 0: pool0, 1: pool1 */
+  int32_t phase; /* 0 for the first segment, then equal to or one above the previous one */
+  int32_t count; /* items */
+  int32_t first; /* set by wb_run_program */
+  int32_t pad;
+  const void* ops;
+  const void* aux;
+} wb_program_segment;
+typedef struct wb_program_params {
+  double b0[3];
+  double gamma;
+  double cfl, dt_eta, dt_kappa; /* the stable step's cfl, resistivity and conductivity */
+  int32_t ndim, ninstances, nlevels, advance;
+  double* reg;
+  double* dt;
+  double* time;
+  const double* end;
+  unsigned long long* keys;
+  unsigned long long* level_keys; /* NULL: one density minimum per instance */
+  const double* inv_dx2_sum;
+  const double* inv_dx2_levels;
+} wb_program_params;
+int wb_run_program(int precision, void* pool0, void* pool1, const void* patches, const wb_program_segment* segments,
+                   int nsegments, const wb_program_params* params, unsigned* counters, void* stream);
+
+/* ---- 4. regrid on the device ---------------------------------------------------------- */
+
+/* The plain refinement tagger, replacing the per-patch loops of carafe/mhd.py:1011-1041
+ * (|J_z| at the cell's four nodes, averaged, times max(dx, dy)) and carafe/mhd3d.py:771-801
+ * (|curl B| of the cell field by central differences, times max(dx, dy, dz)): every cell of
+ * the patches below level `levels`, in float64 from the stored state, over the rate work
+ * list (chunks of 2048 cells). A tagged cell sets tags[base + i s0 + j s1 + k] = 1 (2D:
+ * base + i s0 + j) with {int64 base, s0, s1} of its patch in `place` (device, one record
+ * per patch); the caller zeroes `tags` (the levels' dense arrays) first. */
+int wb_current_tags(int precision, int ndim, const void* pool, const void* patches, const int* chunk_patch,
+                    const int* chunk_start, int nchunks, const void* place, int levels, double b0x, double b0y,
+                    double b0z, double threshold, unsigned char* tags, void* stream);
+/* The state transfer of a regrid (patchwork's AMRHierarchy.regrid as carafe/mhd.py:1043-1056
+ * calls it), level by level on the new hierarchy's pool:
+ * - wb_prolong_ops: the new fine patches from the new coarser level (struct ProlongOp of
+ *   csrc/transfer.cu: fine, coarse, field range, node mask, ndim, n[3], d[3] haloed fine
+ *   start, fine_lo[3], coarse_lo[3] level indices, coarse_n[3] level shape, periodic mask):
+ *   cells minmod-limited (children c -/+ s/4 per axis), potentials linear along node axes;
+ * - wb_kept_ops: the points an old patch of the same level held, from the old pool (struct
+ *   CopyOp: dst a new patch, src1 an old patch in old_patches, unit weights and strides). */
+int wb_prolong_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
+int wb_kept_ops(int precision, void* pool, const void* patches, const void* old_pool, const void* old_patches,
+                const void* ops, int nops, void* stream);
+
+/* Sizes of the engine structs, for callers that mirror them: PatchDesc, Tile, CopyOp,
+ * InterpOp, RestrictOp, FaceFluxOp, RefluxOp, and with n >= 9 wb_program_segment and
+ * wb_program_params. */
 int wb_struct_sizes(int64_t* sizes_host, int n);
 
 /* Learned refinement tagger. No counterpart in the reference: it predicts the cells the

@@ -1,0 +1,144 @@
+"""Tagging and the regrid transfer on the device (GPU).
+
+* ``current_tags`` is one kernel over every cell of the tagged levels: in 2D it equals the
+  oracle's tags (the reference's |J_z| rule, ``carafe/mhd.py:1011-1041``) on uniform and
+  refined hierarchies; in 3D it equals a NumPy restatement of ``carafe/mhd3d.py:771-801``
+  on the same stored state.
+* ``regrid`` moves the state with the prolongation and kept-value kernels: the new pool
+  equals, bit for bit, the host restatement of the transfer on the same tags, in float64
+  and float32, 2D and 3D, periodic and outflow; the conserved totals are kept to
+  round-off.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+K = 2.0 * np.pi
+
+
+def _ot_pair(n, refined=False):
+    from oracle.mesh import Hierarchy
+    from oracle.mhd2d import MHD2D as OracleMHD2D
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    oh = Hierarchy((n, n), ((0.0, 1.0), (0.0, 1.0)), (True, True))
+    dh = AMRHierarchy((n, n), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, True))
+    if refined:
+        box = ((n // 2, 3 * n // 2), (n // 2, n))
+        oh.add_patch(1, box)
+        dh.add_patch(1, box)
+    state = dict(
+        density=25.0 / (36.0 * np.pi),
+        velocity=(lambda x, y: -np.sin(K * y), lambda x, y: np.sin(K * x), 0.0),
+        pressure=5.0 / (12.0 * np.pi),
+        vector_potential=lambda x, y: (np.cos(2 * K * x) / (2 * K) + np.cos(K * y) / K) / np.sqrt(4 * np.pi),
+    )
+    oracle, device = OracleMHD2D(oh, limiter="mc"), MHD2D(dh, limiter="mc", precision=64)
+    for m in (oracle, device):
+        m.set_state(state["density"], state["velocity"], state["pressure"],
+                    vector_potential=state["vector_potential"])
+    return oracle, device
+
+
+@pytest.mark.parametrize("refined", [False, True])
+def test_2d_tags_equal_the_oracle(refined):
+    oracle, device = _ot_pair(32, refined)
+    for _ in range(3):
+        device.step(oracle.step())
+    for threshold in (0.02, 0.05, 0.1):
+        want = oracle.current_tags(threshold, levels=2)
+        got = device.current_tags(threshold, levels=2)
+        assert sorted(want) == sorted(got)
+        for level in want:
+            np.testing.assert_array_equal(got[level], want[level], err_msg=f"level {level}, {threshold}")
+        assert any(g.any() for g in got.values())
+
+
+def test_3d_tags_equal_the_reference_rule():
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    model = MHD3D.turbulence(16, seed=3, precision=32)
+    model.step()
+    eng = model.engine
+    (patch,) = model.hierarchy.patches
+    n = patch.shape
+    h = model.hierarchy.spacing(0)
+    X, Y, Z = n[0] + 4, n[1] + 4, n[2] + 4
+    pot = (eng.view(eng.state, patch, 5)[:X, : Y + 1, : Z + 1].double().cpu().numpy(),
+           eng.view(eng.state, patch, 6)[: X + 1, :Y, : Z + 1].double().cpu().numpy(),
+           eng.view(eng.state, patch, 7)[: X + 1, : Y + 1, :Z].double().cpu().numpy())
+    cells = []
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        face = np.diff(pot[c], axis=b) / h[b] - np.diff(pot[b], axis=c) / h[c]
+        cells.append(0.5 * (np.take(face, np.arange(face.shape[a] - 1), axis=a) +
+                            np.take(face, np.arange(1, face.shape[a]), axis=a)))
+    square = 0.0
+    for c in range(3):
+        a, b = (c + 1) % 3, (c + 2) % 3
+        jc = np.gradient(cells[b], h[a], axis=a) - np.gradient(cells[a], h[b], axis=b)
+        square = square + jc**2
+    size = np.sqrt(square)[2:-2, 2:-2, 2:-2]
+    for threshold in (0.5, 1.0, 2.0):
+        want = size * max(h) > threshold
+        got = model.current_tags(threshold, levels=1)[0]
+        assert 0 < want.sum() < want.size
+        np.testing.assert_array_equal(got, want)
+
+
+def _models_2d(precision, periodic):
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    out = []
+    for _ in range(2):
+        mesh = AMRHierarchy((32, 32), ((0.0, 1.0), (0.0, 1.0)), periodic=periodic)
+        model = MHD2D(mesh, limiter="mc", precision=precision)
+        model.set_state(lambda x, y: 1.0 + 0.3 * np.exp(-((x - 0.5) ** 2 + (y - 0.4) ** 2) / 0.01),
+                        (lambda x, y: -np.sin(K * y), lambda x, y: np.sin(K * x), 0.1), 1.0,
+                        vector_potential=lambda x, y: 0.1 * (np.cos(2 * K * x) + np.cos(K * y)),
+                        bz=lambda x, y: 0.05 * np.cos(K * x))
+        out.append(model)
+    return out
+
+
+def _models_3d(precision):
+    from wellbalanced_b200.mhd3d import MHD3D
+
+    return [MHD3D.turbulence(12, seed=5, precision=precision) for _ in range(2)]
+
+
+CASES = [("2d float64 periodic", lambda: _models_2d(64, (True, True))),
+         ("2d float32 outflow", lambda: _models_2d(32, (True, False))),
+         ("3d float64", lambda: _models_3d(64)),
+         ("3d float32", lambda: _models_3d(32))]
+
+
+@pytest.mark.parametrize("name, build", CASES, ids=[c[0] for c in CASES])
+def test_device_transfer_equals_the_host_restatement(name, build):
+    from wellbalanced_b200.regrid import regrid_model_device, regrid_model_host
+
+    device, host = build()
+    threshold = 0.05 if device.hierarchy.ndim == 2 else 1.0
+    for regrid in range(2):
+        tags = device.current_tags(threshold, levels=2)
+        before = device.totals()
+        regrid_model_device(device, tags, max_patch_size=8)
+        regrid_model_host(host, tags, max_patch_size=8)
+        assert [p.box for p in device.hierarchy.patches] == [p.box for p in host.hierarchy.patches]
+        assert device.hierarchy.max_level == regrid + 1
+        assert torch.equal(device.engine.state, host.engine.state), (name, regrid)
+        after = device.totals()
+        # float64: round-off; float32: the prolonged children are rounded to float32
+        tol = 1e-13 if device.precision == 64 else 1e-6
+        for key in before:
+            assert abs(after[key] - before[key]) < tol * max(1.0, abs(before[key])), key
+        device.step()
+        host.step()

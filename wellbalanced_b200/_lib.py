@@ -68,6 +68,11 @@ SIGNATURES = {
                                  c_double, c_double, c_double, c_dp, c_dp],
     "wb_reflux_apply": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],
     "wb_struct_sizes": [c_dp, c_int],
+    "wb_run_program": [c_int, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],
+    "wb_current_tags": [c_int, c_int, c_dp, c_dp, c_dp, c_dp, c_int, c_dp, c_int, c_double, c_double, c_double,
+                        c_double, c_dp, c_dp],
+    "wb_prolong_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_kept_ops": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
 }
 
 #: Every symbol include/wellbalanced_b200.h declares.
@@ -119,11 +124,12 @@ def load():
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = ctypes.c_int
-    sizes = np.zeros(7, dtype=np.int64)
-    status = lib.wb_struct_sizes(sizes.ctypes.data, 7)
+    sizes = np.zeros(9, dtype=np.int64)
+    status = lib.wb_struct_sizes(sizes.ctypes.data, 9)
     if status != 0:
         raise WBError(lib.wb_last_error().decode())
-    expected = [d.itemsize for d in (PATCH, TILE, COPY_OP, INTERP_OP, RESTRICT_OP, FACE_FLUX_OP, REFLUX_OP)]
+    expected = [d.itemsize for d in (PATCH, TILE, COPY_OP, INTERP_OP, RESTRICT_OP, FACE_FLUX_OP, REFLUX_OP,
+                                     PROGRAM_SEGMENT)] + [ctypes.sizeof(ProgramParams)]
     if list(sizes) != expected:
         raise RuntimeError(f"struct layout mismatch between host and library: {list(sizes)} != {expected}")
     _lib = lib
@@ -215,3 +221,42 @@ REFLUX_OP = np.dtype(
         "itemsize": 96,
     }
 )
+
+# ---- op programs (include/wellbalanced_b200.h: wb_program_segment, wb_program_params) -----
+PROGRAM_SEGMENT = np.dtype(
+    {
+        "names": ["kind", "pool", "phase", "count", "first", "pad", "ops", "aux"],
+        "formats": ["<i4"] * 6 + ["<u8", "<u8"],
+        "offsets": [0, 4, 8, 12, 16, 20, 24, 32],
+        "itemsize": 40,
+    }
+)
+#: WB_SEG_* codes
+SEGMENT_KINDS = {"copy": 0, "interp": 1, "restrict": 2, "reflux": 3, "init_keys": 4, "rate": 5, "finalize_dt": 6,
+                 "advance_time": 7}
+#: WB_PROGRAM_MAX_SEGMENTS
+PROGRAM_MAX_SEGMENTS = 64
+
+
+class ProgramParams(ctypes.Structure):
+    """wb_program_params."""
+
+    _fields_ = [
+        ("b0", c_double * 3),
+        ("gamma", c_double),
+        ("cfl", c_double),
+        ("dt_eta", c_double),
+        ("dt_kappa", c_double),
+        ("ndim", ctypes.c_int32),
+        ("ninstances", ctypes.c_int32),
+        ("nlevels", ctypes.c_int32),
+        ("advance", ctypes.c_int32),
+        ("reg", c_dp),
+        ("dt", c_dp),
+        ("time", c_dp),
+        ("end", c_dp),
+        ("keys", c_dp),
+        ("level_keys", c_dp),
+        ("inv_dx2_sum", c_dp),
+        ("inv_dx2_levels", c_dp),
+    ]

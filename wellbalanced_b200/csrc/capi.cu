@@ -513,8 +513,12 @@ int wb_reflux_apply(int precision, void* pool, const void* patches, const void* 
 int wb_struct_sizes(int64_t* sizes_host, int n) {
   set_error("");
   if (!sizes_host || n < 7) {
-    set_error("struct_sizes: needs room for 7 sizes");
+    set_error("struct_sizes: needs room for 7 sizes (9 with the op-program structs)");
     return kBadArgument;
+  }
+  if (n >= 9) {
+    sizes_host[7] = sizeof(wb_program_segment);
+    sizes_host[8] = sizeof(wb_program_params);
   }
   sizes_host[0] = sizeof(PatchDesc);
   sizes_host[1] = sizeof(Tile);

@@ -8,6 +8,7 @@
 #include <type_traits>
 
 #include "halo.cuh"
+#include "ops.cuh"
 #include "layout.cuh"
 #include "numerics.cuh"
 #include "wb_internal.cuh"
@@ -328,29 +329,13 @@ __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __
   }
 }
 
-// Apply the register of one interface to the coarse cells beside it, then clear it:
-// U -= sign * (0.5 dt) * reg / dx (sign +1 where the interface is the cell's upper face).
-// One block per op, no atomics: the ops of one launch must touch disjoint cells.
+// One block of 128 threads per op (ops.cuh reflux_op), no atomics: the ops of one launch
+// must touch disjoint cells.
 template <typename S>
 __global__ void reflux_apply_kernel(S* __restrict__ pool, const PatchDesc* __restrict__ patches,
                                     const RefluxOp* __restrict__ ops, double* __restrict__ reg,
                                     const double* __restrict__ dt) {
-  const RefluxOp op = ops[blockIdx.x];
-  const PatchDesc C = patches[op.coarse];
-  const double scale = 0.5 * dt[C.instance];
-  const int64_t count = int64_t(op.len) * op.ncomp;
-  for (int64_t t = threadIdx.x; t < count; t += blockDim.x) {
-    const int q = int(t / op.len), s = int(t % op.len);
-    const int s1 = s / op.width, s2 = s % op.width;
-    int idx[3] = {op.c[0], op.c[1], op.c[2]};
-    idx[op.t1] += s1;
-    if (op.t2 >= 0) idx[op.t2] += s2;
-    const int64_t o = cell_offset(C, idx[0], idx[1], idx[2]);
-    double& r = reg[op.reg_off + int64_t(q) * op.len + s];
-    S* u = pool + C.off + int64_t(op.field[q]) * C.fstride + o;
-    *u = S(double(*u) - op.sign * scale * r / op.dx);
-    r = 0.0;
-  }
+  reflux_op<S, 128>(pool, patches, ops[blockIdx.x], reg, dt);
 }
 
 template <typename S, typename R, bool PHYS>

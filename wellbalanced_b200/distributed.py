@@ -216,6 +216,7 @@ class RankLayout:
         local = [g for g in range(layout.npatches) if owner[g] == rank]
         self.local = local
         gmap = {g: i for i, g in enumerate(local)}
+        self._gmap = gmap
         self.own = [layout.own[g] for g in local]
         rows = [r.copy() for r in layout.rows[local]]
         offset = 0
@@ -369,12 +370,28 @@ class RankLayout:
         self.chunk_patch = np.array([gmap[int(c)] for c in layout.chunk_patch[keep]], dtype=np.int32)
         self.chunk_start = layout.chunk_start[keep].astype(np.int32)
         self.inv_dx2_sum = layout.inv_dx2_sum[:1].copy()
+        self.inv_dx2_levels = getattr(layout, "inv_dx2_levels", layout.inv_dx2_sum[:, None])[:1].copy()
         self.instances = np.zeros(len(local), dtype=np.int32)
         self.ninstances = 1
 
     @property
     def reflux_ops(self):
         return _concat(self.reflux_phases, _lib.REFLUX_OP)
+
+    def owns(self, patch):
+        """Whether the hierarchy's patch lives on this rank."""
+        return patch.index in self._gmap
+
+    def patch_view(self, pool, p, f):
+        """A view of field f of this rank's patch p (a hierarchy patch) in `pool`."""
+        r = self.rows[self._gmap[p.index]]
+        start = int(r["off"] + f * r["fstride"])
+        if self.ndim == 2:
+            X, P0 = p.shape[0] + 5, int(r["pitch0"])
+            return pool[start : start + X * P0].reshape(X, P0)[:, : p.shape[1] + 5]
+        X, Y = p.shape[0] + 5, p.shape[1] + 5
+        P0, P1 = int(r["pitch0"]), int(r["pitch1"])
+        return pool[start : start + X * P0].reshape(X, Y, P1)[:, :, : p.shape[2] + 5]
 
     def block(self, local_index):
         """(start, size) of a local patch's fields in the rank's pool."""
@@ -404,27 +421,56 @@ def _keys_from_max_form(k, keys):
 
 
 class TorchTransport:
-    """Exchange and reductions over a ``torch.distributed`` process group."""
+    """Exchange and reductions over a ``torch.distributed`` process group. With NCCL the
+    point-to-point transfers are ordered on the launching stream (`stream_ordered`); with
+    gloo the mailboxes go through host memory."""
 
     def __init__(self, group=None):
         import torch.distributed as dist
 
         self.dist = dist
         self.group = group
+        #: NCCL orders its transfers after the launching stream's pending work
+        self.stream_ordered = dist.get_backend(group) == "nccl"
+
+    def _host(self, view):
+        return view if self.stream_ordered else view.cpu()
 
     def exchange(self, pool, send, recv):
-        ops = []
+        ops, landed = [], []
         for peer, (start, length) in sorted(send.items()):
-            ops.append(self.dist.P2POp(self.dist.isend, pool[start : start + length], peer, self.group))
+            ops.append(self.dist.P2POp(self.dist.isend, self._host(pool[start : start + length]), peer, self.group))
         for peer, (start, length) in sorted(recv.items()):
-            ops.append(self.dist.P2POp(self.dist.irecv, pool[start : start + length], peer, self.group))
+            box = pool[start : start + length]
+            buffer = self._host(box)
+            landed.append((box, buffer))
+            ops.append(self.dist.P2POp(self.dist.irecv, buffer, peer, self.group))
         if ops:
             for request in self.dist.batch_isend_irecv(ops):
                 request.wait()
+        for box, buffer in landed:
+            if buffer is not box:
+                box.copy_(buffer)
+
+    def reduce_min_keys(self, keys):
+        """All-reduce MIN of order-preserving keys (as a MAX of their complements)."""
+        k = torch.bitwise_not(keys.view(torch.int64))
+        if self.stream_ordered:
+            self.dist.all_reduce(k, op=self.dist.ReduceOp.MAX, group=self.group)
+        else:
+            host = k.cpu()
+            self.dist.all_reduce(host, op=self.dist.ReduceOp.MAX, group=self.group)
+            k.copy_(host)
+        keys.view(torch.int64).copy_(torch.bitwise_not(k))
 
     def reduce_keys(self, keys):
         k = _keys_to_max_form(keys)
-        self.dist.all_reduce(k, op=self.dist.ReduceOp.MAX, group=self.group)
+        if self.stream_ordered:
+            self.dist.all_reduce(k, op=self.dist.ReduceOp.MAX, group=self.group)
+        else:
+            host = k.cpu()
+            self.dist.all_reduce(host, op=self.dist.ReduceOp.MAX, group=self.group)
+            k.copy_(host)
         _keys_from_max_form(k, keys)
 
 
@@ -436,6 +482,8 @@ class DistributedEngine(Engine):
         super().__init__(None, layout=rank_layout, **options)
         self.transport = transport
         self.overlap_fluxes = False  # the flux round's exchange runs on the engine's stream
+        # exchange rounds run between the levels' fills and restrictions: no op programs
+        self.use_programs = False
         self.rounds = {}
         for key, rd in rank_layout.rounds.items():
             ops = size_ops(rd.pack_ops) if rd.pack_ops.size else rd.pack_ops
@@ -450,11 +498,15 @@ class DistributedEngine(Engine):
             self.launches += 1
 
     def exchange(self, pool, key):
-        """Pack, then swap the mailboxes of round `key` with the peers."""
+        """Pack, then swap the mailboxes of round `key` with the peers. A transport on the
+        device's stream (NCCL: its sends start after the pack on that stream and the
+        stream waits for its receives) needs no host synchronisation; any other transport
+        gets the packed mailboxes after the stream has drained."""
         self.pack(pool, key)
         _, _, send, recv = self.rounds[key]
         if send or recv:
-            torch.cuda.current_stream(self.device).synchronize()
+            if not getattr(self.transport, "stream_ordered", False):
+                torch.cuda.current_stream(self.device).synchronize()
             self.transport.exchange(pool, send, recv)
 
     def fill(self, pool, levels=None):
@@ -476,6 +528,8 @@ class DistributedEngine(Engine):
 
     def finalize_dt(self, cfl, eta=0.0, kappa=0.0, *, clip_to_end=False, advance=False):
         self.transport.reduce_keys(self.keys)
+        if self.per_level_dt:
+            self.transport.reduce_min_keys(self.level_keys)
         Engine.finalize_dt(self, cfl, eta, kappa, clip_to_end=clip_to_end, advance=advance)
 
     def step(self, cfl):

@@ -19,6 +19,7 @@ memory and streams only; every numerical kernel is in ``libwb200.so``.
 from __future__ import annotations
 
 import contextlib
+import ctypes
 
 import numpy as np
 import torch
@@ -143,6 +144,13 @@ class Engine:
         self._flux_events = None
         #: the launching stream's handle while a step issues its launches (looked up once)
         self._step_stream = None
+        #: run the reflux, restriction, halo-fill and stable-step phases between the stage
+        #: kernels as op programs (`wb_run_program`, one launch each) on refined hierarchies
+        self.use_programs = self.max_level > 0
+        self._programs = {}
+        #: dt on the device belongs to the current state (set by `prime_dt` and each
+        #: programmed step; cleared by every other launch or write that changes the state)
+        self.dt_ready = False
 
     # low-level launches ----------------------------------------------------------------------
     def _s(self):
@@ -324,6 +332,7 @@ class Engine:
 
     def heun_step(self, groups_potential, groups_all):
         """One Heun step with the dt already in self.dt (device), refluxed and restricted."""
+        self.dt_ready = False
         with self.launching():
             self._heun_launches(groups_potential, groups_all)
 
@@ -367,6 +376,141 @@ class Engine:
         if refined:
             self.restrict(U, groups_all)
         self.fill(U)
+
+    # op programs ------------------------------------------------------------------------------
+    def _fill_phases(self, pool):
+        """Phases of the halo fill of every level of pool (0: the state, 1: the stage pool),
+        as `fill` launches them."""
+        phases = []
+        for level in range(len(self.copy_phases)):
+            same, nsame, boundary = self.copy_phases[level]
+            interp, ninterp = self.interp_levels[level]
+            # the interpolation ops are trimmed to the points no copy writes: one phase
+            phases.append([s for s in (("interp", pool, interp, ninterp), ("copy", pool, same, nsame)) if s[3]])
+            phases.extend([("copy", pool, ops, nops)] for ops, nops in boundary if nops)
+        return phases
+
+    def _restrict_phases(self, pool, groups):
+        """Phases of the restriction of `groups` in pool, finest level first, as `restrict`
+        launches them."""
+        key = frozenset(groups)
+        phases = []
+        for level in range(self.max_level, 0, -1):
+            merged = self.restrict_merged.get(level)
+            if merged is not None and merged[0] == key:
+                phases.append([("restrict", pool, merged[1], merged[2])] if merged[2] else [])
+            else:
+                phases.append([("restrict", pool, *self.restrict_levels[level][g]) for g in groups
+                               if self.restrict_levels[level][g][1]])
+        return phases
+
+    def _program(self, phases, dt_params=None):
+        """An op program (segment records, parameters, counters) from phases of segments
+        (kind, pool, ops tensor or None, count[, aux tensor]); empty phases dropped."""
+        phases = [p for p in phases if p]
+        rows = []
+        for k, phase in enumerate(phases):
+            for seg in phase:
+                kind, pool, ops, count = seg[:4]
+                aux = seg[4] if len(seg) > 4 else None
+                rows.append((_lib.SEGMENT_KINDS[kind], pool, k, int(count), 0, 0,
+                             0 if ops is None else ops.data_ptr(), 0 if aux is None else aux.data_ptr()))
+        if len(rows) > _lib.PROGRAM_MAX_SEGMENTS:
+            raise ValueError(f"an op program of {len(rows)} segments (at most {_lib.PROGRAM_MAX_SEGMENTS})")
+        segments = np.array(rows, dtype=_lib.PROGRAM_SEGMENT) if rows else np.zeros(0, _lib.PROGRAM_SEGMENT)
+        params = _lib.ProgramParams()
+        for a in range(3):
+            params.b0[a] = self.mean_field[a]
+        params.gamma = self.gamma
+        params.ndim = self.ndim
+        params.ninstances = self.ninstances
+        params.nlevels = self.nlevels
+        params.reg = self.register.data_ptr()
+        params.dt = self.dt.data_ptr()
+        params.time = self.time.data_ptr()
+        params.keys = self.keys.data_ptr()
+        params.inv_dx2_sum = self.inv_dx2_sum.data_ptr()
+        params.inv_dx2_levels = self.inv_dx2_levels.data_ptr()
+        if self.per_level_dt:
+            params.level_keys = self.level_keys.data_ptr()
+        if dt_params is not None:
+            params.cfl, params.dt_eta, params.dt_kappa = dt_params
+        counters = torch.zeros(3 + len(phases), dtype=torch.int32, device=self.device)
+        return segments, params, counters
+
+    def programs(self, groups_potential, groups_all, dt_params=None):
+        """The two op programs of a step: after stage 1 the restriction of the stage pool's
+        potential and its halo fill; after stage 2 the reflux, the state's restriction and
+        halo fill and, with dt_params (cfl, eta, kappa), the time advanced by this step's
+        dt first and the next step's dt from the new state last."""
+        key = (tuple(groups_potential), tuple(groups_all), dt_params, self.per_level_dt)
+        found = self._programs.get(key)
+        if found is None:
+            first = self._restrict_phases(1, groups_potential) + self._fill_phases(1)
+            second = [[("advance_time", 0, None, 1), ("init_keys", 0, None, 1)]] if dt_params is not None else []
+            size = _lib.REFLUX_OP.itemsize
+            second += [[("reflux", 0, self.reflux_ops[start * size:], count)] for start, count in self.reflux_phases]
+            second += self._restrict_phases(0, groups_all) + self._fill_phases(0)
+            if dt_params is not None:
+                if self.nchunks:
+                    second.append([("rate", 0, self.chunk_patch, self.nchunks, self.chunk_start)])
+                second.append([("finalize_dt", 0, None, 1)])
+            found = (self._program(first), self._program(second, dt_params))
+            self._programs[key] = found
+        return found
+
+    def run_program(self, program):
+        segments, params, counters = program
+        if segments.size == 0:
+            return
+        _lib.call("wb_run_program", self.precision, self.state.data_ptr(), self.stage_pool.data_ptr(),
+                  self.patches.data_ptr(), segments.ctypes.data, int(segments.size), ctypes.addressof(params),
+                  counters.data_ptr(), self._s())
+        self.launches += 1
+
+    def program_error(self):
+        """The error bits the op programs have set since the last call (0: none); cleared."""
+        bits = 0
+        for pair in self._programs.values():
+            for _, _, counters in pair:
+                bits |= int(counters[2].item())
+                counters[2].zero_()
+        return bits
+
+    def prime_dt(self, cfl, eta=0.0, kappa=0.0):
+        """dt of the next programmed step from the current state (time not advanced)."""
+        with self.launching():
+            self.rate()
+            self.finalize_dt(cfl, eta, kappa, advance=False)
+        self.dt_ready = True
+
+    def programmed_step(self, groups_potential, groups_all, cfl, eta=0.0, kappa=0.0):
+        """One Heun step through op programs at the dt on the device (`prime_dt` before the
+        first, then each step leaves the next one): stage 1, the register's face fluxes
+        (beside program 1), program 1, stage 2, face fluxes, program 2. Equal, bit for
+        bit, to rate, finalize_dt(advance) and `heun_step` at the same dt."""
+        first, second = self.programs(groups_potential, groups_all, (float(cfl), float(eta), float(kappa)))
+        with self.launching():
+            U, U1 = self.state, self.stage_pool
+            self.stage(U, None, U1)
+            side = None
+            if self.overlap_fluxes and self.nface:
+                if self._flux_stream is None:
+                    self._flux_stream = torch.cuda.Stream(self.device)
+                    self._flux_events = (torch.cuda.Event(), torch.cuda.Event())
+                side, main = self._flux_stream, self._main()
+                forked, joined = self._flux_events
+                forked.record(main)
+                side.wait_event(forked)
+            self.face_fluxes(U, side)
+            self.run_program(first)
+            if side is not None:
+                joined.record(side)
+                main.wait_event(joined)  # stage 1's fluxes have read U before stage 2 writes it
+            self.stage(U1, U, U)
+            self.face_fluxes(U1)
+            self.run_program(second)
+        self.dt_ready = True  # the second program left the next step's dt
 
     # host views --------------------------------------------------------------------------------
     def view(self, pool, patch, field):

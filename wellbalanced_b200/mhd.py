@@ -268,6 +268,7 @@ class MHD2D:
         return 0.5 * (bxf[:-1] + bxf[1:]), 0.5 * (byf[:, :-1] + byf[:, 1:])
 
     def _write(self, patch, field, values):
+        self.engine.dt_ready = False
         n = values.shape
         view = self.engine.view(self.engine.state, patch, field)
         view[HALO : HALO + n[0], HALO : HALO + n[1]] = torch.from_numpy(np.require(values, requirements=("C", "W"))).to(
@@ -314,6 +315,7 @@ class MHD2D:
         self._after_state()
 
     def _after_state(self):
+        self.engine.dt_ready = False
         eng = self.engine
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
@@ -342,6 +344,8 @@ class MHD2D:
         return float(eng.dt[0].item())
 
     def _raise_if_bad(self):
+        if self.engine.use_programs and self.engine.program_error():
+            raise RuntimeError("an op program's phase wait ran out (its device error word is set)")
         if int(self.engine.bad.item()):
             raise FloatingPointError(f"non-positive density or pressure (or non-finite values) at t = {self.time}")
 
@@ -375,17 +379,27 @@ class MHD2D:
         return taken
 
     def _one_step(self):
-        """The launches of one step at the stable dt (dt, time and state on the device)."""
+        """The launches of one step at the stable dt (dt, time and state on the device).
+        With op programs (refined hierarchies) dt is already on the device: `_prime`
+        before the first step, then each step's second program leaves the next one."""
         eng = self.engine
+        if eng.use_programs:
+            eng.programmed_step(self._groups_potential, self._groups_all, self.cfl, self.resistivity, max(self.conduction))
+            return
         with eng.launching():
             eng.rate()
             eng.finalize_dt(self.cfl, self.resistivity, max(self.conduction), advance=True)
             eng.heun_step(self._groups_potential, self._groups_all)
 
+    def _prime(self):
+        if self.engine.use_programs and not self.engine.dt_ready:
+            self.engine.prime_dt(self.cfl, self.resistivity, max(self.conduction))
+
     def capture(self) -> None:
         """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
         graph that `advance` replays. The recording takes one step. A regrid drops it."""
         self._check_ready()
+        self._prime()
         self._graph = self.engine.capture(self._one_step)
         self.steps += 1
         self.time = float(self.engine.time[0].item())
@@ -396,6 +410,7 @@ class MHD2D:
         self._check_ready()
         eng = self.engine
         eng.bad.zero_()
+        self._prime()
         for _ in range(steps):
             if self._graph is not None:
                 self._graph.replay()
@@ -408,46 +423,12 @@ class MHD2D:
 
     # refinement ----------------------------------------------------------------------------------
     def current_tags(self, threshold: float, levels: int) -> dict[int, np.ndarray]:
-        """Tag cells where ``|J_z|`` times the cell size exceeds ``threshold`` (``mhd.py:1011-1041``)."""
-        self._check_ready()
-        h = self.hierarchy
-        tags = {level: np.zeros(h.level_shape(level), dtype=bool) for level in range(min(levels, h.max_level + 1))}
-        for patch in h.patches:
-            if patch.level not in tags:
-                continue
-            nx, ny = patch.shape
-            dx, dy = h.spacing(patch.level)
-            az = self.engine.view(self.engine.state, patch, 6).to(torch.float64)
-            # face fields of the haloed block, then J_z at its inner nodes
-            bxf = (az[:, 1:] - az[:, :-1]) / dy + self.mean_field[0]
-            byf = -(az[1:, :] - az[:-1, :]) / dx + self.mean_field[1]
-            bxf = bxf[: nx + 5, : ny + 4]
-            byf = byf[: nx + 4, : ny + 5]
-            jz = torch.abs((byf[1:, 1:-1] - byf[:-1, 1:-1]) / dx - (bxf[1:-1, 1:] - bxf[1:-1, :-1]) / dy)
-            h1 = HALO - 1
-            cell = 0.25 * sum(jz[h1 + a : h1 + a + nx, h1 + b : h1 + b + ny] for a in (0, 1) for b in (0, 1))
-            (i0, i1), (j0, j1) = patch.box
-            tags[patch.level][i0:i1, j0:j1] |= (cell * max(dx, dy) > threshold).cpu().numpy()
-        return tags
+        """Tag cells where ``|J_z|`` (the mean over the cell's four nodes) times the cell
+        size exceeds ``threshold`` (``carafe/mhd.py:1011-1041``): one kernel over every
+        cell of the tagged levels (``wb_current_tags``)."""
+        from wellbalanced_b200.regrid import device_tags
 
-    # raw device state (checkpoint / host buffers) ------------------------------------------------
-    def save(self, host=None):
-        """Copy the device state pool into ``host`` (a pinned CPU tensor, allocated if None);
-        returns it once the copy has landed."""
-        pool = self.engine.state
-        if host is None:
-            host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
-        host.copy_(pool, non_blocking=True)
-        torch.cuda.current_stream(pool.device).synchronize()
-        return host
-
-    def load(self, host) -> None:
-        """Replace the device state pool by ``host`` (from `save`, same hierarchy and precision)."""
-        pool = self.engine.state
-        if tuple(host.shape) != tuple(pool.shape) or host.dtype != pool.dtype:
-            raise ValueError("the saved state belongs to another layout or precision")
-        pool.copy_(host, non_blocking=True)
-        self._ready = True
+        return device_tags(self, threshold, levels)
 
     def regrid(self, tags: dict[int, np.ndarray], **options: Any) -> None:
         """Regrid on ``tags`` (``carafe/mhd.py:1043-1056``): new patches over the tagged

@@ -222,6 +222,7 @@ class MHD3D:
         return tuple(slice(HALO, HALO + n + e) for n, e in zip(patch.shape, extra, strict=True))
 
     def _write(self, patch, field, values, extra=(0, 0, 0)):
+        self.engine.dt_ready = False
         view = self.engine.view(self.engine.state, patch, field)
         view[self._slices(patch, extra)] = torch.from_numpy(np.require(values, requirements=("C", "W"))).to(view.device, view.dtype)
 
@@ -272,6 +273,7 @@ class MHD3D:
         self._after_state()
 
     def _after_state(self):
+        self.engine.dt_ready = False
         eng = self.engine
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
@@ -299,6 +301,8 @@ class MHD3D:
         return float(eng.dt[0].item())
 
     def _raise_if_bad(self):
+        if self.engine.use_programs and self.engine.program_error():
+            raise RuntimeError("an op program's phase wait ran out (its device error word is set)")
         if int(self.engine.bad.item()):
             raise FloatingPointError(f"non-positive density or pressure (or non-finite values) at t = {self.time}")
 
@@ -330,17 +334,27 @@ class MHD3D:
         return taken
 
     def _one_step(self):
-        """The launches of one step at the stable dt (dt, time and state on the device)."""
+        """The launches of one step at the stable dt (dt, time and state on the device).
+        With op programs (refined hierarchies) dt is already on the device: `_prime`
+        before the first step, then each step's second program leaves the next one."""
         eng = self.engine
+        if eng.use_programs:
+            eng.programmed_step(self._groups_potential, self._groups_all, self.cfl, self.resistivity, 0.0)
+            return
         with eng.launching():
             eng.rate()
             eng.finalize_dt(self.cfl, self.resistivity, 0.0, advance=True)
             eng.heun_step(self._groups_potential, self._groups_all)
 
+    def _prime(self):
+        if self.engine.use_programs and not self.engine.dt_ready:
+            self.engine.prime_dt(self.cfl, self.resistivity, 0.0)
+
     def capture(self) -> None:
         """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
         graph that `advance` replays. The recording takes one step. A regrid drops it."""
         self._check_ready()
+        self._prime()
         self._graph = self.engine.capture(self._one_step)
         self.steps += 1
         self.time = float(self.engine.time[0].item())
@@ -350,6 +364,7 @@ class MHD3D:
         self._check_ready()
         eng = self.engine
         eng.bad.zero_()
+        self._prime()
         for _ in range(steps):
             if self._graph is not None:
                 self._graph.replay()
@@ -373,6 +388,7 @@ class MHD3D:
 
     def load(self, host) -> None:
         """Replace the device state pool by ``host`` (from `save`, same hierarchy and precision)."""
+        self.engine.dt_ready = False
         pool = self.engine.state
         if tuple(host.shape) != tuple(pool.shape) or host.dtype != pool.dtype:
             raise ValueError("the saved state belongs to another layout or precision")
@@ -382,38 +398,11 @@ class MHD3D:
     # refinement ----------------------------------------------------------------------------------
     def current_tags(self, threshold: float, levels: int) -> dict[int, np.ndarray]:
         """Tag cells where ``|J|`` (central differences of the cell field) times the cell
-        size exceeds ``threshold`` (``carafe/mhd3d.py:771-801``)."""
-        self._check_ready()
-        h = self.hierarchy
-        tags = {level: np.zeros(h.level_shape(level), dtype=bool) for level in range(min(levels, h.max_level + 1))}
-        for patch in h.patches:
-            if patch.level not in tags:
-                continue
-            spacing = h.spacing(patch.level)
-            eng = self.engine
-            nx, ny, nz = patch.shape
-            X, Y, Z = nx + 4, ny + 4, nz + 4
-            pot = (
-                eng.view(eng.state, patch, 5)[:X, : Y + 1, : Z + 1].to(torch.float64),
-                eng.view(eng.state, patch, 6)[: X + 1, :Y, : Z + 1].to(torch.float64),
-                eng.view(eng.state, patch, 7)[: X + 1, : Y + 1, :Z].to(torch.float64),
-            )
-            faces = []
-            for a in range(3):
-                _, b, c = _cyclic(a)
-                faces.append(torch.diff(pot[c], dim=b) / spacing[b] - torch.diff(pot[b], dim=c) / spacing[c]
-                             + self.mean_field[a])
-            cells = [0.5 * (f.narrow(a, 0, f.shape[a] - 1) + f.narrow(a, 1, f.shape[a] - 1)) for a, f in enumerate(faces)]
-            square = 0.0
-            for c in range(3):
-                _, a, b = _cyclic(c)
-                jc = torch.gradient(cells[b], spacing=spacing[a], dim=a)[0] - torch.gradient(
-                    cells[a], spacing=spacing[b], dim=b)[0]
-                square = square + jc**2
-            size = torch.sqrt(square)[HALO:-HALO, HALO:-HALO, HALO:-HALO]
-            index = tuple(slice(lo, hi) for lo, hi in patch.box)
-            tags[patch.level][index] |= (size * max(spacing) > threshold).cpu().numpy()
-        return tags
+        size exceeds ``threshold`` (``carafe/mhd3d.py:771-801``): one kernel over every
+        cell of the tagged levels (``wb_current_tags``)."""
+        from wellbalanced_b200.regrid import device_tags
+
+        return device_tags(self, threshold, levels)
 
     def regrid(self, tags: dict[int, np.ndarray], **options: Any) -> None:
         """Regrid on ``tags`` (``carafe/mhd3d.py:803-816``); the potential is interpolated and

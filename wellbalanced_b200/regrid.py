@@ -245,8 +245,11 @@ def _merge_periodic_planes(values, mask, extra, periodic, shape):
         mask[last] = mask[first]
 
 
-def regrid_model(model, tags, **options):
-    """Regrid ``model`` (an `MHD2D` / `MHD3D`) on ``tags`` and move its state over."""
+def regrid_model_host(model, tags, **options):
+    """Regrid ``model`` (an `MHD2D` / `MHD3D`) on ``tags`` with the transfer restated on the
+    host, level by level on dense arrays (the state goes to the host and back). The
+    solvers regrid with `regrid_model` (the transfer on the device); this restatement is
+    what the tests check the device transfer against."""
     model._check_ready()
     old_h = model.hierarchy
     extras = model._field_extras()
@@ -289,3 +292,179 @@ def regrid_model(model, tags, **options):
     model._after_state()
     model.time, model.steps = time, steps
     model.engine.time.fill_(time)
+
+
+# ---- the transfer on the device ------------------------------------------------------------
+#: mirror of the device prolongation op (wellbalanced_b200/csrc/transfer.cu ProlongOp)
+PROLONG_OP = np.dtype(
+    {
+        "names": ["fine", "coarse", "field_lo", "field_hi", "node_mask", "ndim", "n", "d", "fine_lo", "coarse_lo",
+                  "coarse_n", "periodic"],
+        "formats": ["<i4"] * 6 + [("<i4", 3)] * 5 + ["<i4"],
+        "itemsize": 88,
+    }
+)
+
+#: points per transfer op (one 128-thread block each)
+TRANSFER_OP_POINTS = 4096
+
+
+def _ranges(patches, node_mask, ndim):
+    """(lo, hi) level index ranges of the patches' points of a field group: cells, and one
+    node more along node axes; arrays (patches, ndim)."""
+    lo = np.array([[p.box[a][0] for a in range(ndim)] for p in patches], dtype=np.int64).reshape(-1, ndim)
+    hi = np.array([[p.box[a][1] + ((node_mask >> a) & 1) for a in range(ndim)] for p in patches],
+                  dtype=np.int64).reshape(-1, ndim)
+    return lo, hi
+
+
+def _cut(n, chunk=TRANSFER_OP_POINTS):
+    """Sub-boxes (offset, extent) of a box of extents n (3 axes, the last fastest) of at
+    most `chunk` points: whole planes or rows where they fit."""
+    inner = int(n[1]) * int(n[2])
+    if inner <= chunk:
+        step = max(1, chunk // max(1, inner))
+        return [((a, 0, 0), (min(step, int(n[0]) - a), int(n[1]), int(n[2]))) for a in range(0, int(n[0]), step)]
+    step = max(1, chunk // max(1, int(n[2])))
+    return [((a, b, 0), (1, min(step, int(n[1]) - b), int(n[2]))) for a in range(int(n[0]))
+            for b in range(0, int(n[1]), step)]
+
+
+def _pad3(v, fill=0):
+    v = [int(x) for x in v]
+    return v + [fill] * (3 - len(v))
+
+
+def transfer_ops(old_h, new_h, groups, ndim):
+    """Per level of the new hierarchy: (prolongation ops from the new coarser level,
+    kept-value ops from the old hierarchy's patches of that level, periodic images
+    included)."""
+    periodic = new_h.periodic
+    pmask = sum(1 << a for a in range(ndim) if periodic[a])
+    out = []
+    for level in range(new_h.max_level + 1):
+        shape = new_h.level_shape(level)
+        prolong, kept = [], []
+        fines = new_h.patches_at_level(level)
+        olds = old_h.patches_at_level(level) if level <= old_h.max_level else []
+        coarses = new_h.patches_at_level(level - 1) if level else []
+        shifts = list(itertools.product(*[(-shape[a], 0, shape[a]) if periodic[a] else (0,) for a in range(ndim)]))
+        for g in groups:
+            flo, fhi = _ranges(fines, g.node_mask, ndim)
+            if olds:
+                olo, ohi = _ranges(olds, g.node_mask, ndim)
+                for sh in shifts:
+                    sh = np.array(sh, dtype=np.int64)
+                    lo = np.maximum(flo[:, None, :], olo[None, :, :] + sh)
+                    hi = np.minimum(fhi[:, None, :], ohi[None, :, :] + sh)
+                    for i, j in zip(*np.nonzero(np.all(hi > lo, axis=2)), strict=True):
+                        n = _pad3(hi[i, j] - lo[i, j], 1)
+                        for off, ext in _cut(n):
+                            d = _pad3(lo[i, j] - flo[i] + HALO)
+                            s = _pad3(lo[i, j] - (olo[j] + sh) + HALO)
+                            kept.append((fines[i].index, olds[j].index, g.lo, g.hi,
+                                         [d[a] + off[a] for a in range(3)], [s[a] + off[a] for a in range(3)], ext))
+            if coarses:
+                clo = np.array([[c.box[a][0] for a in range(ndim)] for c in coarses], dtype=np.int64)
+                chi = np.array([[c.box[a][1] for a in range(ndim)] for c in coarses], dtype=np.int64)
+                node = np.array([(g.node_mask >> a) & 1 for a in range(ndim)], dtype=np.int64)
+                # fine points whose coarse stencil (the parent cell; the two nodes along a node
+                # axis) lies in the coarse patch
+                lo = np.maximum(flo[:, None, :], 2 * clo[None, :, :])
+                hi = np.minimum(fhi[:, None, :], 2 * chi[None, :, :] + node)
+                coarse_n = _pad3(new_h.level_shape(level - 1), 1)
+                for i, j in zip(*np.nonzero(np.all(hi > lo, axis=2)), strict=True):
+                    n = _pad3(hi[i, j] - lo[i, j], 1)
+                    d0 = _pad3(lo[i, j] - flo[i] + HALO)
+                    for off, ext in _cut(n):
+                        prolong.append((fines[i].index, coarses[j].index, g.lo, g.hi, g.node_mask, ndim, ext,
+                                        [d0[a] + off[a] for a in range(3)], _pad3(flo[i]), _pad3(clo[j]), coarse_n,
+                                        pmask))
+        p = np.zeros(len(prolong), PROLONG_OP)
+        for k, r in enumerate(prolong):
+            p[k] = r
+        k_ops = np.zeros(len(kept), _lib.COPY_OP)
+        for k, (dst, src, lo_f, hi_f, d, s, ext) in enumerate(kept):
+            k_ops[k] = (dst, src, -1, lo_f, hi_f, -1, ext, d, s, (1, 1, 1), (0, 0, 0), (0, 0, 0), 1.0, 0.0)
+        out.append((p, k_ops))
+    return out
+
+
+def regrid_model_device(model, tags, **options):
+    """Regrid ``model`` on ``tags`` with the state moved on the device: the clustering on the
+    host (from the tags), the transfer by the prolongation and kept-value kernels level by
+    level, the new levels' halos filled between them; no state round trip to the host."""
+    import torch
+
+    from wellbalanced_b200.engine import _device_bytes
+
+    model._check_ready()
+    old_h, old_engine = model.hierarchy, model.engine
+    new_h = old_h.regrid(tags, **options)
+    time, steps = model.time, model.steps
+    model.hierarchy = new_h
+    model._build_engine()
+    eng = model.engine
+    stream = eng._s()
+    for level, (prolong, kept) in enumerate(transfer_ops(old_h, new_h, eng.layout.groups, eng.ndim)):
+        if prolong.size:
+            ops = _device_bytes(prolong, eng.device, PROLONG_OP)
+            _lib.call("wb_prolong_ops", eng.precision, eng.state.data_ptr(), eng.patches.data_ptr(), ops.data_ptr(),
+                      int(prolong.size), stream)
+        if kept.size:
+            ops = _device_bytes(kept, eng.device, _lib.COPY_OP)
+            _lib.call("wb_kept_ops", eng.precision, eng.state.data_ptr(), eng.patches.data_ptr(),
+                      old_engine.state.data_ptr(), old_engine.patches.data_ptr(), ops.data_ptr(), int(kept.size),
+                      stream)
+        eng.fill(eng.state, levels={level})
+    torch.cuda.current_stream(eng.device).synchronize()
+    del old_engine
+    model._after_state()
+    model.time, model.steps = time, steps
+    eng.time.fill_(time)
+
+
+def regrid_model(model, tags, **options):
+    """Regrid ``model`` on ``tags``: clustering on the host, the state moved on the device."""
+    regrid_model_device(model, tags, **options)
+
+
+# ---- the plain tagger on the device ---------------------------------------------------------
+#: where a patch's cells go in the levels' tag arrays (TagPlace in csrc/tags.cu)
+TAG_PLACE = np.dtype({"names": ["base", "s0", "s1"], "formats": ["<i8", "<i8", "<i8"], "itemsize": 24})
+
+
+def device_tags(model, threshold, levels):
+    """``current_tags`` by one kernel over every cell of the tagged levels (|J| dx >
+    threshold), written into the levels' dense arrays on the device and read back once."""
+    import torch
+
+    from wellbalanced_b200.engine import _device_bytes
+
+    model._check_ready()
+    h, eng = model.hierarchy, model.engine
+    nlev = min(levels, h.max_level + 1)
+    shapes = [tuple(h.level_shape(level)) for level in range(nlev)]
+    sizes = [int(np.prod(s)) for s in shapes]
+    offsets = np.cumsum([0, *sizes])
+    place = np.zeros(len(h.patches), TAG_PLACE)
+    for p in h.patches:
+        if p.level >= nlev:
+            continue
+        shape = shapes[p.level]
+        lo = [b[0] for b in p.box]
+        if h.ndim == 2:
+            place[p.index] = (offsets[p.level] + lo[0] * shape[1] + lo[1], shape[1], 0)
+        else:
+            s0, s1 = shape[1] * shape[2], shape[2]
+            place[p.index] = (offsets[p.level] + lo[0] * s0 + lo[1] * s1 + lo[2], s0, s1)
+    out = torch.zeros(max(int(offsets[-1]), 1), dtype=torch.uint8, device=eng.device)
+    if nlev and eng.nchunks:
+        b = eng.mean_field
+        _lib.call("wb_current_tags", eng.precision, h.ndim, eng.state.data_ptr(), eng.patches.data_ptr(),
+                  eng.chunk_patch.data_ptr(), eng.chunk_start.data_ptr(), eng.nchunks,
+                  _device_bytes(place, eng.device, TAG_PLACE).data_ptr(), nlev, b[0], b[1], b[2], float(threshold),
+                  out.data_ptr(), eng._s())
+    host = out.cpu().numpy()
+    return {level: host[offsets[level]:offsets[level + 1]].reshape(shapes[level]).astype(bool)
+            for level in range(nlev)}
