@@ -59,6 +59,9 @@ def parse():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-accuracy", action="store_true")
     parser.add_argument("--no-plain", action="store_true")
+    parser.add_argument("--partition", action="store_true",
+                        help="turbulence on N GPUs as ONE box of N slabs of --cells^3 (patches per rank, "
+                             "halo exchange over NCCL, a global dt) instead of N replicas")
     parser.add_argument("--no-extra", action="store_true",
                         help="turbulence at one GPU: skip the batch and Harris configurations measured beside it")
     parser.add_argument("--lx", default="auto", help="turbulence: x-planes per tile (an integer, or auto: tuned)")
@@ -285,6 +288,60 @@ class Turbulence:
         del ref, low
         torch.cuda.empty_cache()
         return out
+
+
+class PartitionedTurbulence(Turbulence):
+    """The turbulence workload as one periodic box of N slabs of n^3 cells along x, one slab
+    per rank (`AMRHierarchy(..., comm=group)`: the rank's patch, its halos exchanged with
+    the neighbour ranks over NCCL every fill, dt the global minimum): weak scaling of one
+    problem rather than N replicas. Every slab holds the same seeded n^3 fields, so the box
+    is periodic with period n along x."""
+
+    def __init__(self, args, rank):
+        import torch.distributed as dist
+
+        from wellbalanced_b200.mesh import AMRHierarchy
+        from wellbalanced_b200.mhd3d import MHD3D
+        from wellbalanced_b200.problems import conserved_3d, turbulence_3d
+
+        world = dist.get_world_size() if dist.is_initialized() else 1
+        self.n, self.rank, self.args, self.world = args.cells, rank, args, world
+        self.precision = getattr(args, "precision", 32)
+        n = self.n
+        lx = 32 if args.lx == "auto" else int(args.lx)
+        mesh = AMRHierarchy((n * world, n, n), ((0.0, float(world)), (0.0, 1.0), (0.0, 1.0)), periodic=(True,) * 3,
+                            comm=dist.group.WORLD if world > 1 else None, split=(world, 1, 1))
+        self.model = MHD3D(mesh, limiter="mc", cfl=0.3, precision=self.precision, lx=lx)
+        rho, velocity, p, potential = turbulence_3d(n, seed=0, gamma=self.model.gamma)
+        cells = conserved_3d(rho, velocity, p, potential, (1.0 / n,) * 3, gamma=self.model.gamma)
+        extras = ((0, 1, 1), (1, 0, 1), (1, 1, 0))
+        for patch in self.model._local():
+            for f, value in enumerate(cells):
+                self.model._write(patch, f, value)
+            for c, value in enumerate(potential):
+                self.model._write(patch, 5 + c, value, extras[c])
+        self.model._after_state()
+        self.model._ready = True
+        self.engine = self.model.engine
+        self.lx = lx
+        self.cells = n**3
+        self.model.lx_timings = None
+
+    @staticmethod
+    def describe(args):
+        return (f"3D decaying turbulence as one periodic box of N slabs of {args.cells}^3 (one per GPU, halos over "
+                "NCCL, global dt), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.3, float32 state")
+
+    def config(self):
+        out = super().config()
+        out["partition"] = f"{self.world} slabs of {self.n}^3 along x, one per rank"
+        return out
+
+    def plain(self, steps=3):
+        return None
+
+    def accuracy(self, steps=None):
+        return None
 
 
 def _kernel2d(engine):
@@ -803,7 +860,8 @@ def roofline(name, work, run):
 def workload_config(work, world, args, steps):
     eng = work.engine
     config = work.config()
-    config["parallelism"] = f"replicas x{world}"
+    config["parallelism"] = (f"one box in {world} slabs (patches per rank, NCCL halos)"
+                             if getattr(work, "world", None) else f"replicas x{world}")
     limit = getattr(work, "max_steps", None)
     if limit and steps > limit:
         config["timed_runs"] = (f"{-(-steps // limit)} runs of at most {limit} steps, each from the state "
@@ -885,7 +943,9 @@ def main():
         if world > 1:
             dist.barrier()
 
-    work = WORKLOADS[args.workload](args, rank)
+    if args.partition and args.workload != "turbulence":
+        raise SystemExit("--partition splits the turbulence box")
+    work = (PartitionedTurbulence if args.partition else WORKLOADS[args.workload])(args, rank)
     run = measure(work, args, rank, world, local, barrier, steps=args.steps, warmup=args.warmup,
                   e2e=not args.no_e2e)
     value, seconds = run["value"], run["seconds"]

@@ -253,7 +253,7 @@ typedef struct wb_program_segment {
   int32_t phase; /* 0 for the first segment, then equal to or one above the previous one */
   int32_t count; /* items */
   int32_t first; /* set by wb_run_program */
-  int32_t pad;
+  int32_t pad;   /* set by wb_run_program (ops per work item) */
   const void* ops;
   const void* aux;
 } wb_program_segment;

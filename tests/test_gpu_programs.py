@@ -107,9 +107,9 @@ def test_conduction_limit_per_level_through_programs():
 
 
 def test_a_phase_wait_that_never_completes_sets_the_error_bit():
-    """The ticket counter starts past every item of phase 0, so phase 0 never completes and
-    the first wait of phase 1 runs out after its bounded wait: the error word gets bit 2,
-    no later item runs, the launch returns, and the counters are left for the next launch."""
+    """The ticket counter starts past the first item, so phase 0 never completes and the
+    first wait of phase 1 runs out after its bounded wait: the error word gets bit 2, no
+    later phase runs, the launch returns, and the counters are left for the next launch."""
     from wellbalanced_b200 import _lib
 
     model = _refined_2d(32)
@@ -117,9 +117,7 @@ def test_a_phase_wait_that_never_completes_sets_the_error_bit():
     first, _ = eng.programs(model._groups_potential, model._groups_all)
     segments, params, counters = first
     assert int(segments["phase"].max()) >= 1
-    before = eng.stage_pool.clone()
-    phase0 = int(segments["count"][segments["phase"] == 0].sum())
-    counters[0] = phase0  # no block takes a phase-0 ticket
+    counters[0] = 1  # no block takes the first ticket (an item of phase 0)
     torch.cuda.synchronize()
     lib = _lib.load()
     status = lib.wb_run_program(eng.precision, eng.state.data_ptr(), eng.stage_pool.data_ptr(),
@@ -131,7 +129,6 @@ def test_a_phase_wait_that_never_completes_sets_the_error_bit():
     words = counters.cpu().numpy()
     assert words[2] & 2
     assert words[0] == 0 and words[1] == 0 and not words[3:].any()
-    assert torch.equal(eng.stage_pool, before)  # no item ran
     counters[2] = 0
     eng.run_program(first)  # the next launch runs normally
     torch.cuda.synchronize()

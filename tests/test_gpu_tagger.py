@@ -96,3 +96,16 @@ def test_learned_tags_anticipate_the_plain_tagger():
     # growing them by the smallest buffer that brings the miss rate under 1% tags more cells
     buffer = min(c for c in plain if plain[c]["miss"] < 0.01)
     assert buffer >= 1 and learned["tagged"] < plain[buffer]["tagged"]
+
+
+def test_learned_tags_allow_a_longer_regrid_interval():
+    """Regridding a refined multi-blast run on the learned tags keeps every cell the plain
+    tagger flags under a refined patch (under 1% missed) for a longer regrid interval than
+    regridding on the plain tags of the regrid step."""
+    from wellbalanced_b200.tagger import interval_study
+
+    out = interval_study(32, intervals=(2, 4, 8), train_steps=32, test_steps=16)
+    print({K: {k: round(v["miss"], 4) for k, v in runs.items()} for K, runs in out["intervals"].items()},
+          out["learned_interval"], out["plain_interval"])
+    assert out["learned_interval"] > out["plain_interval"]
+    assert out["intervals"][out["learned_interval"]]["learned"]["miss"] < 0.01

@@ -11,6 +11,12 @@
 
 namespace wb {
 
+// A thread's place among the NT threads that run one op (a whole block, or one warp of it).
+template <int NT>
+__device__ __forceinline__ unsigned op_lane() {
+  return threadIdx.x % unsigned(NT);
+}
+
 // element offset of haloed index (i, j, k) of a patch (k ignored in 2D)
 __device__ __forceinline__ int64_t offset_of(const PatchDesc& P, int i, int j, int k) {
   if (P.pitch1) return int64_t(i) * P.pitch0 + int64_t(j) * P.pitch1 + k;
@@ -28,7 +34,7 @@ __device__ __forceinline__ void copy_op(S* __restrict__ pool, const PatchDesc* _
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += NT) {
+  for (unsigned t = op_lane<NT>(); t < count; t += NT) {
     const unsigned line = t / n2;
     const int p2 = int(t - line * n2);
     const int p1 = int(line % n1);
@@ -64,7 +70,7 @@ __device__ __forceinline__ void copy_op_pairs(S* __restrict__ pool, const PatchD
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t0 = threadIdx.x; t0 < count; t0 += 2 * NT) {
+  for (unsigned t0 = op_lane<NT>(); t0 < count; t0 += 2 * NT) {
     S v[2][8];
     int64_t od[2];
 #pragma unroll
@@ -189,7 +195,7 @@ __device__ __forceinline__ void interp_op(S* __restrict__ pool, const PatchDesc*
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += NT) {
+  for (unsigned t = op_lane<NT>(); t < count; t += NT) {
     if (op.ndim == 3)
       interp_point<S, 3>(pool, F, C, op, t, n1, n2);
     else
@@ -213,7 +219,7 @@ __device__ __forceinline__ void restrict_op(S* __restrict__ pool, const PatchDes
   // 32-bit point index (the host keeps every op below 2^31 points)
   const unsigned n1 = unsigned(op.n[1]), n2 = unsigned(op.n[2]);
   const unsigned count = unsigned(op.n[0]) * n1 * n2;
-  for (unsigned t = threadIdx.x; t < count; t += NT) {
+  for (unsigned t = op_lane<NT>(); t < count; t += NT) {
     const unsigned line = t / n2;
     const int q2 = int(t - line * n2);
     const int q1 = int(line % n1);
@@ -255,7 +261,7 @@ __device__ __forceinline__ void reflux_op(S* __restrict__ pool, const PatchDesc*
   const PatchDesc C = patches[op.coarse];
   const double scale = 0.5 * dt[C.instance];
   const int64_t count = int64_t(op.len) * op.ncomp;
-  for (int64_t t = threadIdx.x; t < count; t += NT) {
+  for (int64_t t = op_lane<NT>(); t < count; t += NT) {
     const int q = int(t / op.len), s = int(t % op.len);
     const int s1 = s / op.width, s2 = s % op.width;
     int idx[3] = {op.c[0], op.c[1], op.c[2]};

@@ -7,10 +7,13 @@
 //
 // A program is a list of segments (an op list of one kind on one pool), grouped into
 // phases that run in order; the segments of a phase run together (their ops touch
-// disjoint points, as in the standalone launches). The work items of all segments are
-// numbered in program order and handed out by one ticket counter: a block takes the next
-// ticket, and before it runs an item of phase p it waits until every item of phase p - 1
-// has finished (a per-phase completion counter). Tickets go out in order, so a block only
+// disjoint points, as in the standalone launches). The work items of all segments — runs
+// of consecutive ops, about two per block and phase, so that a block pays the hand-out
+// cost once per run and not per op — are numbered in program order and handed out by one
+// ticket counter: a block takes the next ticket, and before it runs an item of phase p it
+// waits until every item of phase p - 1 has finished (a per-phase completion counter).
+// The halo, interpolation and restriction ops of an item go to the block's four warps,
+// one op per warp at a time (most of them are a few dozen points). Tickets go out in order, so a block only
 // ever waits for items that running blocks hold: the launch needs no co-residency of its
 // blocks (no cooperative launch, no grid barrier), and every wait is bounded (a second);
 // a wait that runs out sets the program's error word, and the blocks skip their remaining
@@ -22,6 +25,7 @@
 // programs equals, bit for bit, the step through the standalone launches.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 
@@ -36,6 +40,8 @@
 namespace wb {
 
 constexpr int kProgramThreads = 128;
+constexpr int kProgramWarps = kProgramThreads / 32;
+constexpr int kProgramMaxRun = 64;  // ops per item at most
 // launch bounds: 128 registers a thread (the interpolation's unrolled weights)
 constexpr int kProgramBlocksPerSM = 4;
 constexpr unsigned long long kProgramWaitNs = 1000000000ull;  // a second
@@ -99,6 +105,9 @@ __global__ void __launch_bounds__(kProgramThreads, kProgramBlocksPerSM)
     const wb_program_segment& sg = a.seg[k];
     const int item = t - sg.first;
     const int phase = sg.phase;
+    const int run = sg.pad;  // ops per item
+    const int op0 = item * run, op1 = min(sg.count, op0 + run);
+    const int warp = tid / 32;
     if (tid == 0) {
       const bool go = phase == 0 || wait_phase(done + phase - 1, unsigned(a.phase_total[phase - 1]), error);
       s_go = go && !load_acquire(error);
@@ -108,16 +117,21 @@ __global__ void __launch_bounds__(kProgramThreads, kProgramBlocksPerSM)
       S* pool = a.pools[sg.pool];
       switch (sg.kind) {
         case WB_SEG_COPY:
-          copy_op<S, kProgramThreads>(pool, a.patches, static_cast<const CopyOp*>(sg.ops)[item]);
+          for (int o = op0 + warp; o < op1; o += kProgramWarps)
+            copy_op<S, 32>(pool, a.patches, static_cast<const CopyOp*>(sg.ops)[o]);
           break;
         case WB_SEG_INTERP:
-          interp_op<S, kProgramThreads>(pool, a.patches, static_cast<const InterpOp*>(sg.ops)[item]);
+          for (int o = op0 + warp; o < op1; o += kProgramWarps)
+            interp_op<S, 32>(pool, a.patches, static_cast<const InterpOp*>(sg.ops)[o]);
           break;
         case WB_SEG_RESTRICT:
-          restrict_op<S, kProgramThreads>(pool, a.patches, static_cast<const RestrictOp*>(sg.ops)[item]);
+          for (int o = op0 + warp; o < op1; o += kProgramWarps)
+            restrict_op<S, 32>(pool, a.patches, static_cast<const RestrictOp*>(sg.ops)[o]);
           break;
         case WB_SEG_REFLUX:
-          reflux_op<S, kProgramThreads>(pool, a.patches, static_cast<const RefluxOp*>(sg.ops)[item], p.reg, p.dt);
+          // the ops of a reflux segment touch disjoint cells: the block's threads over each op
+          for (int o = op0; o < op1; ++o)
+            reflux_op<S, kProgramThreads>(pool, a.patches, static_cast<const RefluxOp*>(sg.ops)[o], p.reg, p.dt);
           break;
         case WB_SEG_INIT_KEYS:
           for (int i = tid; i < p.ninstances; i += kProgramThreads) {
@@ -129,13 +143,15 @@ __global__ void __launch_bounds__(kProgramThreads, kProgramBlocksPerSM)
           break;
         case WB_SEG_RATE: {
           const RateSlots slots{p.keys, p.ninstances, p.level_keys, p.nlevels, error};
-          const int patch = static_cast<const int*>(sg.ops)[item];
-          const int start = static_cast<const int*>(sg.aux)[item];
-          if (p.ndim == 2)
-            rate_chunk2d<S, kProgramThreads>(pool, a.patches, patch, start, p.b0[0], p.b0[1], p.gamma, slots);
-          else
-            rate_chunk3d<S, kProgramThreads>(pool, a.patches, patch, start, p.b0[0], p.b0[1], p.b0[2], p.gamma,
-                                             slots);
+          for (int o = op0; o < op1; ++o) {
+            const int patch = static_cast<const int*>(sg.ops)[o];
+            const int start = static_cast<const int*>(sg.aux)[o];
+            if (p.ndim == 2)
+              rate_chunk2d<S, kProgramThreads>(pool, a.patches, patch, start, p.b0[0], p.b0[1], p.gamma, slots);
+            else
+              rate_chunk3d<S, kProgramThreads>(pool, a.patches, patch, start, p.b0[0], p.b0[1], p.b0[2], p.gamma,
+                                               slots);
+          }
           break;
         }
         case WB_SEG_FINALIZE_DT:
@@ -174,7 +190,7 @@ namespace {
 // Blocks per SM the kernel's registers allow (queried once per instantiation and
 // device), times the SMs; no more blocks than items.
 template <typename S>
-int program_grid(int items) {
+int program_grid(int items, int capacity_only) {
   static std::mutex mutex;
   static int cached[64] = {};
   int device = 0;
@@ -187,12 +203,13 @@ int program_grid(int items) {
       return 0;
     cached[device] = per_sm * sms;
   }
+  if (capacity_only) return cached[device];
   return items < cached[device] ? items : cached[device];
 }
 
 template <typename S>
 int launch_program(const ProgramArgs<S>& a, cudaStream_t stream) {
-  const int grid = program_grid<S>(a.total);
+  const int grid = program_grid<S>(a.total, 0);
   if (grid <= 0) {
     set_error("run_program: occupancy query failed");
     return kCudaError;
@@ -243,8 +260,16 @@ int prepare(ProgramArgs<S>& a, const wb_program_segment* segments, int nsegments
                 k, sg.kind);
       return kBadArgument;
     }
+    // runs of ops: about two items per block of the grid, at most kProgramMaxRun ops each
+    const int capacity = program_grid<S>(0, 1);
+    if (capacity <= 0) {
+      set_error("run_program: occupancy query failed");
+      return kCudaError;
+    }
+    const bool runs = sg.kind <= WB_SEG_REFLUX || sg.kind == WB_SEG_RATE;
+    sg.pad = runs ? std::max(1, std::min(kProgramMaxRun, (sg.count + 2 * capacity - 1) / (2 * capacity))) : 1;
     sg.first = int(total);
-    total += sg.count;
+    total += (sg.count + sg.pad - 1) / sg.pad;
     if (total >= (int64_t(1) << 31) - (int64_t(1) << 20)) {
       set_error("run_program: too many items");
       return kTooLarge;
@@ -255,7 +280,7 @@ int prepare(ProgramArgs<S>& a, const wb_program_segment* segments, int nsegments
   a.nphases = phase + 1;
   a.total = int(total);
   for (int q = 0; q < a.nphases; ++q) a.phase_total[q] = 0;
-  for (int k = 0; k < nsegments; ++k) a.phase_total[a.seg[k].phase] += a.seg[k].count;
+  for (int k = 0; k < nsegments; ++k) a.phase_total[a.seg[k].phase] += (a.seg[k].count + a.seg[k].pad - 1) / a.seg[k].pad;
   return kOk;
 }
 

@@ -271,29 +271,34 @@ __device__ void face_flux(const S* src, const PatchDesc& P, int ndim, int axis, 
   for (int t = 0; t < ncons; ++t) out[t] = double(F[rows[t]]);
 }
 
-// One block per interface side: reg[slot] += mean of the fine faces over each coarse
-// face - the coarse face (each op holds both sides, so no two blocks share a slot). The
-// coarse face and its 2 (2D) or 4 (3D) fine faces are evaluated by separate threads
-// (kFluxThreads / K coarse faces per round), then one thread per coarse face combines
-// them from shared memory, the fine faces summed in the order (a, b).
+// One warp per interface side: reg[slot] += mean of the fine faces over each coarse face -
+// the coarse face (each op holds both sides, so no two warps share a slot). The coarse face
+// and its 2 (2D) or 4 (3D) fine faces are evaluated by separate lanes (32 / K coarse faces
+// per round), then one lane per coarse face combines them from shared memory, the fine
+// faces summed in the order (a, b). Most interfaces are a few coarse faces long, so a warp
+// (four ops per 128-thread block) keeps the lanes busy where a block per op would not.
 constexpr int kFluxThreads = 128;
+constexpr int kFluxWarps = kFluxThreads / 32;
 
 template <typename S, typename R, int LIM, bool PHYS>
 __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __restrict__ pool,
                                                                      const PatchDesc* __restrict__ patches,
-                                                                     const FaceFluxOp* __restrict__ ops, double b0x,
-                                                                     double b0y, double b0z, double gamma,
+                                                                     const FaceFluxOp* __restrict__ ops, int nops,
+                                                                     double b0x, double b0y, double b0z, double gamma,
                                                                      FacePhysics phys, double* __restrict__ reg) {
-  __shared__ double g[kFluxThreads][6];
-  const FaceFluxOp op = ops[blockIdx.x];
+  __shared__ double g_all[kFluxWarps][32][6];
+  const int warp = threadIdx.x / 32, t = threadIdx.x % 32;
+  const int index = blockIdx.x * kFluxWarps + warp;
+  if (index >= nops) return;  // a whole warp: no block-wide barrier follows
+  double(*g)[6] = g_all[warp];
+  const FaceFluxOp op = ops[index];
   const PatchDesc C = patches[op.coarse];
   const PatchDesc F = patches[op.fine];
   const double b0[3] = {b0x, b0y, b0z};
   const int ncons = op.ndim == 2 ? 6 : 5;
   const int fine_b = op.ndim == 3 ? 2 : 1;
-  const int K = 1 + 2 * fine_b;        // evaluations per coarse face
-  const int per = kFluxThreads / K;    // coarse faces per round
-  const int t = threadIdx.x;
+  const int K = 1 + 2 * fine_b;  // evaluations per coarse face
+  const int per = 32 / K;        // coarse faces per round
   const int e = t % K;
   for (int s0 = 0; s0 < op.len; s0 += per) {
     const int s = s0 + t / K;
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __
 #pragma unroll
       for (int q = 0; q < 6; ++q) g[t][q] = out[q];
     }
-    __syncthreads();
+    __syncwarp();
     if (t < per && s0 + t < op.len) {
       const int s = s0 + t;
       double fine[6] = {0, 0, 0, 0, 0, 0};
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __
       const double count = double(K - 1);
       for (int q = 0; q < ncons; ++q) reg[op.reg_off + int64_t(q) * op.len + s] += fine[q] / count - g[t * K][q];
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -343,10 +348,10 @@ void launch_face_flux_kernel(const S* pool, const PatchDesc* patches, const Face
                              const double* b0, double gamma, int limiter, const FacePhysics& phys, double* reg,
                              cudaStream_t stream) {
   switch (limiter) {
-    case 0: face_flux_ops_kernel<S, R, 0, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    case 1: face_flux_ops_kernel<S, R, 1, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    case 2: face_flux_ops_kernel<S, R, 2, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
-    default: face_flux_ops_kernel<S, R, 3, PHYS><<<nops, kFluxThreads, 0, stream>>>(pool, patches, ops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 0: face_flux_ops_kernel<S, R, 0, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 1: face_flux_ops_kernel<S, R, 1, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 2: face_flux_ops_kernel<S, R, 2, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    default: face_flux_ops_kernel<S, R, 3, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
   }
 }
 

@@ -610,3 +610,52 @@ class LocalCluster:
         if refined:
             self.restrict("state", groups)
         self.fill("state")
+
+
+# ---- the solvers on a partitioned hierarchy ------------------------------------------------
+def solver_group(hierarchy):
+    """The process group of a hierarchy (``AMRHierarchy(..., comm=group)``, as the reference
+    passes its MPI communicator) when it spans more than one rank, else None."""
+    comm = getattr(hierarchy, "comm", None)
+    if comm is None:
+        return None
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size(comm) <= 1:
+        return None
+    return comm
+
+
+def solver_engine(hierarchy, group, *, walls=None, lx=32, **options):
+    """A `DistributedEngine` on this rank's share of the hierarchy: the patches of every
+    level in Morton order, cut into runs of nearly equal cells per rank (`partition`)."""
+    import torch.distributed as dist
+
+    from wellbalanced_b200.mesh import Layout
+
+    layout = Layout(hierarchy, walls=walls, precision=_lib.precision_code(options.get("precision", 32)), lx=lx)
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    owner = partition(hierarchy, world)
+    return DistributedEngine(RankLayout(layout, owner, rank), TorchTransport(group), **options)
+
+
+def local_patches(model):
+    """The hierarchy's patches this rank holds (all of them without a partition)."""
+    layout = model.engine.layout
+    if hasattr(layout, "owns"):
+        return [p for p in model.hierarchy.patches if layout.owns(p)]
+    return list(model.hierarchy.patches)
+
+
+def all_reduce(model, values, op):
+    """values (a list of floats) reduced over the model's ranks (op "sum" or "max")."""
+    group = getattr(model, "_group", None)
+    if group is None:
+        return values
+    import torch.distributed as dist
+
+    t = torch.tensor(values, dtype=torch.float64)
+    if dist.get_backend(group) == "nccl":
+        t = t.to(model.engine.device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM if op == "sum" else dist.ReduceOp.MAX, group=group)
+    return [float(v) for v in t.cpu()]

@@ -118,21 +118,32 @@ class MHD2D:
         self.period = float("nan")
         self._ready = False
 
+    def _local(self):
+        """The patches this rank holds (every patch without a partition)."""
+        from wellbalanced_b200.distributed import local_patches
+
+        return local_patches(self)
+
+    def _single_rank(self, what):
+        if getattr(self, "_group", None) is not None:
+            raise NotImplementedError(f"{what} on a hierarchy partitioned over ranks")
+
     #: whether steps run the fused stage kernels (False: the per-kernel float64 path)
     _fused = True
 
     def _build_engine(self):
         self._graph = None
         walls = tuple((w, w) for w in self.walls)
-        self.engine = Engine(
-            self.hierarchy,
-            precision=self.precision,
-            walls=walls,
-            limiter=LIMITER_CODES.index(self.limiter),
-            gamma=self.gamma,
-            mean_field=self.mean_field,
-            device=self.device,
-        )
+        options = dict(precision=self.precision, limiter=LIMITER_CODES.index(self.limiter), gamma=self.gamma,
+                       mean_field=self.mean_field, device=self.device)
+        from wellbalanced_b200.distributed import solver_engine, solver_group
+
+        # a hierarchy over several ranks (AMRHierarchy(..., comm=group)): this rank's patches
+        self._group = solver_group(self.hierarchy)
+        if self._group is not None:
+            self.engine = solver_engine(self.hierarchy, self._group, walls=walls, **options)
+        else:
+            self.engine = Engine(self.hierarchy, walls=walls, **options)
         groups = self.engine.layout.groups
         self._groups_all = groups
         self._groups_potential = groups[1:]
@@ -284,7 +295,7 @@ class MHD2D:
     def set_state(self, density, velocity, pressure, *, vector_potential: Value = 0.0, bz: Value = 0.0) -> None:
         """Set the state on every patch (``carafe/mhd.py:683-737``)."""
         gamma = self.gamma
-        for patch in self.hierarchy.patches:
+        for patch in self._local():
             x, y = self._coordinates(patch, False)
             xn, yn = self._coordinates(patch, True)
             rho = self._evaluate(density, x, y)
@@ -320,7 +331,7 @@ class MHD2D:
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
-        if self._auto_tile and self._fused and eng.physics is None:
+        if self._auto_tile and self._fused and eng.physics is None and getattr(self, "_group", None) is None:
             from wellbalanced_b200.autotune import tune_tile2d
 
             self.tile, timings = tune_tile2d(eng)
@@ -398,6 +409,7 @@ class MHD2D:
     def capture(self) -> None:
         """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
         graph that `advance` replays. The recording takes one step. A regrid drops it."""
+        self._single_rank("capture")
         self._check_ready()
         self._prime()
         self._graph = self.engine.capture(self._one_step)
@@ -426,6 +438,7 @@ class MHD2D:
         """Tag cells where ``|J_z|`` (the mean over the cell's four nodes) times the cell
         size exceeds ``threshold`` (``carafe/mhd.py:1011-1041``): one kernel over every
         cell of the tagged levels (``wb_current_tags``)."""
+        self._single_rank("current_tags")
         from wellbalanced_b200.regrid import device_tags
 
         return device_tags(self, threshold, levels)
@@ -434,6 +447,7 @@ class MHD2D:
         """Regrid on ``tags`` (``carafe/mhd.py:1043-1056``): new patches over the tagged
         cells (`AMRHierarchy.regrid` options: ``max_patch_size``, ``buffer``), the conserved
         fields moved with their integrals kept, ``A_z`` interpolated (div B stays zero)."""
+        self._single_rank("regrid")
         from wellbalanced_b200.regrid import regrid_model
 
         regrid_model(self, tags, **options)
@@ -452,17 +466,20 @@ class MHD2D:
         """The largest ``|div B|`` times the cell size (float64 from the stored ``A_z``)."""
         self._check_ready()
         largest = 0.0
-        for patch in self.hierarchy.patches:
+        for patch in self._local():
             dx, dy = self.hierarchy.spacing(patch.level)
             az = self._read(patch, 6, node=True).to(torch.float64)
             bxf = (az[:, 1:] - az[:, :-1]) / dy + self.mean_field[0]
             byf = -(az[1:, :] - az[:-1, :]) / dx + self.mean_field[1]
             div = (bxf[1:] - bxf[:-1]) / dx + (byf[:, 1:] - byf[:, :-1]) / dy
             largest = max(largest, float(torch.max(torch.abs(div))) * min(dx, dy))
-        return largest
+        from wellbalanced_b200.distributed import all_reduce
+
+        return all_reduce(self, [largest], "max")[0]
 
     def composite_divergence(self) -> float:
         """The largest mismatch of shared coarse/fine ``A_z`` nodes relative to the largest face flux."""
+        self._single_rank("composite_divergence")
         self._check_ready()
         h = self.hierarchy
         worst, scale = 0.0, 0.0
@@ -491,13 +508,15 @@ class MHD2D:
         """Integrals of the conserved fields over the domain from the leaf cells (float64)."""
         self._check_ready()
         out = dict.fromkeys(CONSERVED, 0.0)
-        for patch in self.hierarchy.patches:
+        for patch in self._local():
             volume = float(np.prod(self.hierarchy.spacing(patch.level)))
             leaf = torch.from_numpy(~self._covered(patch)).to(self.engine.device)
             for f, name in enumerate(CONSERVED):
                 values = self._read(patch, f).to(torch.float64)
                 out[name] += float(torch.sum(values[leaf])) * volume
-        return out
+        from wellbalanced_b200.distributed import all_reduce
+
+        return dict(zip(out, all_reduce(self, list(out.values()), "sum"), strict=True))
 
     def gather(self, patch, field: int, node=False) -> np.ndarray:
         return self._read(patch, field, node=node).to(torch.float64).cpu().numpy()

@@ -87,20 +87,31 @@ class MHD3D:
         self.period = float("nan")
         self._ready = False
 
+    def _local(self):
+        """The patches this rank holds (every patch without a partition)."""
+        from wellbalanced_b200.distributed import local_patches
+
+        return local_patches(self)
+
+    def _single_rank(self, what):
+        if getattr(self, "_group", None) is not None:
+            raise NotImplementedError(f"{what} on a hierarchy partitioned over ranks")
+
     #: whether steps run the fused stage kernel (False: the per-kernel float64 path)
     _fused = True
 
     def _build_engine(self):
         self._graph = None
-        self.engine = Engine(
-            self.hierarchy,
-            precision=self.precision,
-            limiter=LIMITER_CODES.index(self.limiter),
-            gamma=self.gamma,
-            mean_field=self.mean_field,
-            device=self.device,
-            lx=self.lx,
-        )
+        options = dict(precision=self.precision, limiter=LIMITER_CODES.index(self.limiter), gamma=self.gamma,
+                       mean_field=self.mean_field, device=self.device)
+        from wellbalanced_b200.distributed import solver_engine, solver_group
+
+        # a hierarchy over several ranks (AMRHierarchy(..., comm=group)): this rank's patches
+        self._group = solver_group(self.hierarchy)
+        if self._group is not None:
+            self.engine = solver_engine(self.hierarchy, self._group, lx=self.lx, **options)
+        else:
+            self.engine = Engine(self.hierarchy, lx=self.lx, **options)
         groups = self.engine.layout.groups
         self._groups_all = groups
         self._groups_potential = groups[1:]
@@ -234,7 +245,7 @@ class MHD3D:
         """Set the state on every patch (``carafe/mhd3d.py:388-441``)."""
         gamma = self.gamma
         h = self.hierarchy
-        for patch in h.patches:
+        for patch in self._local():
             x, y, z = self._coordinates(patch, (0, 0, 0))
             rho = self._evaluate(density, x, y, z)
             if callable(velocity):
@@ -353,6 +364,7 @@ class MHD3D:
     def capture(self) -> None:
         """Record one step (rate, dt, both stages, halos, reflux, restriction) in a CUDA
         graph that `advance` replays. The recording takes one step. A regrid drops it."""
+        self._single_rank("capture")
         self._check_ready()
         self._prime()
         self._graph = self.engine.capture(self._one_step)
@@ -400,6 +412,7 @@ class MHD3D:
         """Tag cells where ``|J|`` (central differences of the cell field) times the cell
         size exceeds ``threshold`` (``carafe/mhd3d.py:771-801``): one kernel over every
         cell of the tagged levels (``wb_current_tags``)."""
+        self._single_rank("current_tags")
         from wellbalanced_b200.regrid import device_tags
 
         return device_tags(self, threshold, levels)
@@ -407,6 +420,7 @@ class MHD3D:
     def regrid(self, tags: dict[int, np.ndarray], **options: Any) -> None:
         """Regrid on ``tags`` (``carafe/mhd3d.py:803-816``); the potential is interpolated and
         restricted, so the field stays divergence-free."""
+        self._single_rank("regrid")
         from wellbalanced_b200.regrid import regrid_model
 
         regrid_model(self, tags, **options)
@@ -428,7 +442,7 @@ class MHD3D:
     def divergence(self) -> float:
         self._check_ready()
         largest = 0.0
-        for patch in self.hierarchy.patches:
+        for patch in self._local():
             spacing = self.hierarchy.spacing(patch.level)
             pot = self._potentials(patch)
             div = 0.0
@@ -437,7 +451,9 @@ class MHD3D:
                 face = torch.diff(pot[c], dim=b) / spacing[b] - torch.diff(pot[b], dim=c) / spacing[c] + self.mean_field[a]
                 div = div + torch.diff(face, dim=a) / spacing[a]
             largest = max(largest, float(torch.max(torch.abs(div))) * min(spacing))
-        return largest
+        from wellbalanced_b200.distributed import all_reduce
+
+        return all_reduce(self, [largest], "max")[0]
 
     def _covered(self, patch):
         mask = np.zeros(patch.shape, dtype=bool)
@@ -457,12 +473,14 @@ class MHD3D:
         """Integrals of the conserved fields from the leaf cells (float64)."""
         self._check_ready()
         out = dict.fromkeys(CONSERVED_3D, 0.0)
-        for patch in self.hierarchy.patches:
+        for patch in self._local():
             volume = float(np.prod(self.hierarchy.spacing(patch.level)))
             leaf = torch.from_numpy(~self._covered(patch)).to(self.engine.device)
             for f, name in enumerate(CONSERVED_3D):
                 out[name] += float(torch.sum(self._read(patch, f).to(torch.float64)[leaf])) * volume
-        return out
+        from wellbalanced_b200.distributed import all_reduce
+
+        return dict(zip(out, all_reduce(self, list(out.values()), "sum"), strict=True))
 
     def gather(self, patch, field):
         extra = (0, 0, 0) if field < 5 else _EXTRA[field - 5]
