@@ -25,6 +25,9 @@ import itertools
 
 import numpy as np
 
+from wellbalanced_b200 import _lib
+from wellbalanced_b200.mesh import HALO
+
 
 def _grow(mask, buffer, periodic):
     out = mask.copy()
