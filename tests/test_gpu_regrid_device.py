@@ -110,9 +110,21 @@ def _models_2d(precision, periodic):
 
 
 def _models_3d(precision):
+    """Turbulence at rms Mach 0.3 and rms |B| 0.3 (beta about 20): with the unit-amplitude
+    field, the prolonged cells of this 12^3 grid (kmax 8: two cells per wavelength) carry
+    more magnetic energy than their share of the total and go negative in pressure."""
+    from wellbalanced_b200.mesh import AMRHierarchy
     from wellbalanced_b200.mhd3d import MHD3D
+    from wellbalanced_b200.problems import turbulence_3d
 
-    return [MHD3D.turbulence(12, seed=5, precision=precision) for _ in range(2)]
+    out = []
+    for _ in range(2):
+        model = MHD3D(AMRHierarchy((12,) * 3, ((0.0, 1.0),) * 3, periodic=(True,) * 3), limiter="mc", cfl=0.3,
+                      precision=precision)
+        rho, velocity, p, potential = turbulence_3d(12, seed=5, mach=0.3, b_rms=0.3, gamma=model.gamma)
+        model.set_state(rho, velocity, p, vector_potential=potential)
+        out.append(model)
+    return out
 
 
 CASES = [("2d float64 periodic", lambda: _models_2d(64, (True, True))),
@@ -126,7 +138,7 @@ def test_device_transfer_equals_the_host_restatement(name, build):
     from wellbalanced_b200.regrid import regrid_model_device, regrid_model_host
 
     device, host = build()
-    threshold = 0.05 if device.hierarchy.ndim == 2 else 1.0
+    threshold = 0.05 if device.hierarchy.ndim == 2 else 0.3
     for regrid in range(2):
         tags = device.current_tags(threshold, levels=2)
         before = device.totals()

@@ -276,7 +276,7 @@ def amr_run(model, tags_of, *, interval, steps, threshold, buffer=1, max_patch_s
 
 
 def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, threshold=0.05, seed=0,
-                   iterations=600, miss=0.005, buffer=1, max_patch_size=8):
+                   iterations=600, miss=0.005, buffer=1, max_patch_size=8, every=2):
     """The regrid interval each tagger reaches on the multi-blast run with one refined level.
 
     For every interval K: a tagger trained on the first ``train_steps`` steps of a uniform
@@ -289,7 +289,7 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
     for K in intervals:
         tagger = LearnedTagger(seed=seed)
         model = multiblast(n, seed=seed)
-        X_raw, Y, _ = collect(model, tagger, steps=train_steps, horizon=K, threshold=threshold, every=2)
+        X_raw, Y, _ = collect(model, tagger, steps=train_steps, horizon=K, threshold=threshold, every=every)
         tagger.fit_normalisation(X_raw)
         X = tagger.normalise(X_raw)
         tagger.fit(X, Y, iterations=iterations, seed=seed)
