@@ -12,10 +12,10 @@ Workloads (``--workload``; one zone-update = one cell advanced by one full RK2 s
   per kernel (the timed steps launch directly; the same steps replayed from a CUDA graph
   are reported beside them).
 * ``harris``: a 2D Harris current sheet on [-1, 1] x [-2, 2], base 128 x 256, periodic in
-  x and outflow in y, refined three times on the current (|J| dx > 1e-4, boxes of at most
-  16 cells a side: ~1800 uneven patches), float32 with float64 refluxing; every level
-  advances at the finest CFL 0.4 step, all patches in one launch per kernel, the small
-  ops between the stages in two op programs per step.
+  x and outflow in y, refined three times on the current (|J| dx > 1e-7, boxes of 16-24
+  fine cells a side where the tags allow: ~1600 uneven patches, 5.6e5 cells), float32 with
+  float64 refluxing; every level advances at the finest CFL 0.4 step, all patches in one
+  launch per kernel.
 
 With N GPUs (torchrun) every rank advances its own copy of the workload (replicas,
 seeded by rank: weak scaling, no data-path collective); `value` is the zone-updates of
@@ -74,11 +74,13 @@ def parse():
 HARRIS_BASE = (128, 256)
 HARRIS_BOUNDS = ((-1.0, 1.0), (-2.0, 2.0))
 HARRIS_LEVELS = 3
-#: the refinement rule of the Harris workload: |J| dx above 1e-4 (the current sheet and its
-#: seeded perturbation out to |y| ~ 0.3), clustered into boxes of at most 8 coarse cells a
-#: side (refined patches of 4-16 cells): ~1800 uneven patches over three levels
-HARRIS_THRESHOLD = 1e-4
-HARRIS_PATCH = 8  # coarse cells a side, so refined patches of at most 16 cells
+#: the refinement rule of the Harris workload: |J| dx above 1e-7 (the current sheet and its
+#: seeded perturbation out to |y| ~ 0.4), clustered into boxes of 8 to 12 coarse cells a
+#: side (refined patches of 12-24 cells, most 16-24): ~1600 uneven patches and 5.6e5 cells
+#: over three levels
+HARRIS_THRESHOLD = 1e-7
+HARRIS_PATCH = 12  # coarse cells a side at most, so refined patches of at most 24 cells
+HARRIS_MIN_PATCH = 8  # coarse cells a side at least, where the tagged region allows
 
 
 def _harris_model(cls, precision, seed, *, levels=HARRIS_LEVELS, base=HARRIS_BASE, **options):
@@ -91,7 +93,8 @@ def _harris_model(cls, precision, seed, *, levels=HARRIS_LEVELS, base=HARRIS_BAS
     model = cls(mesh, limiter="mc", cfl=0.4, precision=precision, **options)
     model.set_state(density, (0.0, 0.0, 0.0), pressure, vector_potential=potential)
     for _ in range(levels):
-        model.regrid(model.current_tags(HARRIS_THRESHOLD, levels=levels), max_patch_size=HARRIS_PATCH)
+        model.regrid(model.current_tags(HARRIS_THRESHOLD, levels=levels), max_patch_size=HARRIS_PATCH,
+                     min_patch_size=HARRIS_MIN_PATCH)
     return model
 
 
@@ -478,11 +481,32 @@ class Harris:
         self.model._graph = None
         return 1e3 * seconds / steps
 
+    def schedule_timing(self, steps):
+        """ms and launches per step of the two schedules of the refined step: the small ops
+        between the stages as separate launches (fill, restrict, register, rate), and as two
+        op programs (device work lists drained by one launch each)."""
+        eng = self.engine
+        default = eng.use_programs
+        out = {}
+        for name, programs in (("separate_launches", False), ("op_programs", True)):
+            eng.use_programs = programs
+            eng.dt_ready = False
+            self.model.advance(2, check=False)
+            first = eng.launches
+            seconds = _time_steps(lambda: self.model.advance(1, check=False), steps)
+            out[name] = {"ms_per_step": 1e3 * seconds / steps,
+                         "launches_per_step": (eng.launches - first) / (steps + 1),
+                         "value": self.cells * steps / seconds}
+        eng.use_programs = default
+        eng.dt_ready = False
+        out["default"] = "op_programs" if default else "separate_launches"
+        return out
+
     @staticmethod
     def describe(args):
         return (f"2D Harris sheet on [-1,1]x[-2,2], base {HARRIS_BASE[0]}x{HARRIS_BASE[1]}, periodic x, "
-                f"outflow y, {HARRIS_LEVELS} refined levels on |J| dx > {HARRIS_THRESHOLD} (patches <= "
-                f"{2 * HARRIS_PATCH} cells a side), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.4 at the finest dx, "
+                f"outflow y, {HARRIS_LEVELS} refined levels on |J| dx > {HARRIS_THRESHOLD} (patches of "
+                f"{2 * HARRIS_MIN_PATCH}-{2 * HARRIS_PATCH} cells a side where the tags allow), MC-PLM + HLLD + CT, SSP-RK2, CFL 0.4 at the finest dx, "
                 "float32 state with float64 refluxing, all patches in one launch per kernel")
 
     def config(self):
@@ -910,6 +934,8 @@ def extra_workload(name, args, rank, world, local, barrier):
     if run["graph_ms"] is not None:
         entry["graph"] = {"ms_per_step": run["graph_ms"], "value": world * work.cells / (run["graph_ms"] / 1e3),
                           "what": "the same steps replayed from one captured CUDA graph"}
+    if hasattr(work, "schedule_timing"):
+        entry["schedules"] = work.schedule_timing(steps)
     if rank == 0 and not args.no_plain and kind != args.workload:
         entry["plain_fp64"] = work.plain()
         entry["plain_fp64"]["speedup_of_value"] = run["value"] / world / entry["plain_fp64"]["value"]

@@ -293,10 +293,20 @@ int wb_current_tags(int precision, int ndim, const void* pool, const void* patch
  *   start, fine_lo[3], coarse_lo[3] level indices, coarse_n[3] level shape, periodic mask):
  *   cells minmod-limited (children c -/+ s/4 per axis), potentials linear along node axes;
  * - wb_kept_ops: the points an old patch of the same level held, from the old pool (struct
- *   CopyOp: dst a new patch, src1 an old patch in old_patches, unit weights and strides). */
+ *   CopyOp: dst a new patch, src1 an old patch in old_patches, unit weights and strides);
+ * - wb_positivity_ops: after both, every prolonged parent (struct PositivityOp of
+ *   csrc/transfer.cu: fine, coarse, ndim, pad, n[3] parents, f0[3] haloed first child,
+ *   c0[3] haloed first parent) whose children include a non-positive density or pressure
+ *   gives them its density, momentum (2D: B_z) and an energy that keeps the pressure
+ *   positive: E + M_i - mean(M) while that pressure is positive (the integral kept), else
+ *   p / (gamma - 1) + K + M_i (M_i a child's magnetic energy from the fine potential). No
+ *   counterpart in the reference, whose transfer leaves such children to fail the next
+ *   step's check; elsewhere the transfer is unchanged. */
 int wb_prolong_ops(int precision, void* pool, const void* patches, const void* ops, int nops, void* stream);
 int wb_kept_ops(int precision, void* pool, const void* patches, const void* old_pool, const void* old_patches,
                 const void* ops, int nops, void* stream);
+int wb_positivity_ops(int precision, void* pool, const void* patches, const void* ops, int nops, double b0x,
+                      double b0y, double b0z, double gamma, void* stream);
 
 /* Sizes of the engine structs, for callers that mirror them: PatchDesc, Tile, CopyOp,
  * InterpOp, RestrictOp, FaceFluxOp, RefluxOp, and with n >= 9 wb_program_segment and

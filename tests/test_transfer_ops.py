@@ -1,7 +1,9 @@
 """The device regrid transfer's op lists (CPU): every point of every new patch is written
 by the prolongation from the level below (levels >= 1), kept-value ops cover exactly the
-points an old patch of the same level held, and every index an op makes its kernel read or
-write lies inside the haloed arrays of its patches (the bounds of csrc/transfer.cu)."""
+points an old patch of the same level held, positivity ops visit every new cell of a level
+>= 1 once (as a child of a parent cell of the level below), and every index an op makes its
+kernel read or write lies inside the haloed arrays of its patches (the bounds of
+csrc/transfer.cu)."""
 
 from __future__ import annotations
 
@@ -40,7 +42,7 @@ def test_transfer_ops_cover_and_stay_in_bounds(ndim, periodic):
     groups = field_groups(ndim)
     ops = transfer_ops(old, new, groups, ndim)
     assert len(ops) == new.max_level + 1
-    for level, (prolong, kept) in enumerate(ops):
+    for level, (prolong, kept, positivity) in enumerate(ops):
         for g in groups:
             for f in new.patches_at_level(level):
                 n = [f.shape[a] + ((g.node_mask >> a) & 1) for a in range(ndim)]
@@ -69,3 +71,22 @@ def test_transfer_ops_cover_and_stay_in_bounds(ndim, periodic):
                     for a in range(ndim):
                         assert 0 <= op["d"][a] and op["d"][a] + op["n"][a] <= _haloed(f, ndim)[a]
                         assert 0 <= op["s1"][a] and op["s1"][a] + op["n"][a] <= _haloed(o, ndim)[a]
+        if level:
+            for f in new.patches_at_level(level):
+                seen = np.zeros(f.shape, dtype=np.int64)
+                for op in positivity[positivity["fine"] == f.index]:
+                    c = new.patches[int(op["coarse"])]
+                    assert c.level == level - 1 and int(op["ndim"]) == ndim
+                    for q in itertools.product(*[range(int(op["n"][a])) for a in range(ndim)]):
+                        parent = [int(op["c0"][a]) + q[a] for a in range(ndim)]
+                        # the parent's cell and its nodes (cell + 1) inside the coarse array
+                        assert all(HALO <= parent[a] < HALO + c.shape[a] for a in range(ndim))
+                        # its level index matches its children's
+                        for o in itertools.product((0, 1), repeat=ndim):
+                            x = [int(op["f0"][a]) + 2 * q[a] + o[a] for a in range(ndim)]
+                            assert all(HALO <= x[a] < HALO + f.shape[a] for a in range(ndim))
+                            level_x = [x[a] - HALO + f.box[a][0] for a in range(ndim)]
+                            level_parent = [parent[a] - HALO + c.box[a][0] for a in range(ndim)]
+                            assert [v // 2 for v in level_x] == level_parent
+                            seen[tuple(x[a] - HALO for a in range(ndim))] += 1
+                assert (seen == 1).all(), (level, f.box)

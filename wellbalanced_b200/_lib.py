@@ -73,6 +73,7 @@ SIGNATURES = {
                         c_double, c_dp, c_dp],
     "wb_prolong_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_kept_ops": [c_int, c_dp, c_dp, c_dp, c_dp, c_dp, c_int, c_dp],
+    "wb_positivity_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_dp],
 }
 
 #: Every symbol include/wellbalanced_b200.h declares.

@@ -207,44 +207,14 @@ __device__ __forceinline__ void hlld_front(const R (&L)[7], const R (&Rt)[7], R 
 // fast speed, small tangential field); above 1e-3 the float32 value is good to ~0.1%.
 constexpr float kNearDegenerate32 = 1.0e-3f;
 
-// The float64 evaluation of a float32 face's front half (taken rarely: only where the
-// float32 star denominator is near zero).
-__device__ __forceinline__ void hlld_front_wide(const float (&L)[7], const float (&Rt)[7], float bn, float gamma,
-                                             HlldFront<float>& o) {
-  double Ld[7], Rd[7];
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    Ld[c] = L[c];
-    Rd[c] = Rt[c];
-  }
-  HlldFront<double> d;
-  hlld_front<double, MathRefined>(Ld, Rd, double(bn), double(gamma), d);
-  o.sl = float(d.sl), o.sr = float(d.sr), o.ptl = float(d.ptl), o.ptr = float(d.ptr);
-  o.dl = float(d.dl), o.dr = float(d.dr), o.sm = float(d.sm), o.pts = float(d.pts);
-  o.rsl = float(d.rsl), o.vtl1 = float(d.vtl1), o.vtl2 = float(d.vtl2);
-  o.btl1 = float(d.btl1), o.btl2 = float(d.btl2), o.den_l = float(d.den_l);
-  o.rsr = float(d.rsr), o.vtr1 = float(d.vtr1), o.vtr2 = float(d.vtr2);
-  o.btr1 = float(d.btr1), o.btr2 = float(d.btr2), o.den_r = float(d.den_r);
-}
-
 template <typename R>
 __device__ __forceinline__ void hlld_front_checked(const R (&L)[7], const R (&Rt)[7], R bn, R gamma,
                                                    HlldFront<R>& o) {
   hlld_front<R, Math<R>>(L, Rt, bn, gamma, o);
 }
 
-template <>
-__device__ __forceinline__ void hlld_front_checked<float>(const float (&L)[7], const float (&Rt)[7], float bn,
-                                                          float gamma, HlldFront<float>& o) {
-  hlld_front<float, Math<float>>(L, Rt, bn, gamma, o);
-  const float bn2 = bn * bn;
-  const bool near = rabs(o.den_l) < kNearDegenerate32 * (o.ptl + bn2) ||
-                    rabs(o.den_r) < kNearDegenerate32 * (o.ptr + bn2);
-  if (near) hlld_front_wide(L, Rt, bn, gamma, o);
-}
-
-// HLLD flux through a face between normal-frame states L and Rt with normal field bn.
-// Straight-line code: the star / double-star flux of the side of the contact the face
+// HLLD flux through a face between normal-frame states L and Rt with normal field bn
+// (float64; the float32 faces take hlld_flux_l of numerics_lanes.cuh). Straight-line code: the star / double-star flux of the side of the contact the face
 // lies on is always formed and the supersonic and star-only cases are selected at the
 // end (no divergent branches). Where a face is supersonic (S_L >= 0 or S_R < 0) the
 // contact lies on the same side as the upwind state, so one side state serves both.
@@ -442,3 +412,5 @@ __device__ __forceinline__ float recover_pressure<float>(float r, float m0, floa
 }
 
 }  // namespace wb
+
+#include "numerics_lanes.cuh"

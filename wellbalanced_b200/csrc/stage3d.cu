@@ -107,6 +107,60 @@ __device__ __forceinline__ int face_slot(int plane) {
   return PHYS ? (plane + 6) % 3 : (plane + 4) & 1;  // plane >= -3
 }
 
+// The y- and z-face of a B1 thread from the primitive plane P (rows of NR values): the
+// y-stencil starts at ry with stride sy, the z-stencil at rz with stride 1; fluxes to
+// outy[c G], outz[c G]. Float32 arithmetic evaluates the two faces together on the packed
+// float32 lanes (F2); float64 one after the other.
+constexpr bool kPairFaces = false;
+
+template <int LIM, typename R>
+__device__ __forceinline__ void yz_faces(const R* P, int NR, int ry, int sy, int rz, R bny, R bnz, R gamma,
+                                         R inv_gm1, R* outy, R* outz, int G) {
+  constexpr int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
+  constexpr int zrow[7] = {0, 3, 1, 2, 4, 5, 6};
+  if constexpr (kPairFaces && std::is_same<R, float>::value) {
+    F2 a0[7], a1[7], a2[7], a3[7];
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+      const R* y = P + yrow[c] * NR + ry;
+      const R* z = P + zrow[c] * NR + rz;
+      a0[c] = F2(y[0], z[0]);
+      a1[c] = F2(y[sy], z[1]);
+      a2[c] = F2(y[2 * sy], z[2]);
+      a3[c] = F2(y[3 * sy], z[3]);
+    }
+    F2 L[7], Rt[7], F[7];
+    reconstruct_l<LIM>(a0, a1, a2, a3, L, Rt);
+    hlld_flux_l<F2>(L, Rt, F2(bny, bnz), F2(gamma), F2(inv_gm1), F);
+#pragma unroll
+    for (int c = 0; c < 7; ++c) {
+      outy[c * G] = F[c].v.x;
+      outz[c * G] = F[c].v.y;
+    }
+  } else {
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const int* rows = side == 0 ? yrow : zrow;
+      const int r0 = side == 0 ? ry : rz, st = side == 0 ? sy : 1;
+      R a0[7], a1[7], a2[7], a3[7];
+#pragma unroll
+      for (int c = 0; c < 7; ++c) {
+        const R* row = P + rows[c] * NR + r0;
+        a0[c] = row[0];
+        a1[c] = row[st];
+        a2[c] = row[2 * st];
+        a3[c] = row[3 * st];
+      }
+      R L[7], Rt[7], F[7];
+      reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
+      hlld_flux(L, Rt, side == 0 ? bny : bnz, gamma, inv_gm1, F);
+      R* out = side == 0 ? outy : outz;
+#pragma unroll
+      for (int c = 0; c < 7; ++c) out[c * G] = F[c];
+    }
+  }
+}
+
 // S: the state's type (loads, the conserved and potential updates, the Heun combine);
 // R: the arithmetic of the reconstruction, HLLD and CT. With a float64 state and float32
 // arithmetic (S = double, R = float) phase A forms the primitive variables and face fields
@@ -176,12 +230,12 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY,
   const int y_g = yj * GZ + (yk + 1);
   const int z_g = (zj + 1) * GZ + zk;
 
-  R q[3][7];    // x-stencil of the column: planes p-1 .. p+1 (x-frame rows)
-  R slope[7];   // limited x-slope of plane p-1 (computed one plane earlier)
+  // the x-stencil of the column: plane p-1 in registers (x-frame rows; planes p and p+1
+  // are read from the primitive slots), and the limited x-slope of plane p-1
+  R qm[7];
+  R slope[7];
 #pragma unroll
-  for (int s = 0; s < 3; ++s)
-#pragma unroll
-    for (int c = 0; c < 7; ++c) q[s][c] = R(1);
+  for (int c = 0; c < 7; ++c) qm[c] = R(1);
 #pragma unroll
   for (int c = 0; c < 7; ++c) slope[c] = R(0);
   R fprev[5] = {R(0), R(0), R(0), R(0), R(0)};
@@ -301,69 +355,37 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY,
       if (need_yz) {
         R* Y7 = sYZ + (slot3 * 2 + 0) * 7 * G;
         R* Z7 = sYZ + (slot3 * 2 + 1) * 7 * G;
-        {
-          // y-face between cells (yj-1, yk) and (yj, yk): frame (y, z, x)
-          const int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
-          const int r0 = (yj - 2 + 2) * RZ + (yk + 2);
-          R a0[7], a1[7], a2[7], a3[7];
-#pragma unroll
-          for (int cc = 0; cc < 7; ++cc) {
-            const R* row = Pp + yrow[cc] * NR + r0;
-            a0[cc] = row[0];
-            a1[cc] = row[RZ];
-            a2[cc] = row[2 * RZ];
-            a3[cc] = row[3 * RZ];
-          }
-          R L[7], Rt[7], F[7];
-          reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
-          hlld_flux(L, Rt, Bp[NR + (yj + 2) * RZ + (yk + 2)], gamma, inv_gm1, F);
-#pragma unroll
-          for (int cc = 0; cc < 7; ++cc) Y7[cc * G + y_g] = F[cc];
-        }
-        {
-          // z-face between cells (zj, zk-1) and (zj, zk): frame (z, x, y)
-          const int zrow[7] = {0, 3, 1, 2, 4, 5, 6};
-          const int r0 = (zj + 2) * RZ + (zk - 2 + 2);
-          R a0[7], a1[7], a2[7], a3[7];
-#pragma unroll
-          for (int cc = 0; cc < 7; ++cc) {
-            const R* row = Pp + zrow[cc] * NR + r0;
-            a0[cc] = row[0];
-            a1[cc] = row[1];
-            a2[cc] = row[2];
-            a3[cc] = row[3];
-          }
-          R L[7], Rt[7], F[7];
-          reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
-          hlld_flux(L, Rt, Bp[2 * NR + (zj + 2) * RZ + (zk + 2)], gamma, inv_gm1, F);
-#pragma unroll
-          for (int cc = 0; cc < 7; ++cc) Z7[cc * G + z_g] = F[cc];
-        }
+        // the y-face between cells (yj-1, yk) and (yj, yk), frame (y, z, x), and the z-face
+        // between cells (zj, zk-1) and (zj, zk), frame (z, x, y)
+        yz_faces<LIM>(Pp, NR, (yj - 2 + 2) * RZ + (yk + 2), RZ, (zj + 2) * RZ + (zk - 2 + 2),
+                      Bp[NR + (yj + 2) * RZ + (yk + 2)], Bp[2 * NR + (zj + 2) * RZ + (zk + 2)], gamma, inv_gm1,
+                      Y7 + y_g, Z7 + z_g, G);
       }
     }
     __syncthreads();
 
     // B2: x-face of plane p (needs plane p + 1 for its stencil) --------------------------
     {
-      const int c = p + 1;
-      const R* Pn = sP + ((c + 4) & 1) * 8 * NR;
+      const R* Pc = sP + ((p + 4) & 1) * 8 * NR;      // plane p
+      const R* Pn = sP + ((p + 1 + 4) & 1) * 8 * NR;  // plane p + 1
+      constexpr int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
+      // plane x0 - 3 (the first p) was never loaded: its column reads as 1 like qm, and the
+      // slopes formed before plane x0 - 1 are never used
+      const bool loaded = p >= x0 - 2;
+      R q1[7], q2[7];
 #pragma unroll
-      for (int s = 0; s < 2; ++s)
-#pragma unroll
-        for (int cc = 0; cc < 7; ++cc) q[s][cc] = q[s + 1][cc];
-      {
-        const int xrow[7] = {0, 1, 2, 3, 4, 6, 7};
-#pragma unroll
-        for (int cc = 0; cc < 7; ++cc) q[2][cc] = Pn[xrow[cc] * NR + col_r];
+      for (int cc = 0; cc < 7; ++cc) {
+        q1[cc] = loaded ? Pc[xrow[cc] * NR + col_r] : R(1);
+        q2[cc] = Pn[xrow[cc] * NR + col_r];
       }
       // the slope of plane p, kept for face p + 1: each cell's x-slope is formed once
       R now[7];
 #pragma unroll
-      for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q[1][cc] - q[0][cc], q[2][cc] - q[1][cc]);
+      for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q1[cc] - qm[cc], q2[cc] - q1[cc]);
       const R* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : ((p + 4) & 1)) * 3 * NR;
       if (p >= x0) {
         R L[7], Rt[7], F[7];
-        reconstruct_sloped(q[0], q[1], slope, now, L, Rt);
+        reconstruct_sloped(qm, q1, slope, now, L, Rt);
         hlld_flux(L, Rt, Bp[col_r], gamma, inv_gm1, F);
         if (PHYS && a.eta != 0.0 && tid < NCORE) {
           // eta (J_y B_z - J_z B_y) on the x-face: J of its two y- and two z-edges, B of
@@ -385,7 +407,10 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY,
         for (int cc = 0; cc < 5; ++cc) fnow[cc] = F[cc];
       }
 #pragma unroll
-      for (int cc = 0; cc < 7; ++cc) slope[cc] = now[cc];
+      for (int cc = 0; cc < 7; ++cc) {
+        slope[cc] = now[cc];
+        qm[cc] = q1[cc];
+      }
       if (PHYS && a.eta != 0.0 && p >= x0) {
         const R eta = R(a.eta);
         if (p < xe) {

@@ -433,6 +433,25 @@ class MHD2D:
             self.time = float(eng.time[0].item())
             self._raise_if_bad()
 
+    def save(self, host=None):
+        """Copy the device state pool into ``host`` (a pinned CPU tensor, allocated if None);
+        returns it once the copy has landed."""
+        pool = self.engine.state
+        if host is None:
+            host = torch.empty(pool.shape, dtype=pool.dtype, pin_memory=True)
+        host.copy_(pool, non_blocking=True)
+        torch.cuda.current_stream(pool.device).synchronize()
+        return host
+
+    def load(self, host) -> None:
+        """Replace the device state pool by ``host`` (from `save`, same hierarchy and precision)."""
+        self.engine.dt_ready = False
+        pool = self.engine.state
+        if tuple(host.shape) != tuple(pool.shape) or host.dtype != pool.dtype:
+            raise ValueError("the saved state belongs to another layout or precision")
+        pool.copy_(host, non_blocking=True)
+        self._ready = True
+
     # refinement ----------------------------------------------------------------------------------
     def current_tags(self, threshold: float, levels: int) -> dict[int, np.ndarray]:
         """Tag cells where ``|J_z|`` (the mean over the cell's four nodes) times the cell

@@ -248,11 +248,93 @@ def _merge_periodic_planes(values, mask, extra, periodic, shape):
         mask[last] = mask[first]
 
 
+def _cell_field(arrays, ndim, spacing, mean_field):
+    """Cell-centred field of a level's dense arrays: the mean of each cell's two faces,
+    every face the curl of the potential plus the mean field (2D: B_z the cell field);
+    operation by operation as the device (csrc/transfer.cu cell_field)."""
+    if ndim == 2:
+        A = arrays[6]
+        dx, dy = spacing
+        fx = np.diff(A, axis=1) / dy + mean_field[0]
+        fy = -np.diff(A, axis=0) / dx + mean_field[1]
+        return 0.5 * (fx[:-1] + fx[1:]), 0.5 * (fy[:, :-1] + fy[:, 1:]), arrays[5]
+    ax, ay, az = arrays[5], arrays[6], arrays[7]
+    dx, dy, dz = spacing
+    fx = (np.diff(az, axis=1) / dy - np.diff(ay, axis=2) / dz) + mean_field[0]
+    fy = (np.diff(ax, axis=2) / dz - np.diff(az, axis=0) / dx) + mean_field[1]
+    fz = (np.diff(ay, axis=0) / dx - np.diff(ax, axis=1) / dy) + mean_field[2]
+    return 0.5 * (fx[:-1] + fx[1:]), 0.5 * (fy[:, :-1] + fy[:, 1:]), 0.5 * (fz[:, :, :-1] + fz[:, :, 1:])
+
+
+def _kinetic(r, m0, m1, m2):
+    return (0.5 * ((m0 * m0 + m1 * m1) + m2 * m2)) / r
+
+
+def _magnetic(b):
+    return 0.5 * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2])
+
+
+def positivity_fix(fine, coarse, ndim, spacing_fine, spacing_coarse, gamma, mean_field):
+    """The positivity pass of the transfer on a level's dense arrays (``fine``, fields as
+    the pool's; ``coarse`` the level below), in place: every parent whose children include a
+    non-positive density or pressure gives them its density, momentum (2D: B_z) and the
+    energy E + M_i - mean(M) while (gamma - 1)(E - K - mean(M)) > 0, else
+    p / (gamma - 1) + K + M_i (M_i a child's magnetic energy from the fine potential;
+    ``csrc/transfer.cu`` positivity_ops_kernel, operation by operation). Returns the count
+    of parents changed."""
+    gm1 = gamma - 1.0
+    offsets = list(itertools.product((0, 1), repeat=ndim))
+
+    def child(a, o):
+        return a[tuple(slice(x, None, 2) for x in o)]
+
+    bf = _cell_field(fine, ndim, spacing_fine, mean_field)
+    bad = np.zeros(coarse[0].shape, dtype=bool)
+    for o in offsets:
+        r = child(fine[0], o)
+        k = _kinetic(r, child(fine[1], o), child(fine[2], o), child(fine[3], o))
+        p = gm1 * ((child(fine[4], o) - k) - _magnetic([child(b, o) for b in bf]))
+        with np.errstate(invalid="ignore"):
+            bad |= ~((r > 0.0) & (p > 0.0) & np.isfinite(p))
+    if not bad.any():
+        return 0
+    bc = _cell_field(coarse, ndim, spacing_coarse, mean_field)
+    k = _kinetic(coarse[0], coarse[1], coarse[2], coarse[3])
+    pc = gm1 * ((coarse[4] - k) - _magnetic(bc))
+    fix = bad & (coarse[0] > 0.0) & (pc > 0.0)
+    mags = []
+    total = np.zeros(coarse[0].shape)
+    for o in offsets:
+        b = [child(x, o) for x in bf]
+        if ndim == 2:
+            b[2] = coarse[5]
+        mags.append(_magnetic(b))
+        total = total + mags[-1]
+    mean = total / float(len(offsets))
+    keep = gm1 * ((coarse[4] - k) - mean) > 0.0
+    floor = pc / gm1 + k
+    for o, mag in zip(offsets, mags, strict=True):
+        energy = np.where(keep, coarse[4] + (mag - mean), floor + mag)
+        for f in range(4):
+            child(fine[f], o)[fix] = coarse[f][fix]
+        child(fine[4], o)[fix] = energy[fix]
+        if ndim == 2:
+            child(fine[5], o)[fix] = coarse[5][fix]
+    return int(fix.sum())
+
+
+def _rounded(values, dtype):
+    """Values as the state holds them (float32 states round)."""
+    return values.astype(np.float32).astype(np.float64) if dtype == np.float32 else values
+
+
 def regrid_model_host(model, tags, **options):
     """Regrid ``model`` (an `MHD2D` / `MHD3D`) on ``tags`` with the transfer restated on the
     host, level by level on dense arrays (the state goes to the host and back). The
     solvers regrid with `regrid_model` (the transfer on the device); this restatement is
     what the tests check the device transfer against."""
+    import torch
+
     model._check_ready()
     old_h = model.hierarchy
     extras = model._field_extras()
@@ -276,6 +358,7 @@ def regrid_model_host(model, tags, **options):
     time, steps = model.time, model.steps
     model.hierarchy = new_h
     model._build_engine()
+    dtype = np.float32 if model.engine.state.dtype == torch.float32 else np.float64
     new_levels = {}
     for level in range(new_h.max_level + 1):
         arrays = []
@@ -286,11 +369,16 @@ def regrid_model_host(model, tags, **options):
             else:
                 coarse = new_levels[level - 1][f]
                 fine = prolong_potential(coarse, extra) if any(extra) else prolong_cells(coarse, periodic)
-                result = fine if old is None else np.where(old[f][1], old[f][0], fine)
+                result = _rounded(fine if old is None else np.where(old[f][1], old[f][0], fine), dtype)
             arrays.append(result)
+        if level:
+            positivity_fix(arrays, new_levels[level - 1], new_h.ndim, new_h.spacing(level), new_h.spacing(level - 1),
+                           model.gamma, model.engine.mean_field)
+            arrays[4] = _rounded(arrays[4], dtype)
+        for f, extra in enumerate(extras):
             for p in new_h.patches_at_level(level):
                 index = tuple(slice(lo, hi + e) for (lo, hi), e in zip(p.box, extra, strict=True))
-                model._write_field(p, f, result[index])
+                model._write_field(p, f, arrays[f][index])
         new_levels[level] = arrays
     model._after_state()
     model.time, model.steps = time, steps
@@ -310,6 +398,13 @@ PROLONG_OP = np.dtype(
 
 #: points per transfer op (one 128-thread block each)
 TRANSFER_OP_POINTS = 4096
+
+#: mirror of the device positivity op (csrc/transfer.cu PositivityOp)
+POSITIVITY_OP = np.dtype({"names": ["fine", "coarse", "ndim", "pad", "n", "f0", "c0"],
+                          "formats": ["<i4"] * 4 + [("<i4", 3)] * 3, "itemsize": 52})
+
+#: parents per positivity op
+POSITIVITY_OP_PARENTS = 1024
 
 
 def _ranges(patches, node_mask, ndim):
@@ -341,7 +436,7 @@ def _pad3(v, fill=0):
 def transfer_ops(old_h, new_h, groups, ndim):
     """Per level of the new hierarchy: (prolongation ops from the new coarser level,
     kept-value ops from the old hierarchy's patches of that level, periodic images
-    included)."""
+    included, positivity ops over the parents of the level's cells)."""
     periodic = new_h.periodic
     pmask = sum(1 << a for a in range(ndim) if periodic[a])
     out = []
@@ -383,13 +478,33 @@ def transfer_ops(old_h, new_h, groups, ndim):
                         prolong.append((fines[i].index, coarses[j].index, g.lo, g.hi, g.node_mask, ndim, ext,
                                         [d0[a] + off[a] for a in range(3)], _pad3(flo[i]), _pad3(clo[j]), coarse_n,
                                         pmask))
+        positivity = []
+        if coarses:
+            # the parents of each new fine patch's cells over each coarse patch (cell ranges
+            # are even, so every parent's children lie in one fine patch)
+            flo, fhi = _ranges(fines, 0, ndim)
+            clo = np.array([[c.box[a][0] for a in range(ndim)] for c in coarses], dtype=np.int64)
+            chi = np.array([[c.box[a][1] for a in range(ndim)] for c in coarses], dtype=np.int64)
+            lo = np.maximum(flo[:, None, :], 2 * clo[None, :, :])
+            hi = np.minimum(fhi[:, None, :], 2 * chi[None, :, :])
+            for i, j in zip(*np.nonzero(np.all(hi > lo, axis=2)), strict=True):
+                n = _pad3((hi[i, j] - lo[i, j]) // 2, 1)
+                f0 = _pad3(lo[i, j] - flo[i] + HALO)
+                c0 = _pad3(lo[i, j] // 2 - clo[j] + HALO)
+                for off, ext in _cut(n, POSITIVITY_OP_PARENTS):
+                    positivity.append((fines[i].index, coarses[j].index, ndim, 0, ext,
+                                       [f0[a] + 2 * off[a] if a < ndim else 0 for a in range(3)],
+                                       [c0[a] + off[a] if a < ndim else 0 for a in range(3)]))
         p = np.zeros(len(prolong), PROLONG_OP)
         for k, r in enumerate(prolong):
             p[k] = r
         k_ops = np.zeros(len(kept), _lib.COPY_OP)
         for k, (dst, src, lo_f, hi_f, d, s, ext) in enumerate(kept):
             k_ops[k] = (dst, src, -1, lo_f, hi_f, -1, ext, d, s, (1, 1, 1), (0, 0, 0), (0, 0, 0), 1.0, 0.0)
-        out.append((p, k_ops))
+        q_ops = np.zeros(len(positivity), POSITIVITY_OP)
+        for k, r in enumerate(positivity):
+            q_ops[k] = r
+        out.append((p, k_ops, q_ops))
     return out
 
 
@@ -409,7 +524,7 @@ def regrid_model_device(model, tags, **options):
     model._build_engine()
     eng = model.engine
     stream = eng._s()
-    for level, (prolong, kept) in enumerate(transfer_ops(old_h, new_h, eng.layout.groups, eng.ndim)):
+    for level, (prolong, kept, positivity) in enumerate(transfer_ops(old_h, new_h, eng.layout.groups, eng.ndim)):
         if prolong.size:
             ops = _device_bytes(prolong, eng.device, PROLONG_OP)
             _lib.call("wb_prolong_ops", eng.precision, eng.state.data_ptr(), eng.patches.data_ptr(), ops.data_ptr(),
@@ -419,6 +534,11 @@ def regrid_model_device(model, tags, **options):
             _lib.call("wb_kept_ops", eng.precision, eng.state.data_ptr(), eng.patches.data_ptr(),
                       old_engine.state.data_ptr(), old_engine.patches.data_ptr(), ops.data_ptr(), int(kept.size),
                       stream)
+        if positivity.size:
+            ops = _device_bytes(positivity, eng.device, POSITIVITY_OP)
+            b = eng.mean_field
+            _lib.call("wb_positivity_ops", eng.precision, eng.state.data_ptr(), eng.patches.data_ptr(), ops.data_ptr(),
+                      int(positivity.size), b[0], b[1], b[2], float(model.gamma), stream)
         eng.fill(eng.state, levels={level})
     torch.cuda.current_stream(eng.device).synchronize()
     del old_engine

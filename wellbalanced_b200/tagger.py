@@ -244,47 +244,65 @@ def experiment(n=32, *, train_steps=48, test_steps=24, horizon=8, threshold=0.05
 
 
 # ---- regridding on the learned tags: the interval the tags allow -----------------------------------
-def covered_level0(model):
-    """Level-0 cells under a level-1 patch (bool, the level-0 shape)."""
+def covered(model, level):
+    """Cells of `level` under a patch of the next level (bool, the level's shape)."""
     h = model.hierarchy
-    out = np.zeros(h.level_shape(0), dtype=bool)
-    for p in h.patches_at_level(1):
+    out = np.zeros(h.level_shape(level), dtype=bool)
+    for p in h.patches_at_level(level + 1):
         out[tuple(slice(lo // 2, (hi + 1) // 2) for lo, hi in p.box)] = True
     return out
 
 
-def amr_run(model, tags_of, *, interval, steps, threshold, buffer=1, max_patch_size=8):
-    """Advance a model with one refined level for `steps` steps, regridding on
-    ``tags_of(model)`` (tags of level 0) before every ``interval``-th step; after each step
-    the plain tagger judges the hierarchy: the fraction of the level-0 cells it flags
-    (``current_tags``, |J| dx > threshold) that no level-1 patch covers.
+def covered_level0(model):
+    """Level-0 cells under a level-1 patch (bool, the level-0 shape)."""
+    return covered(model, 0)
+
+
+def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, max_patch_size=8):
+    """Advance a model with `levels` refined levels for `steps` steps, regridding on
+    ``tags_of(model)`` (tags per level, as ``current_tags``) before every ``interval``-th
+    step (the first regrid repeated `levels` times, so that every level exists from the
+    start); after each step the plain tagger judges the hierarchy: the fraction of the cells
+    it flags (``current_tags``, |J| dx > threshold) on the levels below the finest that no
+    patch of the next level covers.
 
     Returns the largest such miss over the steps, the mean fraction of level-0 cells under
-    level 1 (the refinement's cost) and the regrid count."""
-    worst, refined, regrids = 0.0, [], 0
+    level 1 (the refinement's cost), the mean count of refined cells and the regrid count."""
+    worst, refined, fine_cells, regrids = 0.0, [], [], 0
     for t in range(steps):
         if t % interval == 0:
-            model.regrid({0: tags_of(model)}, buffer=buffer, max_patch_size=max_patch_size)
+            for _ in range(levels if t == 0 else 1):
+                tags = tags_of(model)
+                model.regrid({lev: tags[lev] for lev in tags if lev < levels}, buffer=buffer,
+                             max_patch_size=max_patch_size)
             regrids += 1
         model.step()
-        flagged = model.current_tags(threshold, 1)[0]
-        covered = covered_level0(model)
-        if flagged.any():
-            worst = max(worst, float((flagged & ~covered).sum()) / float(flagged.sum()))
-        refined.append(float(covered.mean()))
-    return {"miss": worst, "refined": float(np.mean(refined)), "regrids": regrids}
+        flagged = model.current_tags(threshold, levels)
+        missed = total = 0
+        for lev, f in flagged.items():
+            total += int(f.sum())
+            missed += int((f & ~covered(model, lev)).sum())
+        if total:
+            worst = max(worst, missed / total)
+        refined.append(float(covered(model, 0).mean()))
+        fine_cells.append(sum(int(np.prod(p.shape)) for p in model.hierarchy.patches if p.level > 0))
+    return {"miss": worst, "refined": float(np.mean(refined)), "refined_cells": float(np.mean(fine_cells)),
+            "regrids": regrids}
 
 
 def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, threshold=0.05, seed=0,
-                   iterations=600, miss=0.005, buffer=1, max_patch_size=8, every=2):
-    """The regrid interval each tagger reaches on the multi-blast run with one refined level.
+                   iterations=600, miss=0.005, levels=1, buffer=1, max_patch_size=8, every=2, fallback=True):
+    """The regrid interval each tagger reaches on the multi-blast run with `levels` refined levels.
 
     For every interval K: a tagger trained on the first ``train_steps`` steps of a uniform
     run to predict the plain flags of the next K steps, then two refined runs over the next
     ``test_steps`` steps from the same state, one regridded every K steps on the learned
     tags, one on the plain tags of the regrid step (``current_tags``, grown by the
     clustering's ``buffer`` like the other); the plain tagger judges both after every step.
-    The interval a tagger reaches is the largest K whose worst miss stays under 1%."""
+    With ``fallback`` the learned run regrids on the union of the learned tags and the plain
+    tags of the regrid step (the plain tagger as the fallback: every cell it flags now is
+    refined, the learned tags add the cells it will flag). The interval a tagger reaches is
+    the largest K whose worst miss stays under 1%."""
     out = {"cells": n**3, "threshold": threshold, "intervals": {}}
     for K in intervals:
         tagger = LearnedTagger(seed=seed)
@@ -295,12 +313,18 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
         tagger.fit(X, Y, iterations=iterations, seed=seed)
         tagger.choose_threshold(X, Y, miss=miss)
         runs = {}
-        for name, tags_of in (("learned", lambda m: tagger.tags(m, 1)[0]),
-                              ("plain", lambda m: m.current_tags(threshold, 1)[0])):
+        def learned(m, tagger=tagger):
+            tags = tagger.tags(m, levels)
+            if fallback:
+                plain = m.current_tags(threshold, levels)
+                tags = {lev: tags[lev] | plain[lev] for lev in tags}
+            return tags
+
+        for name, tags_of in (("learned", learned), ("plain", lambda m: m.current_tags(threshold, levels))):
             model = multiblast(n, seed=seed)
             model.advance(train_steps)
-            runs[name] = amr_run(model, tags_of, interval=K, steps=test_steps, threshold=threshold, buffer=buffer,
-                                 max_patch_size=max_patch_size)
+            runs[name] = amr_run(model, tags_of, interval=K, steps=test_steps, threshold=threshold, levels=levels,
+                                 buffer=buffer, max_patch_size=max_patch_size)
         out["intervals"][K] = runs
     for name in ("learned", "plain"):
         ok = [K for K in intervals if out["intervals"][K][name]["miss"] < 0.01]
