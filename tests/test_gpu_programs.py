@@ -52,8 +52,8 @@ def _refined_3d(precision, **options):
 
 def _pair(build, precision, **options):
     a, b = build(precision, **options), build(precision, **options)
-    assert a.engine.use_programs and a.engine.max_level > 0
-    b.engine.use_programs = False
+    assert a.engine.max_level > 0 and not a.engine.use_programs  # separate launches by default
+    a.engine.use_programs = True
     return a, b
 
 

@@ -1,9 +1,13 @@
 // The float32 face arithmetic (MUSCL slopes, HLLD) written over lane types: `L1` (one
-// face) and `F2` (two faces at once on the packed float32 instructions of sm_100).
+// value) and `F2` (two values on the packed float32 instructions of sm_100). A face pairs
+// what it computes twice: the left and right states' slopes and reconstruction, their fast
+// speeds, total pressures and star states; the rest runs on one lane.
 //
 // Same formulas, region selection and near-degenerate fallback as the float64 templates of
 // numerics.cuh (mhd_sweep_pyccel.py:25-48, 51-61, 64-98, 101-145, 148-251; Miyoshi & Kusano
-// 2005); the multiply-adds are explicit, so one face gets the same bits in either lane type.
+// 2005); the multiply-adds are explicit and every float32 face of every kernel (stage
+// kernels, refluxing) runs this code, so a face's flux has the same bits wherever it is
+// formed.
 #pragma once
 
 #include "lanes.cuh"
@@ -98,63 +102,63 @@ __device__ __forceinline__ void star_tangential_l(const V (&w)[7], V bn, V bn2, 
   bt2 = sel(regular, w[6] * scale, w[6]);
 }
 
-template <typename V>
-__device__ __forceinline__ void hlld_front_l(const V (&L)[7], const V (&Rt)[7], V bn, V gamma, HlldFrontL<V>& o) {
-  const V rl = L[0], vl = L[1], rr = Rt[0], vr = Rt[1];
-  const V cf = lmax(fast_speed_l(rl, L[4], bn, L[5], L[6], gamma), fast_speed_l(rr, Rt[4], bn, Rt[5], Rt[6], gamma));
+// The front half of one face with its left and right sides in the two lanes of F2 (fast
+// speeds, total pressures, d = (S - v) rho and the star states of both sides in one packed
+// evaluation each); S_M and p_T* on one lane. Where either side's star denominator is near
+// zero (relative size below kNearDegenerate32) the front is redone in float64 from the
+// float32 inputs.
+__device__ __forceinline__ void hlld_front_lr(const float (&L)[7], const float (&Rt)[7], float bn, float gamma,
+                                              HlldFrontL<L1>& o) {
+  F2 w[7];
+#pragma unroll
+  for (int c = 0; c < 7; ++c) w[c] = F2(L[c], Rt[c]);
+  const L1 vl = L[1], vr = Rt[1];
+  const F2 cf2 = fast_speed_l<F2>(w[0], w[4], F2(bn), w[5], w[6], F2(gamma));
+  const L1 cf = lmax(L1(cf2.v.x), L1(cf2.v.y));
   o.sl = lmin(vl, vr) - cf;
   o.sr = lmax(vl, vr) + cf;
-  const V bn2 = bn * bn;
-  o.ptl = fma(V(0.5f), fma(L[5], L[5], fma(L[6], L[6], bn2)), L[4]);
-  o.ptr = fma(V(0.5f), fma(Rt[5], Rt[5], fma(Rt[6], Rt[6], bn2)), Rt[4]);
-  const V dl = (o.sl - vl) * rl;
-  const V dr = (o.sr - vr) * rr;
-  const V ndl = lneg(dl);
-  const V inv_dd = linv(dr - dl);
+  const L1 bn2 = L1(bn) * L1(bn);
+  const F2 pt2 = fma(F2(0.5f), fma(w[5], w[5], fma(w[6], w[6], F2(bn2.v))), w[4]);
+  o.ptl = pt2.v.x;
+  o.ptr = pt2.v.y;
+  const F2 s2(o.sl.v, o.sr.v);
+  const F2 d2 = (s2 - w[1]) * w[0];
+  const L1 dl = d2.v.x, dr = d2.v.y;
+  const L1 ndl = lneg(dl);
+  const L1 inv_dd = linv(dr - dl);
   o.sm = fma(dr, vr, fma(ndl, vl, o.ptl - o.ptr)) * inv_dd;
   o.pts = fma(dr, o.ptl, fma(ndl, o.ptr, dl * dr * (vr - vl))) * inv_dd;
-  star_tangential_l(L, bn, bn2, o.sl, dl, o.ptl, o.sm, o.rsl, o.vtl1, o.vtl2, o.btl1, o.btl2, o.den_l);
-  star_tangential_l(Rt, bn, bn2, o.sr, dr, o.ptr, o.sm, o.rsr, o.vtr1, o.vtr2, o.btr1, o.btr2, o.den_r);
-}
-
-// Where a lane's star denominator is near zero (relative size below kNearDegenerate32),
-// that lane's front half is redone in float64 from its float32 inputs.
-template <typename V>
-__device__ __forceinline__ void hlld_front_checked_l(const V (&L)[7], const V (&Rt)[7], V bn, V gamma,
-                                                     HlldFrontL<V>& o) {
-  hlld_front_l(L, Rt, bn, gamma, o);
-  const V bn2 = bn * bn;
-  const V near = V(kNearDegenerate32);
-  const auto mask = labs(o.den_l) < near * (o.ptl + bn2) | labs(o.den_r) < near * (o.ptr + bn2);
-  if (!any(mask)) return;
+  F2 rho_s, vt1, vt2, bt1, bt2, den;
+  star_tangential_l<F2>(w, F2(bn), F2(bn2.v), s2, d2, pt2, F2(o.sm.v), rho_s, vt1, vt2, bt1, bt2, den);
+  o.rsl = rho_s.v.x, o.rsr = rho_s.v.y;
+  o.vtl1 = vt1.v.x, o.vtr1 = vt1.v.y;
+  o.vtl2 = vt2.v.x, o.vtr2 = vt2.v.y;
+  o.btl1 = bt1.v.x, o.btr1 = bt1.v.y;
+  o.btl2 = bt2.v.x, o.btr2 = bt2.v.y;
+  o.den_l = den.v.x, o.den_r = den.v.y;
+  if (!any(labs(den) < F2(kNearDegenerate32) * (pt2 + F2(bn2.v)))) return;
+  double Ld[7], Rd[7];
 #pragma unroll
-  for (int i = 0; i < Lanes<V>::kCount; ++i) {
-    if (!lane_mask(mask, i)) continue;
-    double Ld[7], Rd[7];
-#pragma unroll
-    for (int c = 0; c < 7; ++c) {
-      Ld[c] = lane(L[c], i);
-      Rd[c] = lane(Rt[c], i);
-    }
-    HlldFront<double> d;
-    hlld_front<double, MathRefined>(Ld, Rd, double(lane(bn, i)), double(lane(gamma, i)), d);
-    set_lane(o.sl, i, float(d.sl)), set_lane(o.sr, i, float(d.sr));
-    set_lane(o.ptl, i, float(d.ptl)), set_lane(o.ptr, i, float(d.ptr));
-    set_lane(o.sm, i, float(d.sm)), set_lane(o.pts, i, float(d.pts));
-    set_lane(o.rsl, i, float(d.rsl)), set_lane(o.vtl1, i, float(d.vtl1)), set_lane(o.vtl2, i, float(d.vtl2));
-    set_lane(o.btl1, i, float(d.btl1)), set_lane(o.btl2, i, float(d.btl2)), set_lane(o.den_l, i, float(d.den_l));
-    set_lane(o.rsr, i, float(d.rsr)), set_lane(o.vtr1, i, float(d.vtr1)), set_lane(o.vtr2, i, float(d.vtr2));
-    set_lane(o.btr1, i, float(d.btr1)), set_lane(o.btr2, i, float(d.btr2)), set_lane(o.den_r, i, float(d.den_r));
+  for (int c = 0; c < 7; ++c) {
+    Ld[c] = L[c];
+    Rd[c] = Rt[c];
   }
+  HlldFront<double> d;
+  hlld_front<double, MathRefined>(Ld, Rd, double(bn), double(gamma), d);
+  o.sl = float(d.sl), o.sr = float(d.sr), o.ptl = float(d.ptl), o.ptr = float(d.ptr);
+  o.sm = float(d.sm), o.pts = float(d.pts);
+  o.rsl = float(d.rsl), o.vtl1 = float(d.vtl1), o.vtl2 = float(d.vtl2);
+  o.btl1 = float(d.btl1), o.btl2 = float(d.btl2), o.den_l = float(d.den_l);
+  o.rsr = float(d.rsr), o.vtr1 = float(d.vtr1), o.vtr2 = float(d.vtr2);
+  o.btr1 = float(d.btr1), o.btr2 = float(d.btr2), o.den_r = float(d.den_r);
 }
 
-// HLLD flux of one face per lane (straight-line code: the star / double-star flux of the
-// side of the contact the face lies on, selected at the end; as hlld_flux in numerics.cuh).
+// The back half of the HLLD flux from its front (straight-line code: the star / double-star
+// flux of the side of the contact the face lies on, selected at the end; as hlld_flux in
+// numerics.cuh).
 template <typename V>
-__device__ __forceinline__ void hlld_flux_l(const V (&L)[7], const V (&Rt)[7], V bn, V gamma, V inv_gm1,
-                                            V (&F)[7]) {
-  HlldFrontL<V> fr;
-  hlld_front_checked_l(L, Rt, bn, gamma, fr);
+__device__ __forceinline__ void hlld_tail_l(const V (&L)[7], const V (&Rt)[7], V bn, V inv_gm1,
+                                            const HlldFrontL<V>& fr, V (&F)[7]) {
   const V sm = fr.sm;
   const V sql = lsqrt(fr.rsl);
   const V sqr = lsqrt(fr.rsr);
@@ -214,44 +218,6 @@ __device__ __forceinline__ void hlld_flux_l(const V (&L)[7], const V (&Rt)[7], V
   }
 }
 
-// Left / right states of a face from four consecutive cells (face between q1 and q2),
-// first order where a reconstructed density or pressure is not positive.
-template <int LIM, typename V>
-__device__ __forceinline__ void reconstruct_l(const V (&q0)[7], const V (&q1)[7], const V (&q2)[7],
-                                              const V (&q3)[7], V (&L)[7], V (&Rt)[7]) {
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    const V d1 = q2[c] - q1[c];
-    const V s1 = limited_slope_l<LIM>(q1[c] - q0[c], d1);
-    const V s2 = limited_slope_l<LIM>(d1, q3[c] - q2[c]);
-    L[c] = fma(V(0.5f), s1, q1[c]);
-    Rt[c] = fma(V(-0.5f), s2, q2[c]);
-  }
-  const auto first_order = L[0] <= V(0.0f) | L[4] <= V(0.0f) | Rt[0] <= V(0.0f) | Rt[4] <= V(0.0f);
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    L[c] = sel(first_order, q1[c], L[c]);
-    Rt[c] = sel(first_order, q2[c], Rt[c]);
-  }
-}
-
-// The same from the two cells beside the face and their limited slopes, already formed.
-template <typename V>
-__device__ __forceinline__ void reconstruct_sloped_l(const V (&q1)[7], const V (&q2)[7], const V (&s1)[7],
-                                                     const V (&s2)[7], V (&L)[7], V (&Rt)[7]) {
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    L[c] = fma(V(0.5f), s1[c], q1[c]);
-    Rt[c] = fma(V(-0.5f), s2[c], q2[c]);
-  }
-  const auto first_order = L[0] <= V(0.0f) | L[4] <= V(0.0f) | Rt[0] <= V(0.0f) | Rt[4] <= V(0.0f);
-#pragma unroll
-  for (int c = 0; c < 7; ++c) {
-    L[c] = sel(first_order, q1[c], L[c]);
-    Rt[c] = sel(first_order, q2[c], Rt[c]);
-  }
-}
-
 // ---- float32 entry points of the kernels: one face (L1) ------------------------------------
 template <typename V, int N>
 __device__ __forceinline__ void to_lanes(const float (&a)[N], V (&b)[N]) {
@@ -265,38 +231,69 @@ __device__ __forceinline__ void from_lanes(const L1 (&a)[N], float (&b)[N]) {
   for (int c = 0; c < N; ++c) b[c] = a[c].v;
 }
 
+// The float32 HLLD flux of one face: front on the packed lanes, back half on one lane.
 __device__ __forceinline__ void hlld_flux(const float (&L)[7], const float (&Rt)[7], float bn, float gamma,
                                           float inv_gm1, float (&F)[7]) {
+  HlldFrontL<L1> fr;
+  hlld_front_lr(L, Rt, bn, gamma, fr);
   L1 l[7], r[7], f[7];
   to_lanes(L, l);
   to_lanes(Rt, r);
-  hlld_flux_l<L1>(l, r, L1(bn), L1(gamma), L1(inv_gm1), f);
+  hlld_tail_l<L1>(l, r, L1(bn), L1(inv_gm1), fr, f);
   from_lanes(f, F);
 }
 
+// One face's reconstruction with its left and right states in the two lanes of F2: the
+// two limited slopes of each component in one packed evaluation (lane x: the cell below the
+// face, lane y: the cell above), the states as one packed FMA. Lane by lane the same
+// operations as reconstruct_l<L1>.
 template <int LIM>
 __device__ __forceinline__ void reconstruct(const float (&q0)[7], const float (&q1)[7], const float (&q2)[7],
                                             const float (&q3)[7], float (&L)[7], float (&Rt)[7]) {
-  L1 a0[7], a1[7], a2[7], a3[7], l[7], r[7];
-  to_lanes(q0, a0);
-  to_lanes(q1, a1);
-  to_lanes(q2, a2);
-  to_lanes(q3, a3);
-  reconstruct_l<LIM>(a0, a1, a2, a3, l, r);
-  from_lanes(l, L);
-  from_lanes(r, Rt);
+  const F2 half(0.5f, -0.5f);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    const F2 a01(q0[c], q1[c]), a12(q1[c], q2[c]), a23(q2[c], q3[c]);
+    const F2 lr = fma(half, limited_slope_l<LIM>(a12 - a01, a23 - a12), a12);
+    L[c] = lr.v.x;
+    Rt[c] = lr.v.y;
+  }
+  const bool first_order = L[0] <= 0.0f || L[4] <= 0.0f || Rt[0] <= 0.0f || Rt[4] <= 0.0f;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    L[c] = first_order ? q1[c] : L[c];
+    Rt[c] = first_order ? q2[c] : Rt[c];
+  }
 }
 
 __device__ __forceinline__ void reconstruct_sloped(const float (&q1)[7], const float (&q2)[7], const float (&s1)[7],
                                                    const float (&s2)[7], float (&L)[7], float (&Rt)[7]) {
-  L1 a1[7], a2[7], b1[7], b2[7], l[7], r[7];
-  to_lanes(q1, a1);
-  to_lanes(q2, a2);
-  to_lanes(s1, b1);
-  to_lanes(s2, b2);
-  reconstruct_sloped_l(a1, a2, b1, b2, l, r);
-  from_lanes(l, L);
-  from_lanes(r, Rt);
+  const F2 half(0.5f, -0.5f);
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    const F2 lr = fma(half, F2(s1[c], s2[c]), F2(q1[c], q2[c]));
+    L[c] = lr.v.x;
+    Rt[c] = lr.v.y;
+  }
+  const bool first_order = L[0] <= 0.0f || L[4] <= 0.0f || Rt[0] <= 0.0f || Rt[4] <= 0.0f;
+#pragma unroll
+  for (int c = 0; c < 7; ++c) {
+    L[c] = first_order ? q1[c] : L[c];
+    Rt[c] = first_order ? q2[c] : Rt[c];
+  }
+}
+
+// Limited slopes of seven components from their backward (a) and forward (b) differences,
+// two components per packed evaluation (lane by lane as limited_slope_l<L1>).
+template <int LIM>
+__device__ __forceinline__ void limited_slopes7(const float (&a)[7], const float (&b)[7], float (&out)[7]) {
+#pragma unroll
+  for (int c = 0; c < 6; c += 2) {
+    const F2 s = limited_slope_l<LIM>(F2(a[c], a[c + 1]), F2(b[c], b[c + 1]));
+    out[c] = s.v.x;
+    out[c + 1] = s.v.y;
+  }
+  out[6] = limited_slope_l<LIM>(L1(a[6]), L1(b[6])).v;
 }
 
 template <int LIM>

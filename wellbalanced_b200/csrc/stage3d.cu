@@ -109,55 +109,31 @@ __device__ __forceinline__ int face_slot(int plane) {
 
 // The y- and z-face of a B1 thread from the primitive plane P (rows of NR values): the
 // y-stencil starts at ry with stride sy, the z-stencil at rz with stride 1; fluxes to
-// outy[c G], outz[c G]. Float32 arithmetic evaluates the two faces together on the packed
-// float32 lanes (F2); float64 one after the other.
-constexpr bool kPairFaces = false;
-
+// outy[c G], outz[c G].
 template <int LIM, typename R>
 __device__ __forceinline__ void yz_faces(const R* P, int NR, int ry, int sy, int rz, R bny, R bnz, R gamma,
                                          R inv_gm1, R* outy, R* outz, int G) {
   constexpr int yrow[7] = {0, 2, 3, 1, 4, 7, 5};
   constexpr int zrow[7] = {0, 3, 1, 2, 4, 5, 6};
-  if constexpr (kPairFaces && std::is_same<R, float>::value) {
-    F2 a0[7], a1[7], a2[7], a3[7];
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const int* rows = side == 0 ? yrow : zrow;
+    const int r0 = side == 0 ? ry : rz, st = side == 0 ? sy : 1;
+    R a0[7], a1[7], a2[7], a3[7];
 #pragma unroll
     for (int c = 0; c < 7; ++c) {
-      const R* y = P + yrow[c] * NR + ry;
-      const R* z = P + zrow[c] * NR + rz;
-      a0[c] = F2(y[0], z[0]);
-      a1[c] = F2(y[sy], z[1]);
-      a2[c] = F2(y[2 * sy], z[2]);
-      a3[c] = F2(y[3 * sy], z[3]);
+      const R* row = P + rows[c] * NR + r0;
+      a0[c] = row[0];
+      a1[c] = row[st];
+      a2[c] = row[2 * st];
+      a3[c] = row[3 * st];
     }
-    F2 L[7], Rt[7], F[7];
-    reconstruct_l<LIM>(a0, a1, a2, a3, L, Rt);
-    hlld_flux_l<F2>(L, Rt, F2(bny, bnz), F2(gamma), F2(inv_gm1), F);
+    R L[7], Rt[7], F[7];
+    reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
+    hlld_flux(L, Rt, side == 0 ? bny : bnz, gamma, inv_gm1, F);
+    R* out = side == 0 ? outy : outz;
 #pragma unroll
-    for (int c = 0; c < 7; ++c) {
-      outy[c * G] = F[c].v.x;
-      outz[c * G] = F[c].v.y;
-    }
-  } else {
-#pragma unroll
-    for (int side = 0; side < 2; ++side) {
-      const int* rows = side == 0 ? yrow : zrow;
-      const int r0 = side == 0 ? ry : rz, st = side == 0 ? sy : 1;
-      R a0[7], a1[7], a2[7], a3[7];
-#pragma unroll
-      for (int c = 0; c < 7; ++c) {
-        const R* row = P + rows[c] * NR + r0;
-        a0[c] = row[0];
-        a1[c] = row[st];
-        a2[c] = row[2 * st];
-        a3[c] = row[3 * st];
-      }
-      R L[7], Rt[7], F[7];
-      reconstruct<LIM>(a0, a1, a2, a3, L, Rt);
-      hlld_flux(L, Rt, side == 0 ? bny : bnz, gamma, inv_gm1, F);
-      R* out = side == 0 ? outy : outz;
-#pragma unroll
-      for (int c = 0; c < 7; ++c) out[c * G] = F[c];
-    }
+    for (int c = 0; c < 7; ++c) out[c * G] = F[c];
   }
 }
 
@@ -380,8 +356,18 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY,
       }
       // the slope of plane p, kept for face p + 1: each cell's x-slope is formed once
       R now[7];
+      if constexpr (std::is_same<R, float>::value) {
+        float back[7], fwd[7];
 #pragma unroll
-      for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q1[cc] - qm[cc], q2[cc] - q1[cc]);
+        for (int cc = 0; cc < 7; ++cc) {
+          back[cc] = q1[cc] - qm[cc];
+          fwd[cc] = q2[cc] - q1[cc];
+        }
+        limited_slopes7<LIM>(back, fwd, now);
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) now[cc] = limited_slope<LIM>(q1[cc] - qm[cc], q2[cc] - q1[cc]);
+      }
       const R* Bp = sBn + (PHYS ? face_slot<PHYS>(p) : ((p + 4) & 1)) * 3 * NR;
       if (p >= x0) {
         R L[7], Rt[7], F[7];
@@ -486,7 +472,6 @@ __global__ void __launch_bounds__(threads3d<TY, TZ>(), (Occupancy3D<R, PHYS, TY,
       auto yi = [&](int fj, int kk) { return fj * GZ + (kk + 1); };
       auto zi = [&](int jj, int fk) { return (jj + 1) * GZ + fk; };
       auto gi = [&](int jj, int kk) { return (jj + 1) * GZ + (kk + 1); };
-      const int I = p + kHalo, J = gj + kHalo, K = gk + kHalo;
       // cells of plane p-1
       if (do_cell) {
         const int64_t o = o_cell;

@@ -11,7 +11,7 @@
 //     same level held (periodic images included, so the duplicate node planes of a
 //     periodic axis agree);
 //   * positivity ops revisit every prolonged parent: where a child of the minmod
-//     prolongation has a non-positive density or pressure (conserved cells and a field
+//     prolongation has a non-positive density or a pressure below a quarter of the parent's (conserved cells and a field
 //     from the interpolated potential do not bound the pressure: the children's kinetic
 //     and magnetic energies exceed the coarse ones at a strong front in low-beta gas, where
 //     the reference's next step raises), the parent's children take its density,
@@ -186,14 +186,21 @@ __device__ __forceinline__ double magnetic(const double (&b)[3]) {
   return dmul(0.5, dadd(dadd(dmul(b[0], b[0]), dmul(b[1], b[1])), dmul(b[2], b[2])));
 }
 
+// A child whose pressure falls below this fraction of its parent's counts as collapsed: at
+// a front the prolonged children's pressures fall steeply before they turn negative, and a
+// child left at a few percent of its neighbours' pressure turns negative in the next step.
+constexpr double kPressureFraction = 0.25;
+
 // One thread per parent. Children in the order of their offsets (last axis fastest).
-// Where every child has a positive, finite density and pressure nothing changes. Else,
+// Where every child has a positive density and a pressure above kPressureFraction times
+// the parent's (p = (gamma - 1)(E - K - M), M from the coarse potential) nothing changes. Else,
 // with the parent's density rho, momentum m, energy E, kinetic energy K, magnetic energy
 // M (its cell-centred field from the coarse potential) and pressure p, each child takes
 // rho and m (and, in 2D, the parent's B_z) and, with M_i its own magnetic energy (its field
 // from the fine potential) and M' the children's mean of M_i:
-//   E_i = E + (M_i - M')                 where (gamma - 1)(E - K - M') > 0 (the energy's
-//                                        integral kept; every child at that pressure),
+//   E_i = E + (M_i - M')                 where (gamma - 1)(E - K - M') > kPressureFraction p
+//                                        (the energy's integral kept; every child at that
+//                                        pressure),
 //   E_i = p / (gamma - 1) + K + M_i      else (every child at the parent's pressure).
 template <typename S>
 __global__ void __launch_bounds__(kTransferThreads) positivity_ops_kernel(S* __restrict__ pool,
@@ -217,6 +224,18 @@ __global__ void __launch_bounds__(kTransferThreads) positivity_ops_kernel(S* __r
                         op.ndim == 3 ? i & 1 : 0};
       for (int a = 0; a < 3; ++a) x[a] = a < op.ndim ? op.f0[a] + 2 * q[a] + o[a] : 0;
     };
+    int xc[3];
+    for (int a = 0; a < 3; ++a) xc[a] = a < op.ndim ? op.c0[a] + q[a] : 0;
+    const int64_t oc = point_offset(C, xc[0], xc[1], xc[2]);
+    const S* parent = pool + C.off + oc;
+    const S rho = parent[0], m0 = parent[C.fstride], m1 = parent[2 * C.fstride], m2 = parent[3 * C.fstride];
+    const double energy = double(parent[4 * C.fstride]);
+    double bc[3];
+    cell_field(pool, C, op.ndim, xc, b0, bc);
+    const double k = kinetic(double(rho), double(m0), double(m1), double(m2));
+    const double pc = dmul(gm1, dsub(dsub(energy, k), magnetic(bc)));
+    if (!(double(rho) > 0.0 && pc > 0.0)) continue;  // the parent itself is not a valid state
+    const double low = dmul(kPressureFraction, pc);
     bool bad = false;
     for (int i = 0; i < nchild; ++i) {
       int x[3];
@@ -230,20 +249,9 @@ __global__ void __launch_bounds__(kTransferThreads) positivity_ops_kernel(S* __r
                                                                                    double(cell[2 * F.fstride]),
                                                                                    double(cell[3 * F.fstride]))),
                                       magnetic(b)));
-      if (!(r > 0.0 && p > 0.0 && isfinite(p))) bad = true;
+      if (!(r > 0.0 && p > low && isfinite(p))) bad = true;
     }
     if (!bad) continue;
-    int xc[3];
-    for (int a = 0; a < 3; ++a) xc[a] = a < op.ndim ? op.c0[a] + q[a] : 0;
-    const int64_t oc = point_offset(C, xc[0], xc[1], xc[2]);
-    const S* parent = pool + C.off + oc;
-    const S rho = parent[0], m0 = parent[C.fstride], m1 = parent[2 * C.fstride], m2 = parent[3 * C.fstride];
-    const double energy = double(parent[4 * C.fstride]);
-    double bc[3];
-    cell_field(pool, C, op.ndim, xc, b0, bc);
-    const double k = kinetic(double(rho), double(m0), double(m1), double(m2));
-    const double pc = dmul(gm1, dsub(dsub(energy, k), magnetic(bc)));
-    if (!(double(rho) > 0.0 && pc > 0.0)) continue;  // the parent itself is not a valid state
     // the children's magnetic energies (2D: with the parent's B_z)
     double mag[8];
     double sum = 0.0;
@@ -257,7 +265,7 @@ __global__ void __launch_bounds__(kTransferThreads) positivity_ops_kernel(S* __r
       sum = dadd(sum, mag[i]);
     }
     const double mean = ddiv(sum, double(nchild));
-    const bool keep = dmul(gm1, dsub(dsub(energy, k), mean)) > 0.0;
+    const bool keep = dmul(gm1, dsub(dsub(energy, k), mean)) > low;
     const double floor = dadd(ddiv(pc, gm1), k);
     for (int i = 0; i < nchild; ++i) {
       int x[3];

@@ -145,8 +145,11 @@ class Engine:
         #: the launching stream's handle while a step issues its launches (looked up once)
         self._step_stream = None
         #: run the reflux, restriction, halo-fill and stable-step phases between the stage
-        #: kernels as op programs (`wb_run_program`, one launch each) on refined hierarchies
-        self.use_programs = self.max_level > 0
+        #: kernels as op programs (`wb_run_program`, one launch each: six launches per
+        #: refined step instead of ~26). Off by default: on the B200 the separate launches
+        #: finish the ~2100-patch Harris step in 0.66 ms against 0.79 ms for the programs,
+        #: whose in-kernel phase waits cost more than the launch boundaries they replace
+        self.use_programs = False
         self._programs = {}
         #: dt on the device belongs to the current state (set by `prime_dt` and each
         #: programmed step; cleared by every other launch or write that changes the state)

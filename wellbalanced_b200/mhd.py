@@ -325,13 +325,15 @@ class MHD2D:
         self._write(patch, 6, np.asarray(az, dtype=float))
         self._after_state()
 
-    def _after_state(self):
+    def _after_state(self, tune=True):
+        """The halos and the restriction of a new state; with `tune`, the autotuner's tile
+        (a regrid keeps the tile tuned before it: `tune` False)."""
         self.engine.dt_ready = False
         eng = self.engine
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
-        if self._auto_tile and self._fused and eng.physics is None and getattr(self, "_group", None) is None:
+        if tune and self._auto_tile and self._fused and eng.physics is None and getattr(self, "_group", None) is None:
             from wellbalanced_b200.autotune import tune_tile2d
 
             self.tile, timings = tune_tile2d(eng)

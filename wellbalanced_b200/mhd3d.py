@@ -283,13 +283,15 @@ class MHD3D:
             self._write(patch, 5 + c, np.asarray(value, dtype=float), _EXTRA[c])
         self._after_state()
 
-    def _after_state(self):
+    def _after_state(self, tune=True):
+        """The halos and the restriction of a new state; with `tune`, the autotuner's x-plane
+        count (a regrid keeps the count tuned before it: `tune` False)."""
         self.engine.dt_ready = False
         eng = self.engine
         if self.hierarchy.max_level > 0:
             eng.restrict(eng.state, self._groups_all)
         eng.fill(eng.state)
-        if self._auto_lx:
+        if tune and self._auto_lx:
             from wellbalanced_b200.autotune import tune_lx
 
             self.lx, timings = tune_lx(eng)

@@ -274,11 +274,17 @@ def _magnetic(b):
     return 0.5 * ((b[0] * b[0] + b[1] * b[1]) + b[2] * b[2])
 
 
+#: a prolonged child below this fraction of its parent's pressure counts as collapsed
+#: (csrc/transfer.cu kPressureFraction)
+PRESSURE_FRACTION = 0.25
+
+
 def positivity_fix(fine, coarse, ndim, spacing_fine, spacing_coarse, gamma, mean_field):
     """The positivity pass of the transfer on a level's dense arrays (``fine``, fields as
-    the pool's; ``coarse`` the level below), in place: every parent whose children include a
-    non-positive density or pressure gives them its density, momentum (2D: B_z) and the
-    energy E + M_i - mean(M) while (gamma - 1)(E - K - mean(M)) > 0, else
+    the pool's; ``coarse`` the level below), in place: every valid parent whose children
+    include a non-positive density or a pressure below ``PRESSURE_FRACTION`` times its own
+    gives them its density, momentum (2D: B_z) and the energy E + M_i - mean(M) while
+    (gamma - 1)(E - K - mean(M)) is above that fraction of its pressure p, else
     p / (gamma - 1) + K + M_i (M_i a child's magnetic energy from the fine potential;
     ``csrc/transfer.cu`` positivity_ops_kernel, operation by operation). Returns the count
     of parents changed."""
@@ -288,20 +294,21 @@ def positivity_fix(fine, coarse, ndim, spacing_fine, spacing_coarse, gamma, mean
     def child(a, o):
         return a[tuple(slice(x, None, 2) for x in o)]
 
+    bc = _cell_field(coarse, ndim, spacing_coarse, mean_field)
+    k = _kinetic(coarse[0], coarse[1], coarse[2], coarse[3])
+    pc = gm1 * ((coarse[4] - k) - _magnetic(bc))
+    low = PRESSURE_FRACTION * pc
     bf = _cell_field(fine, ndim, spacing_fine, mean_field)
     bad = np.zeros(coarse[0].shape, dtype=bool)
     for o in offsets:
         r = child(fine[0], o)
-        k = _kinetic(r, child(fine[1], o), child(fine[2], o), child(fine[3], o))
-        p = gm1 * ((child(fine[4], o) - k) - _magnetic([child(b, o) for b in bf]))
+        kc = _kinetic(r, child(fine[1], o), child(fine[2], o), child(fine[3], o))
+        p = gm1 * ((child(fine[4], o) - kc) - _magnetic([child(b, o) for b in bf]))
         with np.errstate(invalid="ignore"):
-            bad |= ~((r > 0.0) & (p > 0.0) & np.isfinite(p))
-    if not bad.any():
-        return 0
-    bc = _cell_field(coarse, ndim, spacing_coarse, mean_field)
-    k = _kinetic(coarse[0], coarse[1], coarse[2], coarse[3])
-    pc = gm1 * ((coarse[4] - k) - _magnetic(bc))
+            bad |= ~((r > 0.0) & (p > low) & np.isfinite(p))
     fix = bad & (coarse[0] > 0.0) & (pc > 0.0)
+    if not fix.any():
+        return 0
     mags = []
     total = np.zeros(coarse[0].shape)
     for o in offsets:
@@ -311,7 +318,7 @@ def positivity_fix(fine, coarse, ndim, spacing_fine, spacing_coarse, gamma, mean
         mags.append(_magnetic(b))
         total = total + mags[-1]
     mean = total / float(len(offsets))
-    keep = gm1 * ((coarse[4] - k) - mean) > 0.0
+    keep = gm1 * ((coarse[4] - k) - mean) > low
     floor = pc / gm1 + k
     for o, mag in zip(offsets, mags, strict=True):
         energy = np.where(keep, coarse[4] + (mag - mean), floor + mag)
@@ -380,7 +387,7 @@ def regrid_model_host(model, tags, **options):
                 index = tuple(slice(lo, hi + e) for (lo, hi), e in zip(p.box, extra, strict=True))
                 model._write_field(p, f, arrays[f][index])
         new_levels[level] = arrays
-    model._after_state()
+    model._after_state(tune=False)
     model.time, model.steps = time, steps
     model.engine.time.fill_(time)
 
@@ -542,7 +549,7 @@ def regrid_model_device(model, tags, **options):
         eng.fill(eng.state, levels={level})
     torch.cuda.current_stream(eng.device).synchronize()
     del old_engine
-    model._after_state()
+    model._after_state(tune=False)
     model.time, model.steps = time, steps
     eng.time.fill_(time)
 

@@ -258,36 +258,52 @@ def covered_level0(model):
     return covered(model, 0)
 
 
-def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, max_patch_size=8):
+def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, max_patch_size=8, judge=None):
     """Advance a model with `levels` refined levels for `steps` steps, regridding on
     ``tags_of(model)`` (tags per level, as ``current_tags``) before every ``interval``-th
     step (the first regrid repeated `levels` times, so that every level exists from the
-    start); after each step the plain tagger judges the hierarchy: the fraction of the cells
-    it flags (``current_tags``, |J| dx > threshold) on the levels below the finest that no
-    patch of the next level covers.
+    start); after each step the plain tagger judges the hierarchy: the fraction of the
+    level-0 cells it flags (|J| dx > threshold) that no level-1 patch covers.
+
+    The flags come from ``judge``, a uniform run of the same problem advanced in lockstep
+    (the refined run's dt), when given: the plain tagger on the refined run's own level 0
+    also flags the coarse cells beside each coarse-fine boundary, where the central
+    differences straddle restricted fine values, and those flags follow the patches rather
+    than the flow. Without a judge, the refined run's own level-0 flags.
 
     Returns the largest such miss over the steps, the mean fraction of level-0 cells under
-    level 1 (the refinement's cost), the mean count of refined cells and the regrid count."""
+    level 1 (the refinement's cost), the mean count of refined cells, the regrid count and
+    the seconds spent regridding and stepping."""
+    import time
+
+    import torch
+
     worst, refined, fine_cells, regrids = 0.0, [], [], 0
+    regrid_seconds = step_seconds = 0.0
     for t in range(steps):
         if t % interval == 0:
+            start = time.perf_counter()
             for _ in range(levels if t == 0 else 1):
                 tags = tags_of(model)
                 model.regrid({lev: tags[lev] for lev in tags if lev < levels}, buffer=buffer,
                              max_patch_size=max_patch_size)
             regrids += 1
-        model.step()
-        flagged = model.current_tags(threshold, levels)
-        missed = total = 0
-        for lev, f in flagged.items():
-            total += int(f.sum())
-            missed += int((f & ~covered(model, lev)).sum())
-        if total:
-            worst = max(worst, missed / total)
-        refined.append(float(covered(model, 0).mean()))
+            torch.cuda.synchronize()
+            regrid_seconds += time.perf_counter() - start
+        start = time.perf_counter()
+        dt = model.step()
+        if judge is not None:
+            judge.step(dt)
+        torch.cuda.synchronize()
+        step_seconds += time.perf_counter() - start
+        flagged = (judge if judge is not None else model).current_tags(threshold, 1)[0]
+        under = covered(model, 0)
+        if flagged.any():
+            worst = max(worst, float((flagged & ~under).sum()) / float(flagged.sum()))
+        refined.append(float(under.mean()))
         fine_cells.append(sum(int(np.prod(p.shape)) for p in model.hierarchy.patches if p.level > 0))
     return {"miss": worst, "refined": float(np.mean(refined)), "refined_cells": float(np.mean(fine_cells)),
-            "regrids": regrids}
+            "regrids": regrids, "regrid_seconds": regrid_seconds, "step_seconds": step_seconds}
 
 
 def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, threshold=0.05, seed=0,
@@ -298,7 +314,8 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
     run to predict the plain flags of the next K steps, then two refined runs over the next
     ``test_steps`` steps from the same state, one regridded every K steps on the learned
     tags, one on the plain tags of the regrid step (``current_tags``, grown by the
-    clustering's ``buffer`` like the other); the plain tagger judges both after every step.
+    clustering's ``buffer`` like the other); the plain tagger on a uniform run of the same
+    problem advanced in lockstep judges both after every step.
     With ``fallback`` the learned run regrids on the union of the learned tags and the plain
     tags of the regrid step (the plain tagger as the fallback: every cell it flags now is
     refined, the learned tags add the cells it will flag). The interval a tagger reaches is
@@ -323,8 +340,10 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
         for name, tags_of in (("learned", learned), ("plain", lambda m: m.current_tags(threshold, levels))):
             model = multiblast(n, seed=seed)
             model.advance(train_steps)
+            judge = multiblast(n, seed=seed)
+            judge.advance(train_steps)
             runs[name] = amr_run(model, tags_of, interval=K, steps=test_steps, threshold=threshold, levels=levels,
-                                 buffer=buffer, max_patch_size=max_patch_size)
+                                 buffer=buffer, max_patch_size=max_patch_size, judge=judge)
         out["intervals"][K] = runs
     for name in ("learned", "plain"):
         ok = [K for K in intervals if out["intervals"][K][name]["miss"] < 0.01]
