@@ -352,3 +352,31 @@ def test_fused_level_fill_and_overlapped_fluxes_equal_the_plain_sequence(dims):
     torch.cuda.synchronize()
     assert fused.time == plain.time
     assert torch.equal(fused.engine.state, plain.engine.state)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [32, 64, "mixed"])
+def test_staged_fine_fluxes_equal_the_recomputed_register(precision):
+    """2D ideal refined steps with the register's fine faces read from the stage kernels'
+    boundary-face output equal, bit for bit, steps whose register recomputes them."""
+    from wellbalanced_b200.mesh import AMRHierarchy
+    from wellbalanced_b200.mhd import MHD2D
+
+    models = []
+    for staged in (True, False):
+        mesh = AMRHierarchy((32, 32), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, False))
+        mesh.add_patch(1, ((12, 40), (20, 44)))
+        mesh.add_patch(2, ((30, 60), (48, 80)))
+        model = MHD2D(mesh, limiter="mc", precision=precision)
+        model.set_state(lambda x, y: 1.0 + 0.4 * np.exp(-((x - 0.5) ** 2 + (y - 0.55) ** 2) / 0.01),
+                        (0.6, -0.3, 0.1), lambda x, y: 1.0 + 0.3 * np.cos(2 * np.pi * x),
+                        vector_potential=lambda x, y: 0.05 * np.sin(2 * np.pi * x) * np.cos(np.pi * y),
+                        bz=0.1)
+        model.engine.staged_fluxes = staged
+        models.append(model)
+    assert models[0].engine._uses_staged_fluxes() and not models[1].engine._uses_staged_fluxes()
+    for _ in range(6):
+        dts = [m.step() for m in models]
+        assert dts[0] == dts[1]
+    assert torch.equal(models[0].engine.state, models[1].engine.state)
+    assert torch.equal(models[0].engine.register, models[1].engine.register)

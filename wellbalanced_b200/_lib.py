@@ -64,6 +64,8 @@ SIGNATURES = {
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_fill_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_int, c_dp],
     "wb_face_flux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp, c_dp],
+    "wb_face_flux_ops_staged": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp,
+                                c_dp, c_dp],
     "wb_face_flux_ops_physics": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int,
                                  c_double, c_double, c_double, c_dp, c_dp],
     "wb_reflux_apply": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],

@@ -77,10 +77,12 @@ int launch_fill_ops(S* pool, const PatchDesc* patches, const InterpOp* interp, i
                     int ncopies, cudaStream_t stream);
 template <typename S>
 int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops, int nops, cudaStream_t stream);
-// R: the arithmetic of the recomputed face fluxes (the stage kernels' for the state type S)
+// R: the arithmetic of the recomputed face fluxes (the stage kernels' for the state type S);
+// bflux: the stage kernel's boundary-face fluxes (2D ideal: the fine faces read there), or null
 template <typename S, typename R = S>
 int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
-                         double gamma, int limiter, const double* physics, double* reg, cudaStream_t stream);
+                         double gamma, int limiter, const double* physics, const double* bflux, double* reg,
+                         cudaStream_t stream);
 template <typename S>
 int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
                         const double* dt, cudaStream_t stream);

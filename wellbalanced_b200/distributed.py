@@ -484,6 +484,8 @@ class DistributedEngine(Engine):
         self.overlap_fluxes = False  # the flux round's exchange runs on the engine's stream
         # exchange rounds run between the levels' fills and restrictions: no op programs
         self.use_programs = False
+        # the fine faces of an interface may live on another rank: recomputed from proxies
+        self.staged_fluxes = False
         self.rounds = {}
         for key, rd in rank_layout.rounds.items():
             ops = size_ops(rd.pack_ops) if rd.pack_ops.size else rd.pack_ops

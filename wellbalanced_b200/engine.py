@@ -117,7 +117,10 @@ class Engine:
         self.time = torch.zeros(n, dtype=torch.float64, device=self.device)
         self.end = torch.zeros(n, dtype=torch.float64, device=self.device)
         self.bad = torch.zeros(1, dtype=torch.int64, device=self.device)
+        #: the 2D stage kernel's boundary-face fluxes (float64, allocated on first use): the
+        #: register reads the fine faces there instead of recomputing them
         self.bflux = None
+        self.staged_fluxes = True
         self.face_flux_ops = _device_bytes(L.face_flux_ops, self.device, _lib.FACE_FLUX_OP)
         self.nface = int(L.face_flux_ops.size)
         self.reflux_ops = _device_bytes(L.reflux_ops, self.device, _lib.REFLUX_OP)
@@ -216,11 +219,23 @@ class Engine:
                       nops, self._s())
             self.launches += 1
 
+    def _uses_staged_fluxes(self):
+        """Whether the register takes the fine faces from the 2D stage kernel's boundary-face
+        output (ideal 2D refined hierarchies; the non-ideal terms and 3D recompute them)."""
+        return self.staged_fluxes and self.ndim == 2 and self.nface > 0 and self.physics is None
+
+    def _stage_bflux(self):
+        if self.bflux is None:
+            self.bflux = torch.zeros(max(int(self.layout.bflux_size), 1), dtype=torch.float64, device=self.device)
+        return self.bflux
+
     def stage(self, src, base, dst, bflux=None):
         b = self.mean_field
         s = self._s()
         if self.ntiles == 0:
             return
+        if bflux is None and self._uses_staged_fluxes():
+            bflux = self._stage_bflux()
         timing = self.stage_events is not None
         if timing:
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -293,7 +308,8 @@ class Engine:
 
     def face_fluxes(self, pool, stream=None):
         """Register += fine-mean minus coarse fluxes of every coarse-fine interface face
-        (on `stream`, else the engine's stream)."""
+        (on `stream`, else the engine's stream). `pool` is the input of the stage just
+        launched: with staged fluxes its fine faces are read from that stage's output."""
         if self.nface:
             s = stream.cuda_stream if stream is not None else self._s()
             b = self.mean_field
@@ -303,6 +319,11 @@ class Engine:
                 _lib.call("wb_face_flux_ops_physics", self.precision, pool.data_ptr(), self.patches.data_ptr(),
                           self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter, eta,
                           kappa_par, kappa_perp, self.register.data_ptr(), s)
+            elif self._uses_staged_fluxes():
+                # the fine faces as the stage kernel that read `pool` wrote them
+                _lib.call("wb_face_flux_ops_staged", self.precision, pool.data_ptr(), self.patches.data_ptr(),
+                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
+                          self._stage_bflux().data_ptr(), self.register.data_ptr(), s)
             else:
                 _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
                           self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
