@@ -25,6 +25,32 @@ from wellbalanced_b200.regrid import (
 K = 2.0 * np.pi
 
 
+def test_cluster_boxes_cover_every_grown_tag_of_thin_3d_shells():
+    """Thin spherical shells and scattered cells on a periodic 32^3 level (the multi-blast's
+    tag pattern): the boxes cover every tagged cell grown by the buffer, do not overlap,
+    and respect the largest side."""
+    n = 32
+    rng = np.random.default_rng(0)
+    x = (np.arange(n) + 0.5) / n
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    tags = np.zeros((n, n, n), dtype=bool)
+    for _ in range(8):
+        c = rng.uniform(0.15, 0.85, 3)
+        r = rng.uniform(0.1, 0.25)
+        tags |= np.abs(np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r) < 0.03
+    tags |= rng.random(tags.shape) < 0.01
+    boxes = cluster_tags(tags, buffer=1, max_size=8, periodic=(True,) * 3)
+    held = np.zeros(tags.shape, dtype=int)
+    for box in boxes:
+        assert all(1 <= hi - lo <= 8 for lo, hi in box)
+        held[tuple(slice(lo, hi) for lo, hi in box)] += 1
+    assert held.max() == 1
+    grown = tags.copy()
+    for a in range(3):
+        grown = grown | np.roll(grown, 1, axis=a) | np.roll(grown, -1, axis=a)
+    assert np.all(held[grown] == 1)
+
+
 def test_cluster_boxes_cover_the_tags_and_do_not_overlap():
     rng = np.random.default_rng(3)
     tags = np.zeros((32, 24), dtype=bool)
@@ -141,7 +167,8 @@ def _three_regrids(merge):
     start = model.totals()
     for _ in range(3):
         before = model.totals()
-        model, mesh = _regrid_oracle(model, mesh, model.current_tags(0.1, 2), merge=merge, max_patch_size=16)
+        # boxes of at most 12 coarse cells: fine patches meet across the periodic boundaries
+        model, mesh = _regrid_oracle(model, mesh, model.current_tags(0.1, 2), merge=merge, max_patch_size=12)
         after = model.totals()
         for name in before:
             assert abs(after[name] - before[name]) < 1e-14, name

@@ -574,13 +574,27 @@ class Layout:
             same = []
             patches = h.patches_at_level(level)
             n_level = h.level_shape(level)
+            shifts = list(itertools.product(*[(0,) if not h.periodic[a] else (-n_level[a], 0, n_level[a])
+                                              for a in range(self.ndim)]))
+            qlo = np.array([[q.box[a][0] for a in range(self.ndim)] for q in patches], dtype=np.int64)
+            qhi = np.array([[q.box[a][1] for a in range(self.ndim)] for q in patches], dtype=np.int64)
+            offsets = np.array(shifts, dtype=np.int64)
             for p in patches:
+                # the (source, shift) pairs whose points can reach p's haloed box (its cells
+                # and one node more, HALO around): the rest give no op
+                plo = np.array([p.box[a][0] - HALO for a in range(self.ndim)], dtype=np.int64)
+                phi = np.array([p.box[a][1] + HALO + 1 for a in range(self.ndim)], dtype=np.int64)
+                reach = np.all((qlo[None, :, :] + offsets[:, None, :] < phi)
+                               & (qhi[None, :, :] + 1 + offsets[:, None, :] > plo), axis=2)
                 for g in self.groups:
                     slabs = self._halo_slabs(p, g)
-                    for q in patches:
+                    for qi, q in enumerate(patches):
+                        if not reach[:, qi].any():
+                            continue
                         comp_q = self._computed_box(q, g)
-                        shifts = [(0,) if not h.periodic[a] else (-n_level[a], 0, n_level[a]) for a in range(self.ndim)]
-                        for shift in itertools.product(*shifts):
+                        for si, shift in enumerate(shifts):
+                            if not reach[si, qi]:
+                                continue
                             # q's computed points in p's haloed coordinates
                             src = tuple(
                                 (lo + q.box[a][0] + shift[a] - p.box[a][0], hi + q.box[a][0] + shift[a] - p.box[a][0])

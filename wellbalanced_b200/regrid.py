@@ -83,19 +83,26 @@ def _signature_cut(sub, axis):
 
 
 def cluster_tags(tags, *, buffer=1, max_size=None, min_size=4, parents=None, periodic=None, efficiency=0.7):
-    """Boxes ``((lo, hi), ...)`` of the level covering the (grown, nestable) tagged cells.
+    """Disjoint boxes ``((lo, hi), ...)`` of the level covering every grown, nestable tagged
+    cell (the tags grown by ``buffer`` cells, within the parents by the nesting margin).
 
-    ``min_size`` is the smallest box side in cells of the REFINED level (boxes are at
-    least ``ceil(min_size / 2)`` cells of this level).
+    Recursive bisection (Berger-Rigoutsos): a box is kept when it is at most ``max_size``
+    cells a side, its tagged fraction reaches ``efficiency`` and it lies in the nestable
+    region; else it is cut at a hole or an inflection of its tag signature, or halved,
+    down to single cells if need be. Boxes are then grown towards ``min_size`` (the
+    smallest side in cells of the REFINED level: ``ceil(min_size / 2)`` cells of this
+    level) into nestable cells no other box holds, where there is room; coverage of the
+    tags comes first, so a box without room keeps its smaller side.
     """
     tags = np.asarray(tags, dtype=bool)
-    periodic = periodic or (False,) * tags.ndim
+    ndim = tags.ndim
+    periodic = periodic or (False,) * ndim
     parents = parents or [tuple((0, n) for n in tags.shape)]
     grown = _grow(tags, buffer, periodic) if buffer else tags.copy()
     allowed = nesting_mask(tags.shape, parents, periodic, margin=1)
     grown &= allowed
     min_side = max(2, (min_size + 1) // 2)
-    max_side = max_size or max(tags.shape)
+    max_side = max(1, max_size or max(tags.shape))
     boxes = []
 
     def shrink(box):
@@ -103,70 +110,68 @@ def cluster_tags(tags, *, buffer=1, max_size=None, min_size=4, parents=None, per
         if not sub.any():
             return None
         out = []
-        for a in range(tags.ndim):
-            along = sub.any(axis=tuple(b for b in range(tags.ndim) if b != a))
+        for a in range(ndim):
+            along = sub.any(axis=tuple(b for b in range(ndim) if b != a))
             idx = np.flatnonzero(along)
             out.append((box[a][0] + int(idx[0]), box[a][0] + int(idx[-1]) + 1))
         return tuple(out)
 
-    def pad(box):
-        """Grow a box to the minimal side, staying in the domain and the allowed region."""
-        out = list(box)
-        for a, (lo, hi) in enumerate(box):
-            while hi - lo < min_side:
-                if hi < tags.shape[a]:
-                    hi += 1
-                elif lo > 0:
-                    lo -= 1
-                else:
-                    break
-            out[a] = (lo, hi)
-        region = allowed[tuple(slice(lo, hi) for lo, hi in out)]
-        return tuple(out) if region.all() else None
-
-    def split(box, depth=0):
+    def split(box):
         box = shrink(box)
         if box is None:
             return
         sub = grown[tuple(slice(lo, hi) for lo, hi in box)]
         sides = [hi - lo for lo, hi in box]
-        fits = all(s <= max_side for s in sides)
-        region = allowed[tuple(slice(lo, hi) for lo, hi in box)]
-        if fits and sub.mean() >= efficiency and region.all():
-            padded = pad(box)
-            if padded is not None:
-                boxes.append(padded)
-                return
-        if max(sides) <= min_side or depth > 64:
-            padded = pad(box)
-            if padded is not None:
-                boxes.append(padded)
+        fits = all(side <= max_side for side in sides)
+        nestable = allowed[tuple(slice(lo, hi) for lo, hi in box)].all()
+        small = max(sides) <= min_side
+        if fits and nestable and (small or sub.mean() >= efficiency):
+            boxes.append(box)
             return
-        order = sorted(range(tags.ndim), key=lambda a: -sides[a])
+        order = sorted(range(ndim), key=lambda a: -sides[a])
+        axis = cut = None
         for a in order:
             if sides[a] < 2 * min_side:
                 continue
-            cut = _signature_cut(sub, a)
-            if cut is not None and min_side <= cut <= sides[a] - min_side:
+            c = _signature_cut(sub, a)
+            if c is not None and min_side <= c <= sides[a] - min_side:
+                axis, cut = a, c
                 break
-        else:
-            a = order[0]
-            cut = sides[a] // 2
-        lo, hi = box[a]
-        left = tuple((lo, lo + cut) if b == a else box[b] for b in range(tags.ndim))
-        right = tuple((lo + cut, hi) if b == a else box[b] for b in range(tags.ndim))
-        split(left, depth + 1)
-        split(right, depth + 1)
+        if axis is None:
+            axis = order[0]
+            cut = sides[axis] // 2  # >= 1: a box with a side of 1 everywhere is one cell, kept above
+        lo, hi = box[axis]
+        split(tuple((lo, lo + cut) if b == axis else box[b] for b in range(ndim)))
+        split(tuple((lo + cut, hi) if b == axis else box[b] for b in range(ndim)))
 
     split(tuple((0, n) for n in tags.shape))
-    # boxes must not overlap (padding may have grown one into another): trim by dropping
-    # the overlap from the later box along its longest side, or drop it
-    kept = []
+    # grow the boxes towards the smallest side through free, nestable cells
+    held = np.zeros(tags.shape, dtype=bool)
     for box in boxes:
-        if any(_overlap(box, other) for other in kept):
-            continue
-        kept.append(box)
-    return kept
+        held[tuple(slice(lo, hi) for lo, hi in box)] = True
+    out = []
+    for box in boxes:
+        box = list(box)
+        for a in range(ndim):
+            for _ in range(2 * min_side):
+                lo, hi = box[a]
+                if hi - lo >= min_side:
+                    break
+                grew = False
+                for new_lo, new_hi, slab in ((lo, hi + 1, (hi, hi + 1)), (lo - 1, hi, (lo - 1, lo))):
+                    if slab[0] < 0 or slab[1] > tags.shape[a]:
+                        continue
+                    region = tuple(slice(*slab) if b == a else slice(*box[b]) for b in range(ndim))
+                    if held[region].any() or not allowed[region].all():
+                        continue
+                    held[region] = True
+                    box[a] = (new_lo, new_hi)
+                    grew = True
+                    break
+                if not grew:
+                    break
+        out.append(tuple(box))
+    return out
 
 
 def _overlap(a, b):
