@@ -586,15 +586,14 @@ class Layout:
                 phi = np.array([p.box[a][1] + HALO + 1 for a in range(self.ndim)], dtype=np.int64)
                 reach = np.all((qlo[None, :, :] + offsets[:, None, :] < phi)
                                & (qhi[None, :, :] + 1 + offsets[:, None, :] > plo), axis=2)
+                near = [(int(qi), [shifts[si] for si in np.flatnonzero(reach[:, qi])])
+                        for qi in np.flatnonzero(reach.any(axis=0))]
                 for g in self.groups:
                     slabs = self._halo_slabs(p, g)
-                    for qi, q in enumerate(patches):
-                        if not reach[:, qi].any():
-                            continue
+                    for qi, reaching in near:
+                        q = patches[qi]
                         comp_q = self._computed_box(q, g)
-                        for si, shift in enumerate(shifts):
-                            if not reach[si, qi]:
-                                continue
+                        for shift in reaching:
                             # q's computed points in p's haloed coordinates
                             src = tuple(
                                 (lo + q.box[a][0] + shift[a] - p.box[a][0], hi + q.box[a][0] + shift[a] - p.box[a][0])
@@ -707,12 +706,26 @@ class Layout:
         for level in range(1, h.max_level + 1):
             ops = []
             n_coarse = h.level_shape(level - 1)
+            coarses = h.patches_at_level(level - 1)
+            shifts = list(itertools.product(*[(0,) if not h.periodic[a] else (-n_coarse[a], 0, n_coarse[a])
+                                              for a in range(self.ndim)]))
+            clo_all = np.array([[c.box[a][0] for a in range(self.ndim)] for c in coarses], dtype=np.int64)
+            chi_all = np.array([[c.box[a][1] for a in range(self.ndim)] for c in coarses], dtype=np.int64)
+            offsets = np.array(shifts, dtype=np.int64)
             for f in h.patches_at_level(level):
+                # the (coarse patch, shift) pairs whose children (and upper nodes) can reach
+                # f's haloed box: the rest give no op
+                flo = np.array([f.box[a][0] - HALO for a in range(self.ndim)], dtype=np.int64)
+                fhi = np.array([f.box[a][1] + HALO + 1 for a in range(self.ndim)], dtype=np.int64)
+                reach = np.all((2 * (clo_all[None, :, :] + offsets[:, None, :]) < fhi)
+                               & (2 * (chi_all[None, :, :] + offsets[:, None, :] + 1) > flo), axis=2)
+                near = [(int(ci), [shifts[si] for si in np.flatnonzero(reach[:, ci])])
+                        for ci in np.flatnonzero(reach.any(axis=0))]
                 for g in self.groups:
                     slabs = self._halo_slabs(f, g)
-                    for c in h.patches_at_level(level - 1):
-                        shifts = [(0,) if not h.periodic[a] else (-n_coarse[a], 0, n_coarse[a]) for a in range(self.ndim)]
-                        for shift in itertools.product(*shifts):
+                    for ci, reaching in near:
+                        c = coarses[ci]
+                        for shift in reaching:
                             # fine haloed points whose coarse parent lies in c (+ shift)
                             region = []
                             for a in range(self.ndim):
@@ -750,6 +763,20 @@ class Layout:
         levels = {0: {}}
         for level in range(1, h.max_level + 1):
             n_fine = h.level_shape(level)
+            coarses = h.patches_at_level(level - 1)
+            clo_all = np.array([[c.box[a][0] for a in range(self.ndim)] for c in coarses], dtype=np.int64)
+            chi_all = np.array([[c.box[a][1] for a in range(self.ndim)] for c in coarses], dtype=np.int64)
+            # per fine patch, the coarse patches its points (an upper node plane included, on
+            # any periodic image) can restrict into: the rest give no op
+            near = {}
+            for f in h.patches_at_level(level):
+                reach = np.zeros(len(coarses), dtype=bool)
+                for shift in itertools.product(*[(0, -n_fine[a], n_fine[a]) if h.periodic[a] else (0,)
+                                                 for a in range(self.ndim)]):
+                    lo = np.array([(f.box[a][0] + shift[a]) // 2 for a in range(self.ndim)], dtype=np.int64)
+                    hi = np.array([(f.box[a][1] + shift[a]) // 2 + 1 for a in range(self.ndim)], dtype=np.int64)
+                    reach |= np.all((clo_all < hi) & (chi_all + 1 > lo), axis=1)
+                near[f.index] = np.flatnonzero(reach)
             per_group = {}
             for g in self.groups:
                 ops = []
@@ -758,7 +785,8 @@ class Layout:
                         (0, -n_fine[a], n_fine[a]) if h.periodic[a] and (g.node_mask >> a) & 1 else (0,)
                         for a in range(self.ndim)
                     ]
-                    for c in h.patches_at_level(level - 1):
+                    for ci in near[f.index]:
+                        c = coarses[ci]
                         cbox = self._computed_box(c, g)
                         for shift in itertools.product(*shifts):
                             ranges = []
