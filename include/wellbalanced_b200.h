@@ -211,7 +211,8 @@ int wb_face_flux_ops(int precision, const void* pool, const void* patches, const
  * boundary-face fluxes the stage kernel of that stage wrote (wb_stage2d's bflux argument,
  * float64 rows per patch at PatchDesc.bflux: for x then y, side (low, high), conserved row,
  * face along the side); only the coarse faces are recomputed. The fluxes read are those the
- * fine cells were advanced with, so the register equals wb_face_flux_ops' bit for bit.
+ * fine cells were advanced with: with float32 face arithmetic the register equals
+ * wb_face_flux_ops' bit for bit, in float64 to rounding.
  * No counterpart in the reference (whose register records the fluxes as its sweeps form
  * them). 3D ops and non-ideal terms are not read from bflux: use wb_face_flux_ops(_physics). */
 int wb_face_flux_ops_staged(int precision, const void* pool, const void* patches, const void* ops, int nops,
