@@ -210,14 +210,16 @@ int wb_face_flux_ops(int precision, const void* pool, const void* patches, const
 /* The same register update for 2D ideal MHD with the fine faces read from `bflux`, the
  * boundary-face fluxes the stage kernel of that stage wrote (wb_stage2d's bflux argument,
  * float64 rows per patch at PatchDesc.bflux: for x then y, side (low, high), conserved row,
- * face along the side); only the coarse faces are recomputed. The fluxes read are those the
+ * face along the side); only the coarse faces are recomputed, one thread per coarse face of
+ * all ops: each op's FaceFluxOp.first holds its first face in that flat numbering (the
+ * prefix sum of the ops' lengths, in list order) and nfaces their total. The fluxes read are those the
  * fine cells were advanced with: with float32 face arithmetic the register equals
  * wb_face_flux_ops' bit for bit, in float64 to rounding.
  * No counterpart in the reference (whose register records the fluxes as its sweeps form
  * them). 3D ops and non-ideal terms are not read from bflux: use wb_face_flux_ops(_physics). */
 int wb_face_flux_ops_staged(int precision, const void* pool, const void* patches, const void* ops, int nops,
-                            double b0x, double b0y, double b0z, double gamma, int limiter, const double* bflux,
-                            double* reg, void* stream);
+                            int nfaces, double b0x, double b0y, double b0z, double gamma, int limiter,
+                            const double* bflux, double* reg, void* stream);
 /* The same register update with the non-ideal face terms of wb_stage2d_physics /
  * wb_stage3d_physics: each recomputed face flux carries the resistive terms (and, in 2D,
  * the Braginskii heat flux), as the reference's fluxes do when its register records them

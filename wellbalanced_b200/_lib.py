@@ -64,8 +64,8 @@ SIGNATURES = {
     "wb_restrict_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp],
     "wb_fill_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_int, c_dp],
     "wb_face_flux_ops": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp, c_dp],
-    "wb_face_flux_ops_staged": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int, c_dp,
-                                c_dp, c_dp],
+    "wb_face_flux_ops_staged": [c_int, c_dp, c_dp, c_dp, c_int, c_int, c_double, c_double, c_double, c_double, c_int,
+                                c_dp, c_dp, c_dp],
     "wb_face_flux_ops_physics": [c_int, c_dp, c_dp, c_dp, c_int, c_double, c_double, c_double, c_double, c_int,
                                  c_double, c_double, c_double, c_dp, c_dp],
     "wb_reflux_apply": [c_int, c_dp, c_dp, c_dp, c_int, c_dp, c_dp, c_dp],
@@ -210,7 +210,7 @@ RESTRICT_OP = np.dtype(
 FACE_FLUX_OP = np.dtype(
     {
         "names": ["coarse", "fine", "ndim", "axis", "t1", "t2", "coarse_plane", "fine_plane", "coarse_t0", "fine_t0",
-                  "len", "width", "pad0", "pad1", "reg_off"],
+                  "len", "width", "first", "pad1", "reg_off"],
         "formats": ["<i4"] * 8 + [("<i4", 2)] * 2 + ["<i4"] * 4 + ["<i8"],
         "offsets": [0, 4, 8, 12, 16, 20, 24, 28, 32, 40, 48, 52, 56, 60, 64],
         "itemsize": 72,

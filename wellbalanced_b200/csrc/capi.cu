@@ -456,8 +456,8 @@ int wb_restrict_ops(int precision, void* pool, const void* patches, const void* 
 }
 
 static int face_flux_ops(int precision, const void* pool, const void* patches, const void* ops, int nops,
-                         const double* b0, double gamma, int limiter, const double* physics, const double* bflux,
-                         double* reg, void* stream) {
+                         int nfaces, const double* b0, double gamma, int limiter, const double* physics,
+                         const double* bflux, double* reg, void* stream) {
   if (!precision_ok(precision, "face_flux_ops") || (nops > 0 && !ptrs_ok({pool, patches, ops, reg}, "face_flux_ops")))
     return kBadArgument;
   if (limiter < 0 || limiter > 3) {
@@ -466,14 +466,14 @@ static int face_flux_ops(int precision, const void* pool, const void* patches, c
   }
   if (precision == 32)
     return launch_face_flux_ops<float>(static_cast<const float*>(pool), static_cast<const PatchDesc*>(patches),
-                                       static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, bflux,
+                                       static_cast<const FaceFluxOp*>(ops), nops, nfaces, b0, gamma, limiter, physics, bflux,
                                        reg, as_stream(stream));
   if (precision == kMath32State64)
     return launch_face_flux_ops<double, float>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
-                                               static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics,
-                                               bflux, reg, as_stream(stream));
+                                               static_cast<const FaceFluxOp*>(ops), nops, nfaces, b0, gamma, limiter,
+                                               physics, bflux, reg, as_stream(stream));
   return launch_face_flux_ops<double>(static_cast<const double*>(pool), static_cast<const PatchDesc*>(patches),
-                                      static_cast<const FaceFluxOp*>(ops), nops, b0, gamma, limiter, physics, bflux,
+                                      static_cast<const FaceFluxOp*>(ops), nops, nfaces, b0, gamma, limiter, physics, bflux,
                                       reg, as_stream(stream));
 }
 
@@ -481,19 +481,19 @@ int wb_face_flux_ops(int precision, const void* pool, const void* patches, const
                      double b0y, double b0z, double gamma, int limiter, double* reg, void* stream) {
   set_error("");
   const double b0[3] = {b0x, b0y, b0z};
-  return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, nullptr, nullptr, reg, stream);
+  return face_flux_ops(precision, pool, patches, ops, nops, 0, b0, gamma, limiter, nullptr, nullptr, reg, stream);
 }
 
 int wb_face_flux_ops_staged(int precision, const void* pool, const void* patches, const void* ops, int nops,
-                            double b0x, double b0y, double b0z, double gamma, int limiter, const double* bflux,
-                            double* reg, void* stream) {
+                            int nfaces, double b0x, double b0y, double b0z, double gamma, int limiter,
+                            const double* bflux, double* reg, void* stream) {
   set_error("");
-  if (nops > 0 && !bflux) {
-    set_error("face_flux_ops_staged: NULL boundary-face fluxes");
+  if (nops > 0 && (!bflux || nfaces < 0)) {
+    set_error("face_flux_ops_staged: NULL boundary-face fluxes or a negative face count");
     return kBadArgument;
   }
   const double b0[3] = {b0x, b0y, b0z};
-  return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, nullptr, bflux, reg, stream);
+  return face_flux_ops(precision, pool, patches, ops, nops, nfaces, b0, gamma, limiter, nullptr, bflux, reg, stream);
 }
 
 int wb_face_flux_ops_physics(int precision, const void* pool, const void* patches, const void* ops, int nops,
@@ -507,7 +507,7 @@ int wb_face_flux_ops_physics(int precision, const void* pool, const void* patche
   }
   const double b0[3] = {b0x, b0y, b0z};
   const double physics[3] = {eta, kappa_par, kappa_perp};
-  return face_flux_ops(precision, pool, patches, ops, nops, b0, gamma, limiter, physics, nullptr, reg, stream);
+  return face_flux_ops(precision, pool, patches, ops, nops, 0, b0, gamma, limiter, physics, nullptr, reg, stream);
 }
 
 int wb_reflux_apply(int precision, void* pool, const void* patches, const void* ops, int nops, double* reg,

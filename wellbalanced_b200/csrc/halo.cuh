@@ -53,7 +53,8 @@ struct FaceFluxOp {
   int32_t coarse_plane, fine_plane;
   int32_t coarse_t0[2], fine_t0[2];
   int32_t len, width;
-  int32_t pad0, pad1;
+  int32_t first;  // the op's first coarse face in the flat numbering of all ops' faces
+  int32_t pad1;
   int64_t reg_off;
 };
 
@@ -80,9 +81,9 @@ int launch_restrict_ops(S* pool, const PatchDesc* patches, const RestrictOp* ops
 // R: the arithmetic of the recomputed face fluxes (the stage kernels' for the state type S);
 // bflux: the stage kernel's boundary-face fluxes (2D ideal: the fine faces read there), or null
 template <typename S, typename R = S>
-int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
-                         double gamma, int limiter, const double* physics, const double* bflux, double* reg,
-                         cudaStream_t stream);
+int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, int nfaces,
+                         const double* b0, double gamma, int limiter, const double* physics, const double* bflux,
+                         double* reg, cudaStream_t stream);
 template <typename S>
 int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, int nops, double* reg,
                         const double* dt, cudaStream_t stream);

@@ -285,9 +285,7 @@ __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __
                                                                      const PatchDesc* __restrict__ patches,
                                                                      const FaceFluxOp* __restrict__ ops, int nops,
                                                                      double b0x, double b0y, double b0z, double gamma,
-                                                                     FacePhysics phys,
-                                                                     const double* __restrict__ bflux,
-                                                                     double* __restrict__ reg) {
+                                                                     FacePhysics phys, double* __restrict__ reg) {
   __shared__ double g_all[kFluxWarps][32][6];
   const int warp = threadIdx.x / 32, t = threadIdx.x % 32;
   const int index = blockIdx.x * kFluxWarps + warp;
@@ -297,31 +295,6 @@ __global__ void __launch_bounds__(kFluxThreads) face_flux_ops_kernel(const S* __
   const PatchDesc C = patches[op.coarse];
   const PatchDesc F = patches[op.fine];
   const double b0[3] = {b0x, b0y, b0z};
-  if (bflux && op.ndim == 2 && !PHYS) {
-    // the fine faces' fluxes as the fine patch's stage kernel formed them (its boundary-face
-    // output, float64 rows (side, conserved row, face along the side)); the coarse face
-    // recomputed; one coarse face per lane, the same sums as below
-    const int along = op.axis == 0 ? F.n[1] : F.n[0];
-    const int side = op.fine_plane == kHalo ? 0 : 1;
-    const double* rows = bflux + F.bflux + (op.axis == 0 ? 0 : 2 * 6 * F.n[1]);
-    for (int s = t; s < op.len; s += 32) {
-      int idx[3] = {0, 0, 0};
-      idx[op.axis] = op.coarse_plane;
-      idx[op.t1] = op.coarse_t0[0] + s;
-      double coarse[6] = {0, 0, 0, 0, 0, 0};
-      face_flux<S, R, LIM, PHYS>(pool + C.off, C, 2, op.axis, idx[0], idx[1], idx[2], b0, gamma, phys, coarse);
-      const int f0 = op.fine_t0[0] + 2 * s - kHalo;
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        const double* row = rows + (side * 6 + q) * along;
-        double fine = 0.0;
-        fine += row[f0];
-        fine += row[f0 + 1];
-        reg[op.reg_off + int64_t(q) * op.len + s] += fine / 2.0 - coarse[q];
-      }
-    }
-    return;
-  }
   const int ncons = op.ndim == 2 ? 6 : 5;
   const int fine_b = op.ndim == 3 ? 2 : 1;
   const int K = 1 + 2 * fine_b;  // evaluations per coarse face
@@ -370,33 +343,96 @@ __global__ void reflux_apply_kernel(S* __restrict__ pool, const PatchDesc* __res
   reflux_op<S, 128>(pool, patches, ops[blockIdx.x], reg, dt);
 }
 
+// 2D ideal MHD with the fine faces' fluxes as the fine patches' stage kernel formed them
+// (its boundary-face output `bflux`: float64 rows (side, conserved row, face along the side)
+// at each patch's PatchDesc.bflux, x-faces then y-faces): one thread per coarse face of all
+// ops (op.first: the op's first face in that flat numbering), which recomputes the coarse
+// face and sums the two fine faces in the order of face_flux_ops_kernel, so the register
+// gets the same values as there.
+constexpr int kStagedThreads = 128;
+
+template <typename S, typename R, int LIM>
+__global__ void __launch_bounds__(kStagedThreads) face_flux_staged_kernel(
+    const S* __restrict__ pool, const PatchDesc* __restrict__ patches, const FaceFluxOp* __restrict__ ops, int nops,
+    int nfaces, double b0x, double b0y, double b0z, double gamma, const double* __restrict__ bflux,
+    double* __restrict__ reg) {
+  const int face = blockIdx.x * kStagedThreads + threadIdx.x;
+  if (face >= nfaces) return;
+  // the op holding this face: the last one whose first face is not after it
+  int lo = 0, hi = nops - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ops[mid].first <= face) lo = mid; else hi = mid - 1;
+  }
+  const FaceFluxOp op = ops[lo];
+  const int s = face - op.first;
+  if (s < 0 || s >= op.len || op.ndim != 2) return;
+  const PatchDesc C = patches[op.coarse];
+  const PatchDesc F = patches[op.fine];
+  const double b0[3] = {b0x, b0y, b0z};
+  int idx[3] = {0, 0, 0};
+  idx[op.axis] = op.coarse_plane;
+  idx[op.t1] = op.coarse_t0[0] + s;
+  double coarse[6] = {0, 0, 0, 0, 0, 0};
+  face_flux<S, R, LIM, false>(pool + C.off, C, 2, op.axis, idx[0], idx[1], idx[2], b0, gamma,
+                              FacePhysics{0.0, 0.0, 0.0}, coarse);
+  const int along = op.axis == 0 ? F.n[1] : F.n[0];
+  const int side = op.fine_plane == kHalo ? 0 : 1;
+  const double* rows = bflux + F.bflux + (op.axis == 0 ? 0 : 2 * 6 * F.n[1]);
+  const int f0 = op.fine_t0[0] + 2 * s - kHalo;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const double* row = rows + (side * 6 + q) * along;
+    double fine = 0.0;
+    fine += row[f0];
+    fine += row[f0 + 1];
+    reg[op.reg_off + int64_t(q) * op.len + s] += fine / 2.0 - coarse[q];
+  }
+}
+
+template <typename S, typename R>
+void launch_face_flux_staged(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, int nfaces,
+                             const double* b0, double gamma, int limiter, const double* bflux, double* reg,
+                             cudaStream_t stream) {
+  const int grid = (nfaces + kStagedThreads - 1) / kStagedThreads;
+  switch (limiter) {
+    case 0: face_flux_staged_kernel<S, R, 0><<<grid, kStagedThreads, 0, stream>>>(pool, patches, ops, nops, nfaces, b0[0], b0[1], b0[2], gamma, bflux, reg); break;
+    case 1: face_flux_staged_kernel<S, R, 1><<<grid, kStagedThreads, 0, stream>>>(pool, patches, ops, nops, nfaces, b0[0], b0[1], b0[2], gamma, bflux, reg); break;
+    case 2: face_flux_staged_kernel<S, R, 2><<<grid, kStagedThreads, 0, stream>>>(pool, patches, ops, nops, nfaces, b0[0], b0[1], b0[2], gamma, bflux, reg); break;
+    default: face_flux_staged_kernel<S, R, 3><<<grid, kStagedThreads, 0, stream>>>(pool, patches, ops, nops, nfaces, b0[0], b0[1], b0[2], gamma, bflux, reg); break;
+  }
+}
+
 template <typename S, typename R, bool PHYS>
 void launch_face_flux_kernel(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops,
-                             const double* b0, double gamma, int limiter, const FacePhysics& phys,
-                             const double* bflux, double* reg, cudaStream_t stream) {
+                             const double* b0, double gamma, int limiter, const FacePhysics& phys, double* reg,
+                             cudaStream_t stream) {
   switch (limiter) {
-    case 0: face_flux_ops_kernel<S, R, 0, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, bflux, reg); break;
-    case 1: face_flux_ops_kernel<S, R, 1, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, bflux, reg); break;
-    case 2: face_flux_ops_kernel<S, R, 2, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, bflux, reg); break;
-    default: face_flux_ops_kernel<S, R, 3, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, bflux, reg); break;
+    case 0: face_flux_ops_kernel<S, R, 0, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 1: face_flux_ops_kernel<S, R, 1, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    case 2: face_flux_ops_kernel<S, R, 2, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
+    default: face_flux_ops_kernel<S, R, 3, PHYS><<<(nops + kFluxWarps - 1) / kFluxWarps, kFluxThreads, 0, stream>>>(pool, patches, ops, nops, b0[0], b0[1], b0[2], gamma, phys, reg); break;
   }
 }
 
 // physics: null for ideal MHD, else {eta, kappa_par, kappa_perp} (3D interfaces take eta only).
 // R: the arithmetic of the recomputed faces (the stage kernels' R for the state's type S).
 // bflux: the stage kernel's boundary-face fluxes of the patches (2D ideal MHD: the fine
-// faces are read there instead of recomputed), or null.
+// faces are read there instead of recomputed, one thread per coarse face of the `nfaces`
+// the ops hold), or null.
 template <typename S, typename R>
-int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, const double* b0,
-                         double gamma, int limiter, const double* physics, const double* bflux, double* reg,
-                         cudaStream_t stream) {
+int launch_face_flux_ops(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, int nfaces,
+                         const double* b0, double gamma, int limiter, const double* physics, const double* bflux,
+                         double* reg, cudaStream_t stream) {
   if (nops <= 0) return kOk;
-  if (physics && (physics[0] != 0.0 || physics[1] != 0.0 || physics[2] != 0.0))
+  if (bflux)
+    launch_face_flux_staged<S, R>(pool, patches, ops, nops, nfaces, b0, gamma, limiter, bflux, reg, stream);
+  else if (physics && (physics[0] != 0.0 || physics[1] != 0.0 || physics[2] != 0.0))
     launch_face_flux_kernel<S, R, true>(pool, patches, ops, nops, b0, gamma, limiter,
-                                        FacePhysics{physics[0], physics[1], physics[2]}, nullptr, reg, stream);
+                                        FacePhysics{physics[0], physics[1], physics[2]}, reg, stream);
   else
     launch_face_flux_kernel<S, R, false>(pool, patches, ops, nops, b0, gamma, limiter, FacePhysics{0.0, 0.0, 0.0},
-                                         bflux, reg, stream);
+                                         reg, stream);
   return check_launch("face flux ops");
 }
 
@@ -407,13 +443,13 @@ int launch_reflux_apply(S* pool, const PatchDesc* patches, const RefluxOp* ops, 
   return check_launch("reflux");
 }
 
-template int launch_face_flux_ops<float, float>(const float*, const PatchDesc*, const FaceFluxOp*, int,
+template int launch_face_flux_ops<float, float>(const float*, const PatchDesc*, const FaceFluxOp*, int, int,
                                                 const double*, double, int, const double*, const double*, double*,
                                                 cudaStream_t);
-template int launch_face_flux_ops<double, double>(const double*, const PatchDesc*, const FaceFluxOp*, int,
+template int launch_face_flux_ops<double, double>(const double*, const PatchDesc*, const FaceFluxOp*, int, int,
                                                   const double*, double, int, const double*, const double*, double*,
                                                   cudaStream_t);
-template int launch_face_flux_ops<double, float>(const double*, const PatchDesc*, const FaceFluxOp*, int,
+template int launch_face_flux_ops<double, float>(const double*, const PatchDesc*, const FaceFluxOp*, int, int,
                                                  const double*, double, int, const double*, const double*, double*,
                                                  cudaStream_t);
 template int launch_reflux_apply<float>(float*, const PatchDesc*, const RefluxOp*, int, double*, const double*,

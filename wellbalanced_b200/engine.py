@@ -121,7 +121,13 @@ class Engine:
         #: register reads the fine faces there instead of recomputing them
         self.bflux = None
         self.staged_fluxes = True
-        self.face_flux_ops = _device_bytes(L.face_flux_ops, self.device, _lib.FACE_FLUX_OP)
+        face_ops = L.face_flux_ops.copy()
+        if face_ops.size:
+            # each op's first coarse face in the flat numbering of all ops' faces (the staged
+            # register kernel's thread index)
+            face_ops["first"] = np.concatenate([[0], np.cumsum(face_ops["len"])[:-1]]).astype(np.int32)
+        self.nface_faces = int(face_ops["len"].sum()) if face_ops.size else 0
+        self.face_flux_ops = _device_bytes(face_ops, self.device, _lib.FACE_FLUX_OP)
         self.nface = int(L.face_flux_ops.size)
         self.reflux_ops = _device_bytes(L.reflux_ops, self.device, _lib.REFLUX_OP)
         self.nreflux = int(L.reflux_ops.size)
@@ -322,8 +328,8 @@ class Engine:
             elif self._uses_staged_fluxes():
                 # the fine faces as the stage kernel that read `pool` wrote them
                 _lib.call("wb_face_flux_ops_staged", self.precision, pool.data_ptr(), self.patches.data_ptr(),
-                          self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
-                          self._stage_bflux().data_ptr(), self.register.data_ptr(), s)
+                          self.face_flux_ops.data_ptr(), self.nface, self.nface_faces, b[0], b[1], b[2], self.gamma,
+                          self.limiter, self._stage_bflux().data_ptr(), self.register.data_ptr(), s)
             else:
                 _lib.call("wb_face_flux_ops", self.precision, pool.data_ptr(), self.patches.data_ptr(),
                           self.face_flux_ops.data_ptr(), self.nface, b[0], b[1], b[2], self.gamma, self.limiter,
