@@ -216,12 +216,17 @@ def split_box_ops(ops, chunk=OP_MAX_POINTS):
     if ops.size == 0:
         return ops
     dtype = ops.dtype
+    big = np.flatnonzero(np.prod(ops["n"].astype(np.int64), axis=1) > chunk)
+    if big.size == 0:
+        return ops
     out = []
-    for o in ops:
+    last = 0
+    for b in big:
+        if b > last:
+            out.append(ops[last:b])  # the ops that fit, unchanged and in order
+        last = b + 1
+        o = ops[b]
         n = [int(v) for v in o["n"]]
-        if n[0] * n[1] * n[2] <= chunk:
-            out.append(np.atleast_1d(o))
-            continue
         parts = _box_parts(n, chunk)
         block = np.repeat(np.atleast_1d(o), len(parts))
         starts = np.array([st for st, _ in parts], dtype=np.int64)
@@ -236,6 +241,8 @@ def split_box_ops(ops, chunk=OP_MAX_POINTS):
             block["c"] += starts.astype(np.int32)
             block["f"] += (2 * starts).astype(np.int32)
         out.append(block)
+    if last < ops.size:
+        out.append(ops[last:])
     return np.concatenate(out).astype(dtype)
 
 
@@ -296,22 +303,35 @@ def trim_interp_ops(interp, same):
     same = np.atleast_1d(np.asarray(same))
     if interp.size == 0 or same.size == 0:
         return interp
-    covers = {}
-    for op in same:
-        key = (int(op["dst"]), int(op["field_lo"]), int(op["field_hi"]))
-        covers.setdefault(key, []).append((op["d"].astype(np.int64), op["n"].astype(np.int64)))
+    # the copy boxes per (patch, field range), as arrays
+    sd = same["d"].astype(np.int64)
+    sn = same["n"].astype(np.int64)
+    skeys = list(zip(same["dst"].tolist(), same["field_lo"].tolist(), same["field_hi"].tolist(), strict=True))
+    groups = {}
+    for i, key in enumerate(skeys):
+        groups.setdefault(key, []).append(i)
+    covers = {key: (sd[idx], sn[idx]) for key, idx in ((k, np.array(v)) for k, v in groups.items())}
+    idd = interp["d"].astype(np.int64)
+    inn = interp["n"].astype(np.int64)
+    ikeys = zip(interp["fine"].tolist(), interp["field_lo"].tolist(), interp["field_hi"].tolist(), strict=True)
     out = []
-    for op in interp:
-        boxes = covers.get((int(op["fine"]), int(op["field_lo"]), int(op["field_hi"])))
-        if not boxes:
+    for i, key in enumerate(ikeys):
+        op = interp[i]
+        boxes = covers.get(key)
+        if boxes is None:
             out.append(np.atleast_1d(op))
             continue
-        d, n = op["d"].astype(np.int64), op["n"].astype(np.int64)
+        d, n = idd[i], inn[i]
+        lo = np.maximum(d, boxes[0])
+        hi = np.minimum(d + n, boxes[0] + boxes[1])
+        meet = np.flatnonzero(np.all(lo < hi, axis=1))
+        if meet.size == 0:
+            out.append(np.atleast_1d(op))
+            continue
         free = np.ones(tuple(int(v) for v in n), dtype=bool)
-        for cd, cn in boxes:
-            lo, hi = np.maximum(d, cd), np.minimum(d + n, cd + cn)
-            if np.all(lo < hi):
-                free[lo[0] - d[0]:hi[0] - d[0], lo[1] - d[1]:hi[1] - d[1], lo[2] - d[2]:hi[2] - d[2]] = False
+        for j in meet:
+            a, b = lo[j] - d, hi[j] - d
+            free[a[0]:b[0], a[1]:b[1], a[2]:b[2]] = False
         if free.all():
             out.append(np.atleast_1d(op))
             continue
@@ -1042,15 +1062,13 @@ class Layout:
         `chunk` points (default `OP_MAX_POINTS`; the engine cuts small lists further)."""
         if not ops:
             return np.zeros(0, dtype)
-        for o in ops:
-            if dtype in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
-                rec = np.asarray(o).reshape(())
-                points = int(np.prod([int(v) for v in rec["n"]]))
-                if points >= 2**31:  # the op kernels index an op's points in 32 bits
-                    raise ValueError(f"an op of {points} points; the kernels take below 2**31")
-                if not 0 <= int(rec["field_lo"]) <= int(rec["field_hi"]) <= 8:  # the copy kernel holds 8 fields
-                    raise ValueError("op fields outside 0..7")
         packed = np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
         if dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
             return packed
+        points = np.prod(packed["n"].astype(np.int64), axis=1)
+        if np.any(points >= 2**31):  # the op kernels index an op's points in 32 bits
+            raise ValueError(f"an op of {int(points.max())} points; the kernels take below 2**31")
+        lo, hi = packed["field_lo"], packed["field_hi"]
+        if np.any((lo < 0) | (lo > hi) | (hi > 8)):  # the copy kernel holds 8 fields
+            raise ValueError("op fields outside 0..7")
         return split_box_ops(packed, chunk)
