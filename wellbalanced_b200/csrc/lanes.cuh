@@ -1,15 +1,15 @@
 // Lane types of the float32 face arithmetic.
 //
-// `F2` holds two independent float32 lanes (two faces evaluated together) and advances
-// them with the packed float32 instructions of sm_100 (add / sub / mul / fma on .f32x2:
-// one instruction for both lanes). Comparisons give a lane mask `M2`; selects, min / max,
-// absolute values and the special functions act on each lane.
+// `F2` holds two independent float32 lanes (the left and right states of a face, or two
+// components) and advances them with the packed float32 instructions of sm_100 (add /
+// sub / mul / fma on .f32x2: one instruction for both lanes). Comparisons give a lane
+// mask `M2`; selects, min / max, absolute values and the special functions act on each
+// lane.
 //
 // `L1` is one float32 lane with the same rounding: every add, subtract and multiply is
 // rounded on its own (no implicit contraction into FMA) and every fused multiply-add is
-// written as `fma`. A face evaluated in one lane of F2 and the same face evaluated in L1
-// therefore carry the same bits, so the stage kernels (which pair faces) and the
-// refluxing kernel (which evaluates single faces) agree exactly on the flux of a face.
+// written as `fma`, so a value has the same bits in a lane of F2 and in L1, and the
+// kernels that form the same face (the stage kernels, the refluxing kernel) agree on it.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -39,16 +39,6 @@ __device__ __forceinline__ L1 lcopysign(L1 m, L1 s) { return L1(copysignf(m.v, s
 __device__ __forceinline__ L1 linv(L1 a) { return L1(__fdividef(1.0f, a.v)); }
 __device__ __forceinline__ L1 lrsqrt(L1 a) { return L1(rsqrtf(a.v)); }
 __device__ __forceinline__ bool any(bool m) { return m; }
-__device__ __forceinline__ bool lane_mask(bool m, int) { return m; }
-__device__ __forceinline__ float lane(L1 a, int) { return a.v; }
-__device__ __forceinline__ void set_lane(L1& a, int, float x) { a.v = x; }
-template <typename V>
-struct Lanes;
-template <>
-struct Lanes<L1> {
-  static constexpr int kCount = 1;
-  using Mask = bool;
-};
 
 struct M2 {
   bool x, y;
@@ -58,7 +48,6 @@ __device__ __forceinline__ M2 operator&(M2 a, M2 b) { return {a.x && b.x, a.y &&
 __device__ __forceinline__ M2 operator^(M2 a, M2 b) { return {a.x != b.x, a.y != b.y}; }
 __device__ __forceinline__ M2 operator!(M2 a) { return {!a.x, !a.y}; }
 __device__ __forceinline__ bool any(M2 m) { return m.x || m.y; }
-__device__ __forceinline__ bool lane_mask(M2 m, int i) { return i == 0 ? m.x : m.y; }
 
 struct F2 {
   float2 v;
@@ -97,19 +86,6 @@ __device__ __forceinline__ F2 lmax(F2 a, F2 b) { return F2(fmaxf(a.v.x, b.v.x), 
 __device__ __forceinline__ F2 lcopysign(F2 m, F2 s) { return F2(copysignf(m.v.x, s.v.x), copysignf(m.v.y, s.v.y)); }
 __device__ __forceinline__ F2 linv(F2 a) { return F2(__fdividef(1.0f, a.v.x), __fdividef(1.0f, a.v.y)); }
 __device__ __forceinline__ F2 lrsqrt(F2 a) { return F2(rsqrtf(a.v.x), rsqrtf(a.v.y)); }
-__device__ __forceinline__ float lane(F2 a, int i) { return i == 0 ? a.v.x : a.v.y; }
-__device__ __forceinline__ void set_lane(F2& a, int i, float x) {
-  if (i == 0)
-    a.v.x = x;
-  else
-    a.v.y = x;
-}
-template <>
-struct Lanes<F2> {
-  static constexpr int kCount = 2;
-  using Mask = M2;
-};
-
 // 0 - a (a negation for the packed type, kept identical in both lane types)
 template <typename V>
 __device__ __forceinline__ V lneg(V a) {

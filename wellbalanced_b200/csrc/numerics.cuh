@@ -214,7 +214,7 @@ __device__ __forceinline__ void hlld_front_checked(const R (&L)[7], const R (&Rt
 }
 
 // HLLD flux through a face between normal-frame states L and Rt with normal field bn
-// (float64; the float32 faces take hlld_flux_l of numerics_lanes.cuh). Straight-line code: the star / double-star flux of the side of the contact the face
+// (float64; the float32 faces take the lane code of numerics_lanes.cuh). Straight-line code: the star / double-star flux of the side of the contact the face
 // lies on is always formed and the supersonic and star-only cases are selected at the
 // end (no divergent branches). Where a face is supersonic (S_L >= 0 or S_R < 0) the
 // contact lies on the same side as the upwind state, so one side state serves both.

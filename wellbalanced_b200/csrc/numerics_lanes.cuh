@@ -246,7 +246,7 @@ __device__ __forceinline__ void hlld_flux(const float (&L)[7], const float (&Rt)
 // One face's reconstruction with its left and right states in the two lanes of F2: the
 // two limited slopes of each component in one packed evaluation (lane x: the cell below the
 // face, lane y: the cell above), the states as one packed FMA. Lane by lane the same
-// operations as reconstruct_l<L1>.
+// operations as the one-lane form.
 template <int LIM>
 __device__ __forceinline__ void reconstruct(const float (&q0)[7], const float (&q1)[7], const float (&q2)[7],
                                             const float (&q3)[7], float (&L)[7], float (&Rt)[7]) {
