@@ -623,18 +623,13 @@ class Layout:
                                 box = _boxes_intersect(slab, src)
                                 if box is None:
                                     continue
-                                op = np.zeros((), dtype=_lib.COPY_OP)
-                                op["dst"], op["src1"], op["src2"] = p.index, q.index, -1
-                                op["field_lo"], op["field_hi"], op["negate"] = g.lo, g.hi, -1
                                 n = [hi - lo for lo, hi in box] + [1] * (3 - self.ndim)
                                 d = [lo for lo, _ in box] + [0] * (3 - self.ndim)
                                 s1 = [lo - q.box[a][0] - shift[a] + p.box[a][0] for a, (lo, _) in enumerate(box)]
                                 s1 += [0] * (3 - self.ndim)
-                                op["n"], op["d"], op["s1"] = n, d, s1
-                                op["m1"] = [1, 1, 1]
-                                op["s2"], op["m2"] = [0, 0, 0], [0, 0, 0]
-                                op["w1"], op["w2"] = 1.0, 0.0
-                                same.append(op)
+                                # a COPY_OP record, fields in order
+                                same.append((p.index, q.index, -1, g.lo, g.hi, -1, n, d, s1, (1, 1, 1), (0, 0, 0),
+                                             (0, 0, 0), 1.0, 0.0))
             boundary = [[] for _ in range(self.ndim)]
             for p in patches:
                 for a in range(self.ndim):
@@ -759,15 +754,12 @@ class Layout:
                                 box = _boxes_intersect(slab, tuple(region))
                                 if box is None:
                                     continue
-                                op = np.zeros((), dtype=_lib.INTERP_OP)
-                                op["fine"], op["coarse"] = f.index, c.index
-                                op["field_lo"], op["field_hi"] = g.lo, g.hi
-                                op["node_mask"], op["ndim"] = g.node_mask, self.ndim
-                                op["n"] = [hi - lo for lo, hi in box] + [1] * (3 - self.ndim)
-                                op["d"] = [lo for lo, _ in box] + [0] * (3 - self.ndim)
-                                op["fine_lo"] = [f.box[a][0] for a in range(self.ndim)] + [0] * (3 - self.ndim)
-                                op["coarse_lo"] = [c.box[a][0] + shift[a] for a in range(self.ndim)] + [0] * (3 - self.ndim)
-                                ops.append(op)
+                                # an INTERP_OP record, fields in order
+                                ops.append((f.index, c.index, g.lo, g.hi, g.node_mask, self.ndim,
+                                            [hi - lo for lo, hi in box] + [1] * (3 - self.ndim),
+                                            [lo for lo, _ in box] + [0] * (3 - self.ndim),
+                                            [f.box[a][0] for a in range(self.ndim)] + [0] * (3 - self.ndim),
+                                            [c.box[a][0] + shift[a] for a in range(self.ndim)] + [0] * (3 - self.ndim)))
             levels.append(self._pack(ops, _lib.INTERP_OP))
         return levels
 
@@ -1062,7 +1054,10 @@ class Layout:
         `chunk` points (default `OP_MAX_POINTS`; the engine cuts small lists further)."""
         if not ops:
             return np.zeros(0, dtype)
-        packed = np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
+        if isinstance(ops[0], tuple):  # records given as tuples of their fields, in order
+            packed = np.array(ops, dtype=dtype)
+        else:
+            packed = np.array([np.asarray(o).reshape(()) for o in ops], dtype=dtype)
         if dtype not in (_lib.COPY_OP, _lib.INTERP_OP, _lib.RESTRICT_OP):
             return packed
         points = np.prod(packed["n"].astype(np.int64), axis=1)
