@@ -502,6 +502,28 @@ class Harris:
         out["default"] = "op_programs" if default else "separate_launches"
         return out
 
+    def regrid_timing(self):
+        """Milliseconds of one regrid of the hierarchy on its own rule (|J| dx above the
+        threshold on every level, the same boxes): the device tags read back, then the
+        clustering, the new op lists and the device transfer (`MHD2D.regrid`). Leaves the
+        model on the new hierarchy."""
+        import torch
+
+        model = self.model
+        torch.cuda.synchronize()
+        start = time.perf_counter()
+        tags = model.current_tags(HARRIS_THRESHOLD, levels=HARRIS_LEVELS)
+        tagged = time.perf_counter()
+        model.regrid(tags, max_patch_size=HARRIS_PATCH, min_patch_size=HARRIS_MIN_PATCH)
+        torch.cuda.synchronize()
+        done = time.perf_counter()
+        self.engine = model.engine
+        self.cells = int(sum(p.shape[0] * p.shape[1] for p in model.hierarchy.patches))
+        return {"tags_ms": 1e3 * (tagged - start), "regrid_ms": 1e3 * (done - tagged),
+                "patches_after": len(model.hierarchy.patches),
+                "what": "one regrid on the current tags: device tags read back (tags_ms); host clustering, "
+                        "op lists and engine, device transfer (regrid_ms)"}
+
     @staticmethod
     def describe(args):
         return (f"2D Harris sheet on [-1,1]x[-2,2], base {HARRIS_BASE[0]}x{HARRIS_BASE[1]}, periodic x, "
@@ -941,6 +963,8 @@ def extra_workload(name, args, rank, world, local, barrier):
         entry["plain_fp64"]["speedup_of_value"] = run["value"] / world / entry["plain_fp64"]["value"]
     if rank == 0 and not args.no_accuracy:
         entry["accuracy"] = work.accuracy()
+    if hasattr(work, "regrid_timing"):
+        entry["regrid"] = work.regrid_timing()  # last: it moves the model to a new hierarchy
     del work
     torch.cuda.empty_cache()
     return entry
