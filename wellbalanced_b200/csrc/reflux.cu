@@ -394,6 +394,7 @@ template <typename S, typename R>
 void launch_face_flux_staged(const S* pool, const PatchDesc* patches, const FaceFluxOp* ops, int nops, int nfaces,
                              const double* b0, double gamma, int limiter, const double* bflux, double* reg,
                              cudaStream_t stream) {
+  if (nfaces <= 0) return;
   const int grid = (nfaces + kStagedThreads - 1) / kStagedThreads;
   switch (limiter) {
     case 0: face_flux_staged_kernel<S, R, 0><<<grid, kStagedThreads, 0, stream>>>(pool, patches, ops, nops, nfaces, b0[0], b0[1], b0[2], gamma, bflux, reg); break;
