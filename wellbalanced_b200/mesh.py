@@ -93,7 +93,15 @@ class AMRHierarchy:
         return tuple((hi - lo) / n for (lo, hi), n in zip(self.bounds, self.level_shape(level), strict=True))
 
     def patches_at_level(self, level):
-        return [p for p in self.patches if p.level == level]
+        # grouped once per state of the patch list (patches are only appended; a new list
+        # object or a new length regroups)
+        key = (id(self.patches), len(self.patches))
+        if getattr(self, "_by_level_key", None) != key:
+            grouped = {}
+            for p in self.patches:
+                grouped.setdefault(p.level, []).append(p)
+            self._by_level, self._by_level_key = grouped, key
+        return list(self._by_level.get(level, ()))
 
     def add_patch(self, level, box):
         """A patch on ``level`` (>= 1) over ``box``, aligned to the coarse cells."""
