@@ -9,7 +9,7 @@ tagger will flag at any of the next K steps; regridding on its tags every K step
 the refined region ahead of the flow. Network: 16 -> 64 -> 64 -> 1 with ReLU, bfloat16
 weights and float32 accumulation; forward pass on the tensor cores (``wb_mlp_forward``),
 backward pass and Adam on the device (``wb_mlp_backward``, ``wb_mlp_adam``); the float64
-NumPy restatement ``oracle/mlp.py`` checks them. The plain tagger stays the judge: the
+NumPy restatement ``oracle/mlp.py`` checks them. The plain tagger stays the referee: the
 miss rate is the fraction of its flagged cells the learned tags do not cover.
 
 `multiblast` builds the 3D magnetised multi-blast problem (eight seeded overpressure
@@ -258,18 +258,18 @@ def covered_level0(model):
     return covered(model, 0)
 
 
-def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, max_patch_size=8, judge=None):
+def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, max_patch_size=8, uniform=None):
     """Advance a model with `levels` refined levels for `steps` steps, regridding on
     ``tags_of(model)`` (tags per level, as ``current_tags``) before every ``interval``-th
     step (the first regrid repeated `levels` times, so that every level exists from the
-    start); after each step the plain tagger judges the hierarchy: the fraction of the
+    start); after each step the plain tagger scores the hierarchy: the fraction of the
     level-0 cells it flags (|J| dx > threshold) that no level-1 patch covers.
 
-    The flags come from ``judge``, a uniform run of the same problem advanced in lockstep
+    The flags come from ``uniform``, a uniform run of the same problem advanced in lockstep
     (the refined run's dt), when given: the plain tagger on the refined run's own level 0
     also flags the coarse cells beside each coarse-fine boundary, where the central
     differences straddle restricted fine values, and those flags follow the patches rather
-    than the flow. Without a judge, the refined run's own level-0 flags.
+    than the flow. Without it, the refined run's own level-0 flags.
 
     Returns the largest such miss over the steps, the mean fraction of level-0 cells under
     level 1 (the refinement's cost), the mean count of refined cells, the regrid count and
@@ -292,11 +292,11 @@ def amr_run(model, tags_of, *, interval, steps, threshold, levels=1, buffer=1, m
             regrid_seconds += time.perf_counter() - start
         start = time.perf_counter()
         dt = model.step()
-        if judge is not None:
-            judge.step(dt)
+        if uniform is not None:
+            uniform.step(dt)
         torch.cuda.synchronize()
         step_seconds += time.perf_counter() - start
-        flagged = (judge if judge is not None else model).current_tags(threshold, 1)[0]
+        flagged = (uniform if uniform is not None else model).current_tags(threshold, 1)[0]
         under = covered(model, 0)
         if flagged.any():
             worst = max(worst, float((flagged & ~under).sum()) / float(flagged.sum()))
@@ -315,7 +315,7 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
     ``test_steps`` steps from the same state, one regridded every K steps on the learned
     tags, one on the plain tags of the regrid step (``current_tags``, grown by the
     clustering's ``buffer`` like the other); the plain tagger on a uniform run of the same
-    problem advanced in lockstep judges both after every step.
+    problem advanced in lockstep scores both after every step.
     With ``fallback`` the learned run regrids on the union of the learned tags and the plain
     tags of the regrid step (the plain tagger as the fallback: every cell it flags now is
     refined, the learned tags add the cells it will flag). The interval a tagger reaches is
@@ -340,10 +340,10 @@ def interval_study(n=32, *, intervals=(2, 4, 8), train_steps=48, test_steps=24, 
         for name, tags_of in (("learned", learned), ("plain", lambda m: m.current_tags(threshold, levels))):
             model = multiblast(n, seed=seed)
             model.advance(train_steps)
-            judge = multiblast(n, seed=seed)
-            judge.advance(train_steps)
+            uniform = multiblast(n, seed=seed)
+            uniform.advance(train_steps)
             runs[name] = amr_run(model, tags_of, interval=K, steps=test_steps, threshold=threshold, levels=levels,
-                                 buffer=buffer, max_patch_size=max_patch_size, judge=judge)
+                                 buffer=buffer, max_patch_size=max_patch_size, uniform=uniform)
         out["intervals"][K] = runs
     for name in ("learned", "plain"):
         ok = [K for K in intervals if out["intervals"][K][name]["miss"] < 0.01]
