@@ -99,3 +99,36 @@ def test_op_points_follow_the_list_size():
     assert op_points(64 * OP_WAVE) == 64
     assert op_points(64 * OP_WAVE + 1) == 128
     assert op_points(10**9) == 1024
+
+
+def test_face_numbering_maps_every_face_to_its_op():
+    """The staged register's flat face numbering (CPU): each op's `first` is the prefix sum of
+    the lengths, and the binary search the kernel runs over `first` returns, for every face,
+    the op holding it and its position in the op."""
+    from wellbalanced_b200.mesh import AMRHierarchy, Layout, number_faces
+
+    mesh = AMRHierarchy((32, 32), ((0.0, 1.0), (0.0, 1.0)), periodic=(True, False))
+    mesh.add_patch(1, ((12, 40), (20, 44)))
+    mesh.add_patch(1, ((40, 60), (8, 30)))
+    mesh.add_patch(2, ((30, 60), (48, 80)))
+    layout = Layout(mesh)
+    ops, total = number_faces(layout.face_flux_ops)
+    assert ops.size == layout.face_flux_ops.size > 0
+    assert total == int(layout.face_flux_ops["len"].sum())
+    seen = []
+    for face in range(total):
+        lo, hi = 0, ops.size - 1
+        while lo < hi:  # the kernel's search: the last op whose first face is not after `face`
+            mid = (lo + hi + 1) >> 1
+            if ops["first"][mid] <= face:
+                lo = mid
+            else:
+                hi = mid - 1
+        s = face - int(ops["first"][lo])
+        assert 0 <= s < int(ops["len"][lo])
+        seen.append((lo, s))
+    assert seen == [(i, s) for i in range(ops.size) for s in range(int(ops["len"][i]))]
+    # the numbering leaves the other fields alone
+    for name in ops.dtype.names:
+        if name != "first":
+            np.testing.assert_array_equal(ops[name], layout.face_flux_ops[name])

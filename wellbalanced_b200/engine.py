@@ -25,7 +25,7 @@ import numpy as np
 import torch
 
 from wellbalanced_b200 import _lib
-from wellbalanced_b200.mesh import Layout, _concat, size_ops
+from wellbalanced_b200.mesh import Layout, _concat, number_faces, size_ops
 
 _DTYPES = {32: torch.float32, 64: torch.float64, _lib.MATH32_STATE64: torch.float64}
 
@@ -121,12 +121,7 @@ class Engine:
         #: register reads the fine faces there instead of recomputing them
         self.bflux = None
         self.staged_fluxes = True
-        face_ops = L.face_flux_ops.copy()
-        if face_ops.size:
-            # each op's first coarse face in the flat numbering of all ops' faces (the staged
-            # register kernel's thread index)
-            face_ops["first"] = np.concatenate([[0], np.cumsum(face_ops["len"])[:-1]]).astype(np.int32)
-        self.nface_faces = int(face_ops["len"].sum()) if face_ops.size else 0
+        face_ops, self.nface_faces = number_faces(L.face_flux_ops)
         self.face_flux_ops = _device_bytes(face_ops, self.device, _lib.FACE_FLUX_OP)
         self.nface = int(L.face_flux_ops.size)
         self.reflux_ops = _device_bytes(L.reflux_ops, self.device, _lib.REFLUX_OP)

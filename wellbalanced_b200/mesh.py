@@ -355,6 +355,19 @@ def trim_interp_ops(interp, same):
     return np.concatenate(out).astype(interp.dtype)
 
 
+def number_faces(face_ops):
+    """A copy of the interface ops with each op's first coarse face in the flat numbering
+    of all ops' faces (`FaceFluxOp.first`: the prefix sum of the lengths, in list order),
+    and the total count: the staged register kernel runs one thread per face and finds its
+    op by binary search over `first`."""
+    ops = np.atleast_1d(np.asarray(face_ops)).copy()
+    if ops.size == 0:
+        return ops, 0
+    lengths = ops["len"].astype(np.int64)
+    ops["first"] = np.concatenate([[0], np.cumsum(lengths)[:-1]]).astype(np.int32)
+    return ops, int(lengths.sum())
+
+
 def _concat(arrays, dtype):
     """Records of ``arrays`` in one array of the C layout ``dtype`` (``np.concatenate``
     alone may repack a padded structured dtype)."""
