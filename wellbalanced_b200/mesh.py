@@ -418,6 +418,22 @@ class Layout:
                 flags.append(not self._plane_provided(p, a))
             self.own.append(tuple(flags))
 
+    def _level_lows(self, level):
+        """The lower corners of the level's patches (patches x axes), cached."""
+        cache = self.__dict__.setdefault("_lows_cache", {})
+        if level not in cache:
+            cache[level] = np.array([[q.box[b][0] for b in range(self.ndim)] for q in self.h.patches_at_level(level)],
+                                    dtype=np.int64).reshape(-1, self.ndim)
+        return cache[level]
+
+    def _level_highs(self, level):
+        """The upper corners of the level's patches (patches x axes), cached."""
+        cache = self.__dict__.setdefault("_highs_cache", {})
+        if level not in cache:
+            cache[level] = np.array([[q.box[b][1] for b in range(self.ndim)] for q in self.h.patches_at_level(level)],
+                                    dtype=np.int64).reshape(-1, self.ndim)
+        return cache[level]
+
     def _plane_provided(self, p, a):
         """Whether same-level patches' lower node planes cover p's upper plane along a."""
         h = self.h
@@ -426,20 +442,22 @@ class Layout:
         # transverse node range of the plane, inclusive
         need = [(p.box[b][0], p.box[b][1] + 1) for b in range(self.ndim) if b != a]
         covered = np.zeros([hi - lo for lo, hi in need], dtype=bool)
-        for q in h.patches_at_level(p.level):
-            lo = q.box[a][0]
-            if lo == plane or (h.periodic[a] and lo + n_level == plane):
-                # q's computed node range along the transverse axes (its lower plane),
-                # conservatively [lo, hi) there: its upper nodes may be someone else's
-                idx = []
-                for (nlo, nhi), b in zip(need, [b for b in range(self.ndim) if b != a], strict=True):
-                    qlo, qhi = q.box[b]
-                    s, e = max(nlo, qlo), min(nhi, qhi + 1)
-                    if s >= e:
-                        break
-                    idx.append(slice(s - nlo, e - nlo))
-                else:
-                    covered[tuple(idx)] = True
+        same = h.patches_at_level(p.level)
+        lows = self._level_lows(p.level)[:, a]
+        touch = (lows == plane) | ((lows + n_level == plane) if h.periodic[a] else False)
+        for qi in np.flatnonzero(touch):  # the patches whose lower plane is p's upper one
+            q = same[qi]
+            # q's computed node range along the transverse axes (its lower plane),
+            # conservatively [lo, hi) there: its upper nodes may be someone else's
+            idx = []
+            for (nlo, nhi), b in zip(need, [b for b in range(self.ndim) if b != a], strict=True):
+                qlo, qhi = q.box[b]
+                s, e = max(nlo, qlo), min(nhi, qhi + 1)
+                if s >= e:
+                    break
+                idx.append(slice(s - nlo, e - nlo))
+            else:
+                covered[tuple(idx)] = True
         return bool(covered.all())
 
     # pool ----------------------------------------------------------------------------------
@@ -998,9 +1016,10 @@ class Layout:
                     else:
                         continue
                     face_c = outside_w + 1 if side == 0 else outside_w
-                    for c in h.patches_at_level(f.level - 1):
-                        if not c.box[a][0] <= outside_w < c.box[a][1]:
-                            continue
+                    coarses = h.patches_at_level(f.level - 1)
+                    lows, highs = self._level_lows(f.level - 1)[:, a], self._level_highs(f.level - 1)[:, a]
+                    for ci in np.flatnonzero((lows <= outside_w) & (outside_w < highs)):
+                        c = coarses[ci]
                         ranges = []
                         for b in trans:
                             lo = max(f.box[b][0] // 2, c.box[b][0])
