@@ -189,3 +189,49 @@ def test_unmerged_periodic_planes_break_conservation():
     periodic boundary start from different A_z and their shared-face fluxes disagree."""
     _, drift = _three_regrids(merge=False)
     assert drift > 1e-12
+
+
+@pytest.mark.parametrize("periodic", [(False, False), (True, False)])
+def test_cluster_boxes_respect_the_parents_and_cover_the_nestable_tags(periodic):
+    """Clustering a refined level under two parent patches (outflow and periodic x): every
+    box lies in the nestable region (inside the parents by the nesting margin), the boxes are
+    disjoint, at most `max_size` a side, and every grown tag of the nestable region is
+    covered; boxes reach the smallest side where free nestable cells allow."""
+    rng = np.random.default_rng(7)
+    shape = (48, 40)
+    parents = [((0, 20), (4, 36)), ((20, 44), (8, 30))]
+    tags = rng.random(shape) < 0.06
+    tags[10:16, 12:20] = True
+    boxes = cluster_tags(tags, buffer=1, max_size=8, min_size=8, parents=parents, periodic=periodic)
+    allowed = nesting_mask(shape, parents, periodic)
+    held = np.zeros(shape, dtype=int)
+    for box in boxes:
+        assert all(1 <= hi - lo <= 8 for lo, hi in box)
+        region = tuple(slice(lo, hi) for lo, hi in box)
+        assert allowed[region].all()
+        held[region] += 1
+    assert held.max() == 1
+    grown = tags.copy()
+    for a in range(2):
+        up = np.roll(grown, 1, axis=a)
+        down = np.roll(grown, -1, axis=a)
+        if not periodic[a]:
+            edge = [slice(None)] * 2
+            edge[a] = 0
+            up[tuple(edge)] = False
+            edge[a] = -1
+            down[tuple(edge)] = False
+        grown = grown | up | down
+    assert np.all(held[grown & allowed] == 1)
+    # a box below the smallest side (4 cells here: min_size 8 on the refined level) has no
+    # room left along that axis: each neighbouring slab is outside the level, outside the
+    # nestable region, or holds part of another box
+    for box in boxes:
+        for a, (lo, hi) in enumerate(box):
+            if hi - lo >= 4:
+                continue
+            for slab in ((hi, hi + 1), (lo - 1, lo)):
+                if slab[0] < 0 or slab[1] > shape[a]:
+                    continue
+                region = tuple(slice(*slab) if b == a else slice(*box[b]) for b in range(2))
+                assert held[region].any() or not allowed[region].all(), (box, a, slab)
