@@ -151,7 +151,7 @@ class Engine:
         #: run the reflux, restriction, halo-fill and stable-step phases between the stage
         #: kernels as op programs (`wb_run_program`, one launch each: six launches per
         #: refined step instead of ~26). Off by default: on the B200 the separate launches
-        #: finish the ~2100-patch Harris step in 0.66 ms against 0.79 ms for the programs,
+        #: finish the ~2300-patch Harris step in 0.62 ms against 0.74 ms for the programs,
         #: whose in-kernel phase waits cost more than the launch boundaries they replace
         self.use_programs = False
         self._programs = {}
